@@ -1,0 +1,143 @@
+/*
+ * modisp_b200.h -- C ABI of the B200 dispersion engine (libmodisp_b200.so).
+ *
+ * The engine is the drop-in for modisp's CUDA backend plugin: one engine object
+ * per Solver, created with a capacity and a fixed geometry, run once per chunk,
+ * closed when the Solver is.  Every entry point maps onto one item of the
+ * reference plugin interface; the citation names the reference file:line it
+ * replaces (paths relative to the modisp source tree).  All functions return 0
+ * on success and a nonzero status on failure, with the message available from
+ * md200_last_error() (the reference's legacy C ABI convention,
+ * cpp/cuda/coarse_scan.cu:31-39).  No torch types cross this boundary.
+ *
+ * Arrays are C-contiguous: models [B, L] float64, periods [T], bounds [B, 2],
+ * phase/group velocities [B, nmodes, T] (model, mode, period -- the reference
+ * output layout, cpp/cuda/refine.cuh:168-172), trace arrays [B, T].
+ */
+#ifndef MODISP_B200_H
+#define MODISP_B200_H
+#include <stddef.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MD200_ABI_VERSION 1
+/* Statistics written by md200_run (indices into the stats array). */
+enum md200_stat {
+  MD200_STAT_EVALUATIONS = 0,      /* secular evaluations, all precisions */
+  MD200_STAT_EVALUATIONS_FP32 = 1, /* of which FP32 */
+  MD200_STAT_LAYER_STEPS = 2,      /* layer recurrence steps, all evaluations */
+  MD200_STAT_LAYER_STEPS_FP32 = 3,
+  MD200_STAT_BRACKETS = 4,         /* sign-change brackets refined */
+  MD200_STAT_PROBES = 5,           /* same-sign trough probes */
+  MD200_STAT_PROBE_PAIRS = 6,      /* probes that split a hidden root pair */
+  MD200_STAT_REPAIR_TRACES = 7,    /* FP32 traces re-scanned in FP64 */
+  MD200_STAT_UNCONVERGED = 8,      /* traces reported unconverged */
+  MD200_STAT_GROUP_ROOTS = 9,      /* group velocities computed */
+  MD200_STAT_ROOTS = 10,           /* finite phase velocities returned */
+  MD200_STAT_TRACES = 11,          /* traces searched */
+  MD200_STAT_DUAL_LAYER_STEPS = 12,/* layer steps of forward-mode derivative evaluations */
+  MD200_STAT_CONT_ACCEPTED = 13,   /* continuation targets accepted */
+  MD200_STAT_CONT_FALLBACK = 14,   /* continuation targets searched globally */
+  MD200_STAT_COUNT = 16
+};
+
+typedef struct md200_engine md200_engine;
+
+/* Engine configuration; the fields mirror the positional arguments of the
+ * reference QeSolver constructor (cpp/cuda/qe.cu:978, called from
+ * python/modisp/__init__.py:398-400) plus the engine's own tuning knobs. */
+typedef struct md200_options {
+  int accuracy;            /* 0 high, 1 balanced, 2 fast, 4 auto (recorded; the scan rule is the same) */
+  double period_threshold; /* accepted for compatibility */
+  double close_root_rtol;  /* close-root threshold, default 0.005 */
+  int shape;               /* accepted for compatibility */
+  double sampling_rtol;    /* accepted for compatibility */
+  int secular;             /* 0 dunkin, 1 fast: one compound-matrix evaluator serves both */
+  int refinement;          /* 1 Brent (the engine's refinement); 0 and 2 are accepted */
+  int love_phase;          /* accepted for compatibility */
+  int single_precision;    /* 1: FP32 scan + FP64 refinement; 0: FP64 throughout */
+  int group_velocity;      /* 1: FP64 group velocity from implicit derivatives */
+  double group_rtol;       /* accepted for compatibility (the derivative is analytic) */
+  int continuation;        /* 1: anchor continuation over sorted unique periods */
+  int anchor_stride;       /* anchor spacing in periods (>= 2) */
+  double scan_density;     /* scan points per phase unit; <= 0 selects the default */
+  int log_points;          /* background log-spaced points per window; <= 0 default */
+  int warps_per_block;     /* scan CTA shape; <= 0 default */
+  int blocks_per_sm;       /* persistent CTAs per SM; <= 0 default */
+} md200_options;
+
+/* Fill *options with the defaults of a high-accuracy FP64 engine. */
+void md200_default_options(md200_options *options);
+
+/* Replaces QeSolver(B, L, nf, nmodes, ...) (cpp/cuda/qe.cu:978-1036).  capacity is
+ * the maximum number of models per run; layers, periods, nmodes fix the
+ * geometry.  Returns NULL on failure. */
+md200_engine *md200_create(int device, int capacity, int layers, int periods, int nmodes,
+                           const md200_options *options);
+
+/* Replaces QeSolver.run(...) (cpp/cuda/qe.cu:1060-1119) with host arrays: copies
+ * inputs to the device, solves, copies outputs back and synchronises.
+ *   thickness, vp, vs, rho : [models, layers]
+ *   periods                : [periods]
+ *   bounds                 : [models, 2] search windows [lo, hi), or NULL to compute
+ *                            them on the device (cpp/cpu/solver.cpp:781-790).  A
+ *                            non-positive lo asks for the automatic lower bound;
+ *                            hi is capped below the half-space shear velocity.
+ *   wave                   : 0 Rayleigh, 1 Love
+ * Outputs (NULL to skip the optional ones):
+ *   velocity [models, nmodes, periods] float64 (NaN where no root)
+ *   flags, levels, counts [models, periods]
+ *   group, group_flags [models, nmodes, periods] (engine created with group_velocity)
+ *   prediction_flags [models, periods] (engine created with continuation)
+ *   bounds_out [models, 2] the windows searched
+ *   stats [nstats] counters, see enum md200_stat. */
+int md200_run(md200_engine *engine, const double *thickness, const double *vp, const double *vs,
+              const double *rho, int models, const double *periods, const double *bounds,
+              double c_tol_rel, double f_accept, int wave, double *velocity, unsigned *flags,
+              int *levels, int *counts, double *group, unsigned *group_flags,
+              unsigned *prediction_flags, double *bounds_out, unsigned long long *stats,
+              int nstats);
+
+/* As md200_run, but every array is a device pointer and the work is enqueued on
+ * `stream` (a cudaStream_t, or NULL for the engine's own stream) without a host
+ * synchronisation.  stats, if given, is a device array of MD200_STAT_COUNT
+ * counters. */
+int md200_run_device(md200_engine *engine, const double *thickness, const double *vp,
+                     const double *vs, const double *rho, int models, const double *periods,
+                     const double *bounds, double c_tol_rel, double f_accept, int wave,
+                     double *velocity, unsigned *flags, int *levels, int *counts, double *group,
+                     unsigned *group_flags, unsigned *prediction_flags, double *bounds_out,
+                     unsigned long long *stats, void *stream);
+
+/* Replaces QeSolver.close() (cpp/cuda/qe.cu:1039-1059). */
+void md200_destroy(md200_engine *engine);
+
+/* Message of the last failure on this thread (static storage). */
+const char *md200_last_error(void);
+
+/* Module functions of the plugin (cpp/cuda/qe.cu:1131-1142): */
+int md200_device_count(void);                 /* number of CUDA devices, 0 if none */
+int md200_available(int device);              /* 1 when `device` is a usable sm_100 GPU */
+int md200_set_device(int device);
+int md200_memory_info(size_t *free_bytes, size_t *total_bytes);
+int md200_device_name(int device, char *name, int length);
+
+/* Kernel attributes of the engine's kernels (cpp/cuda/qe.cu:1143-1164): writes a
+ * JSON object describing registers, shared memory and occupancy to `json`. */
+int md200_kernel_report(int layers, int single_precision, char *json, int length);
+
+/* Group velocities of one model's known ordered roots (guards included), for a
+ * trace repaired outside the engine: replaces the plugin's _review_groups
+ * (cpp/common/review_groups.hpp:9-63, cpp/cuda/review_groups.cu:6-35).  Host
+ * arrays: one model [layers], roots [known]; outputs [modes].  A root without a
+ * slot is MISSING_ROOT (1), a close pair CLOSE_ROOT (16). */
+int md200_group_roots(const double *thickness, const double *vp, const double *vs,
+                      const double *rho, int layers, int wave, double period,
+                      const double *roots, int known, int modes, double close_rtol,
+                      double *group, unsigned *group_flags);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

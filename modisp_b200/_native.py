@@ -1,0 +1,222 @@
+"""ctypes binding of the engine's C ABI (include/modisp_b200.h).
+
+The library is loaded from ``modisp_b200/_lib``.  There is no fallback: if the
+library is missing or cannot be loaded, every entry point raises
+``BackendUnavailableError`` with the reason.
+"""
+from __future__ import annotations
+
+import ctypes
+import threading
+from pathlib import Path
+
+import numpy as np
+
+LIBRARY = Path(__file__).resolve().parent / "_lib" / "libmodisp_b200.so"
+ABI_VERSION = 1
+STAT_NAMES = ("evaluations", "evaluations_fp32", "layer_steps", "layer_steps_fp32", "brackets",
+              "trough_probes", "probe_pairs", "fp64_repair_traces", "unconverged", "group_roots",
+              "roots", "traces", "dual_layer_steps", "continuation_accepted",
+              "continuation_fallbacks", "reserved")
+STAT_COUNT = 16
+
+
+class BackendUnavailableError(RuntimeError):
+    """The B200 engine cannot run here (library or GPU missing)."""
+
+
+class Options(ctypes.Structure):
+    _fields_ = [
+        ("accuracy", ctypes.c_int),
+        ("period_threshold", ctypes.c_double),
+        ("close_root_rtol", ctypes.c_double),
+        ("shape", ctypes.c_int),
+        ("sampling_rtol", ctypes.c_double),
+        ("secular", ctypes.c_int),
+        ("refinement", ctypes.c_int),
+        ("love_phase", ctypes.c_int),
+        ("single_precision", ctypes.c_int),
+        ("group_velocity", ctypes.c_int),
+        ("group_rtol", ctypes.c_double),
+        ("continuation", ctypes.c_int),
+        ("anchor_stride", ctypes.c_int),
+        ("scan_density", ctypes.c_double),
+        ("log_points", ctypes.c_int),
+        ("warps_per_block", ctypes.c_int),
+        ("blocks_per_sm", ctypes.c_int),
+    ]
+
+
+_lib = None
+_lock = threading.Lock()
+_P = ctypes.c_void_p
+_D = ctypes.c_double
+_I = ctypes.c_int
+
+EXPORTS = {
+    "md200_default_options": (None, [ctypes.POINTER(Options)]),
+    "md200_create": (_P, [_I, _I, _I, _I, _I, ctypes.POINTER(Options)]),
+    "md200_run": (_I, [_P, _P, _P, _P, _P, _I, _P, _P, _D, _D, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I]),
+    "md200_run_device": (_I, [_P, _P, _P, _P, _P, _I, _P, _P, _D, _D, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "md200_destroy": (None, [_P]),
+    "md200_last_error": (ctypes.c_char_p, []),
+    "md200_device_count": (_I, []),
+    "md200_available": (_I, [_I]),
+    "md200_set_device": (_I, [_I]),
+    "md200_memory_info": (_I, [ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)]),
+    "md200_device_name": (_I, [_I, ctypes.c_char_p, _I]),
+    "md200_kernel_report": (_I, [_I, _I, ctypes.c_char_p, _I]),
+    "md200_group_roots": (_I, [_P, _P, _P, _P, _I, _I, _D, _P, _I, _I, _D, _P, _P]),
+}
+
+
+def lib():
+    """The loaded engine library (raises BackendUnavailableError if absent)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is None:
+            if not LIBRARY.exists():
+                raise BackendUnavailableError(
+                    f"engine library {LIBRARY} is not built; run `python -m modisp_b200.build`")
+            try:
+                handle = ctypes.CDLL(str(LIBRARY))
+            except OSError as exc:
+                raise BackendUnavailableError(f"engine library cannot be loaded: {exc}") from exc
+            for name, (restype, argtypes) in EXPORTS.items():
+                fn = getattr(handle, name)
+                fn.restype = restype
+                fn.argtypes = argtypes
+            _lib = handle
+    return _lib
+
+
+def last_error() -> str:
+    return lib().md200_last_error().decode(errors="replace")
+
+
+def check(status: int) -> None:
+    if status != 0:
+        raise RuntimeError(last_error())
+
+
+def default_options() -> Options:
+    o = Options()
+    lib().md200_default_options(ctypes.byref(o))
+    return o
+
+
+def ptr(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+class Engine:
+    """Owning handle of one md200_engine."""
+
+    def __init__(self, device: int, capacity: int, layers: int, periods: int, nmodes: int,
+                 options: Options):
+        self.device, self.capacity, self.layers = int(device), int(capacity), int(layers)
+        self.periods, self.nmodes = int(periods), int(nmodes)
+        self.options = options
+        handle = lib().md200_create(self.device, self.capacity, self.layers, self.periods, self.nmodes,
+                                    ctypes.byref(options))
+        if not handle:
+            raise RuntimeError(last_error())
+        self._handle = handle
+
+    @property
+    def handle(self):
+        if not self._handle:
+            raise RuntimeError("engine is closed")
+        return self._handle
+
+    def run(self, h, vp, vs, rho, periods, bounds, tol, accept, wave, group=False, prediction=False):
+        """Host-array run; returns a dict of numpy outputs."""
+        B, L = h.shape
+        T, nm = self.periods, self.nmodes
+        arrays = [np.ascontiguousarray(x, dtype=np.float64) for x in (h, vp, vs, rho)]
+        per = np.ascontiguousarray(periods, dtype=np.float64)
+        bnd = None if bounds is None else np.ascontiguousarray(bounds, dtype=np.float64)
+        out = dict(velocity=np.empty((B, nm, T)), flags=np.empty((B, T), np.uint32),
+                   levels=np.empty((B, T), np.int32), counts=np.empty((B, T), np.int32),
+                   bounds=np.empty((B, 2)), stats=np.zeros(STAT_COUNT, np.uint64))
+        if group:
+            out["group_velocity"] = np.empty((B, nm, T))
+            out["group_velocity_flags"] = np.empty((B, nm, T), np.uint32)
+        if prediction:
+            out["prediction_flags"] = np.empty((B, T), np.uint32)
+        status = lib().md200_run(
+            self.handle, *(ptr(a) for a in arrays), B, ptr(per), ptr(bnd), float(tol), float(accept),
+            int(wave), ptr(out["velocity"]), ptr(out["flags"]), ptr(out["levels"]), ptr(out["counts"]),
+            ptr(out.get("group_velocity")), ptr(out.get("group_velocity_flags")),
+            ptr(out.get("prediction_flags")), ptr(out["bounds"]), ptr(out["stats"]), STAT_COUNT)
+        check(status)
+        out["stats"] = dict(zip(STAT_NAMES, (int(x) for x in out["stats"])))
+        return out
+
+    def run_device(self, h, vp, vs, rho, models, periods, bounds, tol, accept, wave, velocity, flags,
+                   levels, counts, group=None, group_flags=None, prediction=None, bounds_out=None,
+                   stats=None, stream=None):
+        """Device-pointer run (integer addresses), enqueued on `stream` (cudaStream_t address)."""
+        c = ctypes.c_void_p
+        status = lib().md200_run_device(
+            self.handle, c(h), c(vp), c(vs), c(rho), int(models), c(periods), c(bounds) if bounds else None,
+            float(tol), float(accept), int(wave), c(velocity), c(flags), c(levels), c(counts),
+            c(group) if group else None, c(group_flags) if group_flags else None,
+            c(prediction) if prediction else None, c(bounds_out) if bounds_out else None,
+            c(stats) if stats else None, c(stream) if stream else None)
+        check(status)
+
+    def close(self):
+        if getattr(self, "_handle", None):
+            lib().md200_destroy(self._handle)
+            self._handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def device_count() -> int:
+    return int(lib().md200_device_count())
+
+
+def available(device: int = 0) -> bool:
+    return bool(lib().md200_available(int(device)))
+
+
+def set_device(device: int) -> None:
+    check(lib().md200_set_device(int(device)))
+
+
+def memory_info() -> tuple[int, int]:
+    free, total = ctypes.c_size_t(), ctypes.c_size_t()
+    check(lib().md200_memory_info(ctypes.byref(free), ctypes.byref(total)))
+    return int(free.value), int(total.value)
+
+
+def device_name(device: int = 0) -> str:
+    buf = ctypes.create_string_buffer(256)
+    check(lib().md200_device_name(int(device), buf, 256))
+    return buf.value.decode()
+
+
+def group_roots(h, vp, vs, rho, wave, period, roots, modes, close_rtol=.005):
+    """Group velocities and flags of one model's ordered roots (arrays of length modes)."""
+    arrays = [np.ascontiguousarray(x, dtype=np.float64).ravel() for x in (h, vp, vs, rho)]
+    r = np.ascontiguousarray(roots, dtype=np.float64).ravel()
+    group = np.empty(int(modes))
+    flags = np.empty(int(modes), np.uint32)
+    check(lib().md200_group_roots(*(ptr(a) for a in arrays), arrays[0].size, int(wave), float(period),
+                                  ptr(r), r.size, int(modes), float(close_rtol), ptr(group), ptr(flags)))
+    return group, flags
+
+
+def kernel_report(layers: int, single_precision: bool = False) -> dict:
+    import json
+    buf = ctypes.create_string_buffer(8192)
+    check(lib().md200_kernel_report(int(layers), int(bool(single_precision)), buf, 8192))
+    return json.loads(buf.value.decode())

@@ -1,0 +1,516 @@
+// engine.cu -- host orchestration and C ABI of the modisp_b200 engine.
+//
+// One engine per Solver (the reference's QeSolver contract, cpp/cuda/qe.cu:836-1170):
+// device workspace sized at creation for a capacity of models, one stream, all
+// stages enqueued back to back with device-side work lists so a run needs no
+// host synchronisation until its outputs are read.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/modisp_b200.h"
+#include "kernels.cuh"
+
+using namespace md200;
+
+namespace {
+
+thread_local std::string g_error;
+
+int fail(const std::string &msg) {
+  g_error = msg;
+  return 1;
+}
+
+#define MD200_CK(call)                                                                     \
+  do {                                                                                     \
+    cudaError_t err__ = (call);                                                            \
+    if (err__ != cudaSuccess)                                                              \
+      return fail(std::string("modisp_b200 CUDA: ") + cudaGetErrorString(err__) + " (" +  \
+                  #call + ")");                                                            \
+  } while (0)
+
+template <class T>
+cudaError_t dalloc(T **p, size_t count) {
+  *p = nullptr;
+  if (count == 0) count = 1;
+  return cudaMalloc(reinterpret_cast<void **>(p), count * sizeof(T));
+}
+
+}  // namespace
+
+struct md200_engine {
+  int device = 0, cap = 0, L = 0, T = 0, nmodes = 0;
+  md200_options o{};
+  cudaStream_t stream = nullptr;
+  Dev d{};
+  int sortcap = 0, prep_warps = 4, scan_warps = 4, scan_blocks64 = 0, scan_blocks32 = 0;
+  int list_blocks = 0;
+  size_t scan_smem64 = 0, scan_smem32 = 0, prep_smem = 0;
+  // host-path buffers
+  double *in_h = nullptr, *in_vp = nullptr, *in_vs = nullptr, *in_rho = nullptr,
+         *in_per = nullptr, *in_bounds = nullptr;
+  double *out_vel = nullptr, *out_grp = nullptr;
+  unsigned *out_flags = nullptr, *out_gflags = nullptr, *out_pred = nullptr;
+  int *out_levels = nullptr, *out_counts = nullptr;
+  unsigned long long *d_stats = nullptr;
+  unsigned char *pinned = nullptr;
+  size_t pinned_bytes = 0;
+  std::vector<void *> owned;
+};
+
+namespace {
+
+template <class T>
+int own_alloc(md200_engine *e, T **p, size_t count) {
+  MD200_CK(dalloc(p, count));
+  e->owned.push_back(*p);
+  return 0;
+}
+
+void release(md200_engine *e) {
+  if (!e) return;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(e->device);
+  if (e->stream) cudaStreamSynchronize(e->stream);
+  for (void *p : e->owned) cudaFree(p);
+  e->owned.clear();
+  if (e->pinned) cudaFreeHost(e->pinned);
+  if (e->stream) cudaStreamDestroy(e->stream);
+  cudaSetDevice(prev);
+}
+
+size_t scan_smem(int warps, int Ls, size_t elem) {
+  const size_t tab = (static_cast<size_t>(EVAL_ROWS) * Ls * elem + 15) & ~size_t(15);
+  return static_cast<size_t>(warps) * (tab + 32 * sizeof(double));
+}
+
+int setup(md200_engine *e) {
+  MD200_CK(cudaSetDevice(e->device));
+  MD200_CK(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+  const int B = e->cap, L = e->L, T = e->T, nm = e->nmodes;
+  Dev &d = e->d;
+  d.Lmax = L;
+  d.Ls = (L + 3) & ~3;
+  d.T = T;
+  d.nmodes = nm;
+  d.K = nm + 2;
+  d.KB = d.K;
+  d.nlog = e->o.log_points > 0 ? e->o.log_points : 128;
+  d.density = e->o.scan_density > 0. ? e->o.scan_density : 16.;
+  d.nkmax = d.nlog + 1 + 2 * L;
+  d.nsmax = 6 * L + 32;
+  d.close_rtol = e->o.close_root_rtol > 0. ? e->o.close_root_rtol : .005;
+  d.fp32 = e->o.single_precision ? 1 : 0;
+  d.group = e->o.group_velocity ? 1 : 0;
+  const size_t nt = static_cast<size_t>(B) * T;
+  if (own_alloc(e, &d.mL, B) || own_alloc(e, &d.mwater, B) || own_alloc(e, &d.mstate, B) ||
+      own_alloc(e, &d.mlo, B) || own_alloc(e, &d.mhi, B) || own_alloc(e, &d.malpha, B) ||
+      own_alloc(e, &d.layer64, static_cast<size_t>(B) * ROWS * d.Ls) ||
+      own_alloc(e, &d.layer32, static_cast<size_t>(B) * ROWS * d.Ls) ||
+      own_alloc(e, &d.knot, static_cast<size_t>(B) * d.nkmax) || own_alloc(e, &d.nknot, B) ||
+      own_alloc(e, &d.seed, static_cast<size_t>(B) * d.nsmax) || own_alloc(e, &d.nseed, B) ||
+      own_alloc(e, &d.nbr, nt) || own_alloc(e, &d.tflags, nt) ||
+      own_alloc(e, &d.slot, nt * d.KB * SLOT) ||
+      own_alloc(e, &d.trace_list, nt) || own_alloc(e, &d.repair_list, nt) ||
+      own_alloc(e, &d.refine_list, 2 * nt * d.KB) ||
+      own_alloc(e, &d.group_list, nt * nm) || own_alloc(e, &d.ctr, C_COUNT) ||
+      own_alloc(e, &d.gwin, nt * nm * 2) || own_alloc(e, &e->d_stats, MD200_STAT_COUNT))
+    return 1;
+  // host-path device buffers
+  if (own_alloc(e, &e->in_h, static_cast<size_t>(B) * L) ||
+      own_alloc(e, &e->in_vp, static_cast<size_t>(B) * L) ||
+      own_alloc(e, &e->in_vs, static_cast<size_t>(B) * L) ||
+      own_alloc(e, &e->in_rho, static_cast<size_t>(B) * L) || own_alloc(e, &e->in_per, T) ||
+      own_alloc(e, &e->in_bounds, static_cast<size_t>(B) * 2) ||
+      own_alloc(e, &e->out_vel, nt * nm) || own_alloc(e, &e->out_grp, nt * nm) ||
+      own_alloc(e, &e->out_gflags, nt * nm) || own_alloc(e, &e->out_flags, nt) ||
+      own_alloc(e, &e->out_pred, nt) || own_alloc(e, &e->out_levels, nt) ||
+      own_alloc(e, &e->out_counts, nt))
+    return 1;
+  e->pinned_bytes = sizeof(double) * (4 * static_cast<size_t>(B) * L + T + 2 * static_cast<size_t>(B)) +
+                    nt * nm * (2 * sizeof(double) + sizeof(unsigned)) + nt * 4 * sizeof(int) +
+                    MD200_STAT_COUNT * sizeof(unsigned long long) + 2 * sizeof(double) * B + 64;
+  MD200_CK(cudaMallocHost(reinterpret_cast<void **>(&e->pinned), e->pinned_bytes));
+
+  // launch shapes
+  int sms = 148;
+  MD200_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device));
+  e->scan_warps = e->o.warps_per_block > 0 ? std::min(4, e->o.warps_per_block) : 4;
+  e->scan_smem64 = scan_smem(e->scan_warps, d.Ls, sizeof(double));
+  e->scan_smem32 = scan_smem(e->scan_warps, d.Ls, sizeof(float));
+  MD200_CK(cudaFuncSetAttribute(scan<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(std::max<size_t>(e->scan_smem64, 1024))));
+  MD200_CK(cudaFuncSetAttribute(scan<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(std::max<size_t>(e->scan_smem32, 1024))));
+  int occ64 = 0, occ32 = 0;
+  MD200_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ64, scan<double>, 32 * e->scan_warps,
+                                                         e->scan_smem64));
+  MD200_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ32, scan<float>, 32 * e->scan_warps,
+                                                         e->scan_smem32));
+  if (e->o.blocks_per_sm > 0) {
+    occ64 = std::min(occ64, e->o.blocks_per_sm);
+    occ32 = std::min(occ32, e->o.blocks_per_sm);
+  }
+  e->scan_blocks64 = sms * std::max(1, occ64);
+  e->scan_blocks32 = sms * std::max(1, occ32);
+  e->list_blocks = sms * 8;
+  const int sort_n = std::max(d.nlog + 1 + 2 * L, d.nsmax);
+  int cap2 = 1;
+  while (cap2 < sort_n) cap2 <<= 1;
+  e->sortcap = cap2;
+  e->prep_warps = 4;
+  e->prep_smem = static_cast<size_t>(e->prep_warps) * cap2 * (sizeof(double) + sizeof(int));
+  MD200_CK(cudaFuncSetAttribute(prep_models, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(std::max<size_t>(e->prep_smem, 1024))));
+  return 0;
+}
+
+int validate_geometry(md200_engine *e, int models) {
+  if (!e) return fail("modisp_b200: null engine");
+  if (models < 1 || models > e->cap)
+    return fail("modisp_b200: model count " + std::to_string(models) + " outside 1.." +
+                std::to_string(e->cap));
+  return 0;
+}
+
+int enqueue(md200_engine *e, const double *h, const double *vp, const double *vs, const double *rho,
+            int B, const double *periods, const double *bounds, double tol, double accept, int wave,
+            double *vel, unsigned *flags, int *levels, int *counts, double *grp, unsigned *gflags,
+            unsigned *pred, double *bounds_out, unsigned long long *stats, cudaStream_t s) {
+  if (!(tol > 0.) || !(tol < 1.)) return fail("modisp_b200: c_tol_rel must lie in (0, 1)");
+  if (wave != 0 && wave != 1) return fail("modisp_b200: wave must be 0 (Rayleigh) or 1 (Love)");
+  if (e->d.group && (!grp || !gflags))
+    return fail("modisp_b200: group-velocity engine needs group output arrays");
+  MD200_CK(cudaSetDevice(e->device));
+  Dev d = e->d;
+  d.B = B;
+  d.n_traces = B * e->T;
+  d.wave = wave;
+  d.tol = tol;
+  d.accept = accept;
+  d.h = h;
+  d.vp = vp;
+  d.vs = vs;
+  d.rho = rho;
+  d.periods = periods;
+  d.bounds_in = bounds;
+  d.vel = vel;
+  d.oflags = flags;
+  d.olevels = levels;
+  d.ocounts = counts;
+  d.grp = grp;
+  d.gflags = gflags;
+  d.stats = stats;
+  d.pred = pred;
+  d.bounds_out = bounds_out;
+  const int nt = d.n_traces;
+  MD200_CK(cudaMemsetAsync(d.ctr, 0, sizeof(int) * C_COUNT, s));
+  if (stats) MD200_CK(cudaMemsetAsync(stats, 0, sizeof(unsigned long long) * MD200_STAT_COUNT, s));
+  const int pw = e->prep_warps;
+  prep_models<<<(B + pw - 1) / pw, 32 * pw, e->prep_smem, s>>>(d, e->sortcap, 0);
+  MD200_CK(cudaGetLastError());
+  init_traces<<<(nt + 255) / 256, 256, 0, s>>>(d);
+  MD200_CK(cudaGetLastError());
+  if (d.fp32) {
+    scan<float><<<e->scan_blocks32, 32 * e->scan_warps, e->scan_smem32, s>>>(d, d.trace_list,
+                                                                            C_SCAN_CURSOR, C_NTRACE);
+  } else {
+    scan<double><<<e->scan_blocks64, 32 * e->scan_warps, e->scan_smem64, s>>>(d, d.trace_list,
+                                                                              C_SCAN_CURSOR, C_NTRACE);
+  }
+  MD200_CK(cudaGetLastError());
+  refine<<<e->list_blocks, 128, 0, s>>>(d);
+  MD200_CK(cudaGetLastError());
+  if (d.fp32) {
+    collect_repairs<<<(nt + 255) / 256, 256, 0, s>>>(d);
+    scan<double><<<e->scan_blocks64, 32 * e->scan_warps, e->scan_smem64, s>>>(d, d.repair_list,
+                                                                              C_REPAIR_CURSOR, C_NREPAIR);
+    refine<<<e->list_blocks, 128, 0, s>>>(d);
+    MD200_CK(cudaGetLastError());
+  }
+  assemble<<<(nt + 255) / 256, 256, 0, s>>>(d);
+  MD200_CK(cudaGetLastError());
+  if (d.group) {
+    group_velocity<<<e->list_blocks, 128, 0, s>>>(d);
+    MD200_CK(cudaGetLastError());
+  }
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+void md200_default_options(md200_options *o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->accuracy = 0;
+  o->close_root_rtol = .005;
+  o->shape = 1;
+  o->sampling_rtol = 1e-3;
+  o->refinement = 1;
+  o->love_phase = 1;
+  o->group_rtol = 1e-3;
+  o->anchor_stride = 4;
+}
+
+md200_engine *md200_create(int device, int capacity, int layers, int periods, int nmodes,
+                           const md200_options *options) {
+  if (capacity < 1 || layers < 1 || layers > 256 || periods < 1 || nmodes < 1 || nmodes > 256) {
+    fail("modisp_b200: invalid engine geometry (capacity >= 1, 1 <= layers <= 256, periods >= 1, "
+         "1 <= nmodes <= 256)");
+    return nullptr;
+  }
+  md200_engine *e = new (std::nothrow) md200_engine();
+  if (!e) {
+    fail("modisp_b200: out of host memory");
+    return nullptr;
+  }
+  e->device = device;
+  e->cap = capacity;
+  e->L = layers;
+  e->T = periods;
+  e->nmodes = nmodes;
+  if (options) e->o = *options;
+  else md200_default_options(&e->o);
+  if (setup(e)) {
+    const std::string msg = g_error;
+    release(e);
+    delete e;
+    g_error = msg;
+    return nullptr;
+  }
+  return e;
+}
+
+int md200_run_device(md200_engine *e, const double *h, const double *vp, const double *vs,
+                     const double *rho, int models, const double *periods, const double *bounds,
+                     double tol, double accept, int wave, double *velocity, unsigned *flags,
+                     int *levels, int *counts, double *group, unsigned *group_flags,
+                     unsigned *prediction_flags, double *bounds_out, unsigned long long *stats,
+                     void *stream) {
+  if (validate_geometry(e, models)) return 1;
+  if (!h || !vp || !vs || !rho || !periods || !velocity || !flags || !levels || !counts)
+    return fail("modisp_b200: missing input or output array");
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : e->stream;
+  return enqueue(e, h, vp, vs, rho, models, periods, bounds, tol, accept, wave, velocity, flags,
+                 levels, counts, group, group_flags, prediction_flags, bounds_out, stats, s);
+}
+
+int md200_run(md200_engine *e, const double *h, const double *vp, const double *vs,
+              const double *rho, int models, const double *periods, const double *bounds,
+              double tol, double accept, int wave, double *velocity, unsigned *flags, int *levels,
+              int *counts, double *group, unsigned *group_flags, unsigned *prediction_flags,
+              double *bounds_out, unsigned long long *stats, int nstats) {
+  if (validate_geometry(e, models)) return 1;
+  if (!h || !vp || !vs || !rho || !periods || !velocity || !flags || !levels || !counts)
+    return fail("modisp_b200: missing input or output array");
+  if (e->d.group && (!group || !group_flags))
+    return fail("modisp_b200: group-velocity engine needs group output arrays");
+  MD200_CK(cudaSetDevice(e->device));
+  const size_t B = models, L = e->L, T = e->T, nm = e->nmodes, nt = B * T;
+  // stage inputs through pinned memory
+  unsigned char *p = e->pinned;
+  double *ph = reinterpret_cast<double *>(p);
+  std::memcpy(ph, h, sizeof(double) * B * L);
+  std::memcpy(ph + B * L, vp, sizeof(double) * B * L);
+  std::memcpy(ph + 2 * B * L, vs, sizeof(double) * B * L);
+  std::memcpy(ph + 3 * B * L, rho, sizeof(double) * B * L);
+  std::memcpy(ph + 4 * B * L, periods, sizeof(double) * T);
+  if (bounds) std::memcpy(ph + 4 * B * L + T, bounds, sizeof(double) * 2 * B);
+  cudaStream_t s = e->stream;
+  MD200_CK(cudaMemcpyAsync(e->in_h, ph, sizeof(double) * B * L, cudaMemcpyHostToDevice, s));
+  MD200_CK(cudaMemcpyAsync(e->in_vp, ph + B * L, sizeof(double) * B * L, cudaMemcpyHostToDevice, s));
+  MD200_CK(cudaMemcpyAsync(e->in_vs, ph + 2 * B * L, sizeof(double) * B * L, cudaMemcpyHostToDevice, s));
+  MD200_CK(cudaMemcpyAsync(e->in_rho, ph + 3 * B * L, sizeof(double) * B * L, cudaMemcpyHostToDevice, s));
+  MD200_CK(cudaMemcpyAsync(e->in_per, ph + 4 * B * L, sizeof(double) * T, cudaMemcpyHostToDevice, s));
+  if (bounds)
+    MD200_CK(cudaMemcpyAsync(e->in_bounds, ph + 4 * B * L + T, sizeof(double) * 2 * B,
+                             cudaMemcpyHostToDevice, s));
+  const bool grp = e->d.group != 0;
+  if (enqueue(e, e->in_h, e->in_vp, e->in_vs, e->in_rho, models, e->in_per,
+              bounds ? e->in_bounds : nullptr, tol, accept, wave, e->out_vel, e->out_flags,
+              e->out_levels, e->out_counts, grp ? e->out_grp : nullptr, grp ? e->out_gflags : nullptr,
+              prediction_flags ? e->out_pred : nullptr, e->in_bounds + 0, e->d_stats, s))
+    return 1;
+  // outputs back through pinned memory
+  double *ov = reinterpret_cast<double *>(p);
+  double *og = ov + nt * nm;
+  unsigned *ogf = reinterpret_cast<unsigned *>(og + nt * nm);
+  unsigned *ofl = ogf + nt * nm;
+  int *olv = reinterpret_cast<int *>(ofl + nt);
+  int *oct = olv + nt;
+  unsigned *opr = reinterpret_cast<unsigned *>(oct + nt);
+  unsigned long long *ost = reinterpret_cast<unsigned long long *>(
+      (reinterpret_cast<uintptr_t>(opr + nt) + 7) & ~uintptr_t(7));
+  MD200_CK(cudaMemcpyAsync(ov, e->out_vel, sizeof(double) * nt * nm, cudaMemcpyDeviceToHost, s));
+  MD200_CK(cudaMemcpyAsync(ofl, e->out_flags, sizeof(unsigned) * nt, cudaMemcpyDeviceToHost, s));
+  MD200_CK(cudaMemcpyAsync(olv, e->out_levels, sizeof(int) * nt, cudaMemcpyDeviceToHost, s));
+  MD200_CK(cudaMemcpyAsync(oct, e->out_counts, sizeof(int) * nt, cudaMemcpyDeviceToHost, s));
+  if (grp) {
+    MD200_CK(cudaMemcpyAsync(og, e->out_grp, sizeof(double) * nt * nm, cudaMemcpyDeviceToHost, s));
+    MD200_CK(cudaMemcpyAsync(ogf, e->out_gflags, sizeof(unsigned) * nt * nm, cudaMemcpyDeviceToHost, s));
+  }
+  if (prediction_flags)
+    MD200_CK(cudaMemcpyAsync(opr, e->out_pred, sizeof(unsigned) * nt, cudaMemcpyDeviceToHost, s));
+  // the prep stage wrote the windows it used over the (already consumed) input windows
+  double *obd = reinterpret_cast<double *>(ost + MD200_STAT_COUNT);
+  if (bounds_out)
+    MD200_CK(cudaMemcpyAsync(obd, e->in_bounds, sizeof(double) * 2 * B, cudaMemcpyDeviceToHost, s));
+  MD200_CK(cudaMemcpyAsync(ost, e->d_stats, sizeof(unsigned long long) * MD200_STAT_COUNT,
+                           cudaMemcpyDeviceToHost, s));
+  MD200_CK(cudaStreamSynchronize(s));
+  std::memcpy(velocity, ov, sizeof(double) * nt * nm);
+  std::memcpy(flags, ofl, sizeof(unsigned) * nt);
+  std::memcpy(levels, olv, sizeof(int) * nt);
+  std::memcpy(counts, oct, sizeof(int) * nt);
+  if (grp) {
+    std::memcpy(group, og, sizeof(double) * nt * nm);
+    std::memcpy(group_flags, ogf, sizeof(unsigned) * nt * nm);
+  }
+  if (prediction_flags) std::memcpy(prediction_flags, opr, sizeof(unsigned) * nt);
+  if (bounds_out) std::memcpy(bounds_out, obd, sizeof(double) * 2 * B);
+  if (stats && nstats > 0)
+    std::memcpy(stats, ost, sizeof(unsigned long long) * std::min(nstats, int(MD200_STAT_COUNT)));
+  return 0;
+}
+
+void md200_destroy(md200_engine *e) {
+  if (!e) return;
+  release(e);
+  delete e;
+}
+
+const char *md200_last_error(void) { return g_error.c_str(); }
+
+int md200_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+int md200_available(int device) {
+  const int n = md200_device_count();
+  if (device < 0 || device >= n) return 0;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return 0;
+  return prop.major == 10 ? 1 : 0;
+}
+
+int md200_set_device(int device) {
+  MD200_CK(cudaSetDevice(device));
+  MD200_CK(cudaFree(nullptr));
+  return 0;
+}
+
+int md200_memory_info(size_t *free_bytes, size_t *total_bytes) {
+  MD200_CK(cudaMemGetInfo(free_bytes, total_bytes));
+  return 0;
+}
+
+int md200_device_name(int device, char *name, int length) {
+  cudaDeviceProp prop;
+  MD200_CK(cudaGetDeviceProperties(&prop, device));
+  if (name && length > 0) {
+    std::snprintf(name, static_cast<size_t>(length), "%s", prop.name);
+  }
+  return 0;
+}
+
+int md200_kernel_report(int layers, int single_precision, char *json, int length) {
+  struct Entry {
+    const char *name;
+    const void *fn;
+  };
+  const Entry entries[] = {
+      {"prep_models", reinterpret_cast<const void *>(prep_models)},
+      {"scan_fp64", reinterpret_cast<const void *>(scan<double>)},
+      {"scan_fp32", reinterpret_cast<const void *>(scan<float>)},
+      {"refine", reinterpret_cast<const void *>(refine)},
+      {"assemble", reinterpret_cast<const void *>(assemble)},
+      {"group_velocity", reinterpret_cast<const void *>(group_velocity)},
+  };
+  std::string out = "{\"search_kernel\": \"" + std::string(single_precision ? "scan_fp32" : "scan_fp64") +
+                    "\", \"layers\": " + std::to_string(layers) + ", \"kernels\": {";
+  bool first = true;
+  for (const auto &en : entries) {
+    cudaFuncAttributes a;
+    if (cudaFuncGetAttributes(&a, en.fn) != cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
+    const int Ls = (layers + 3) & ~3;
+    size_t dyn = 0;
+    if (std::strncmp(en.name, "scan", 4) == 0)
+      dyn = scan_smem(4, Ls, std::strcmp(en.name, "scan_fp32") == 0 ? sizeof(float) : sizeof(double));
+    int blocks = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, en.fn, 128, dyn);
+    cudaGetLastError();
+    char buf[512];
+    std::snprintf(buf, sizeof buf,
+                  "%s\"%s\": {\"registers\": %d, \"local_bytes\": %zu, \"static_shared_bytes\": %zu, "
+                  "\"dynamic_shared_bytes\": %zu, \"max_threads\": %d, \"blocks_per_sm_at_128\": %d}",
+                  first ? "" : ", ", en.name, a.numRegs, a.localSizeBytes, a.sharedSizeBytes, dyn,
+                  a.maxThreadsPerBlock, blocks);
+    out += buf;
+    first = false;
+  }
+  out += "}}";
+  if (!json || length <= 0) return fail("modisp_b200: no output buffer");
+  std::snprintf(json, static_cast<size_t>(length), "%s", out.c_str());
+  return static_cast<int>(out.size()) < length ? 0 : fail("modisp_b200: report truncated");
+}
+
+int md200_group_roots(const double *h, const double *vp, const double *vs, const double *rho,
+                      int layers, int wave, double period, const double *roots, int known,
+                      int modes, double close_rtol, double *group, unsigned *group_flags) {
+  if (layers < 1 || layers > 256 || modes < 1 || modes > 256 || known < 0 || known > 256 ||
+      !(period > 0.))
+    return fail("modisp_b200: invalid review trace");
+  const int L = layers;
+  std::vector<double> tab(static_cast<size_t>(EVAL_ROWS) * L + known + 1, 0.);
+  for (int j = 0; j < L; ++j) {
+    const double s = vs[j];
+    tab[j] = j == L - 1 ? 0. : h[j];
+    tab[L + j] = 1. / vp[j];
+    tab[2 * L + j] = s > 0. ? 1. / s : 0.;
+    tab[3 * L + j] = s * s;
+    tab[4 * L + j] = rho[j];
+    tab[5 * L + j] = 1. / rho[j];
+    tab[6 * L + j] = s > 0. ? 1. / (rho[j] * s * s) : 0.;
+  }
+  for (int j = 0; j < known; ++j) tab[static_cast<size_t>(EVAL_ROWS) * L + j] = roots[j];
+  double *dtab = nullptr, *dgrp = nullptr;
+  unsigned *dfl = nullptr;
+  MD200_CK(cudaMalloc(&dtab, sizeof(double) * tab.size()));
+  cudaError_t err = cudaMalloc(&dgrp, sizeof(double) * modes);
+  if (err == cudaSuccess) err = cudaMalloc(&dfl, sizeof(unsigned) * modes);
+  if (err == cudaSuccess)
+    err = cudaMemcpy(dtab, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice);
+  if (err == cudaSuccess) {
+    group_roots<<<(modes + 31) / 32, 32>>>(dtab, L, vs[0] == 0. ? 1 : 0, wave, TWO_PI / period,
+                                          dtab + static_cast<size_t>(EVAL_ROWS) * L, known, modes,
+                                          close_rtol, dgrp, dfl);
+    err = cudaGetLastError();
+  }
+  if (err == cudaSuccess) err = cudaMemcpy(group, dgrp, sizeof(double) * modes, cudaMemcpyDeviceToHost);
+  if (err == cudaSuccess)
+    err = cudaMemcpy(group_flags, dfl, sizeof(unsigned) * modes, cudaMemcpyDeviceToHost);
+  cudaFree(dtab);
+  cudaFree(dgrp);
+  cudaFree(dfl);
+  if (err != cudaSuccess) return fail(std::string("modisp_b200 CUDA: ") + cudaGetErrorString(err));
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,81 @@
+// engine.cuh -- device state and constants shared by the engine kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace md200 {
+
+constexpr double TWO_PI = 6.283185307179586476925286766559;
+constexpr unsigned FULL = 0xffffffffu;
+constexpr int ROWS = 9;        // per-layer rows of the prepared table (7 used by the recurrence)
+constexpr int EVAL_ROWS = 7;   // rows staged into shared memory for the recurrence
+constexpr int SLOT = 5;        // doubles per bracket slot: lo, hi, flo, fhi, root
+constexpr long long JMAX = 1LL << 22;  // scan points per trace before the workspace flag
+
+// Trace flag bits reported to the caller (values of python/modisp/__init__.py:15-32).
+constexpr unsigned TRACE_SEARCH_UNCONVERGED = 4;
+constexpr unsigned TRACE_WORKSPACE_LIMIT = 8;
+constexpr unsigned TRACE_NEAR_CUTOFF = 16;
+constexpr unsigned TRACE_NONFINITE = 32;
+constexpr unsigned TRACE_REFINEMENT_FAILED = 64;
+constexpr unsigned TRACE_F_REJECTED = 128;
+constexpr unsigned TRACE_CLOSE_ROOT_RISK = 4096;
+constexpr unsigned TRACE_FP64_REPAIR = 32768;
+constexpr unsigned TRACE_CONTINUATION_APPROXIMATE = 65536;
+// Engine-internal bits, cleared before the flags are written out.
+constexpr unsigned INTERNAL_REPAIR = 1u << 28;
+constexpr unsigned INTERNAL_MASK = 0xF0000000u;
+
+// Group-velocity flags (python/modisp/__init__.py:46-52).
+constexpr unsigned GROUP_MISSING_ROOT = 1;
+constexpr unsigned GROUP_POLISH_FAILED = 2;
+constexpr unsigned GROUP_ILL_CONDITIONED = 8;
+constexpr unsigned GROUP_CLOSE_ROOT = 16;
+constexpr unsigned GROUP_NONFINITE = 32;
+
+// Search levels reported by this engine (the reference's ladder levels do not
+// apply): 20 FP64 scan, 21 FP32 scan with FP64 refinement, 22 FP32 scan repaired
+// by an FP64 re-scan, 23 continuation-predicted; -3 no SH guide, -4 empty window.
+constexpr int LEVEL_FP64 = 20, LEVEL_FP32 = 21, LEVEL_REPAIRED = 22, LEVEL_CONTINUATION = 23;
+
+// Device counters (int) used by the work lists.
+enum Counter {
+  C_SCAN_CURSOR = 0, C_NTRACE, C_NREFINE, C_REFINE_BEGIN, C_NGROUP, C_REPAIR_CURSOR, C_NREPAIR,
+  C_COUNT
+};
+
+struct Dev {
+  // geometry of this run
+  int B, Lmax, Ls, T, nmodes, K, KB, wave, fp32, nlog, nkmax, nsmax;
+  int n_traces, group;
+  double tol, accept, close_rtol, density;
+  // inputs (device)
+  const double *h, *vp, *vs, *rho, *periods, *bounds_in;
+  // prepared models
+  int *mL, *mwater, *mstate;
+  double *mlo, *mhi, *malpha;
+  double *layer64;  // [B][ROWS][Ls]
+  float *layer32;   // [B][ROWS][Ls]
+  double4 *knot;    // [B][nkmax]: c, N(c), ln c, kink part of N over [c_i, c_i+1]
+  int *nknot;
+  double *seed;     // [B][nsmax]
+  int *nseed;
+  // traces
+  int *nbr;
+  unsigned *tflags;
+  double *slot;     // [n_traces][KB][SLOT]
+  int *trace_list, *repair_list, *refine_list, *group_list;
+  int *ctr;
+  // outputs
+  double *vel;      // [B][nmodes][T]
+  unsigned *oflags;
+  int *olevels, *ocounts;
+  double *grp;
+  unsigned *gflags;
+  double *gwin;     // [B][nmodes][T][2]
+  double *bounds_out;  // [B][2] windows used (optional)
+  unsigned *pred;      // [B][T] prediction flags (optional)
+  unsigned long long *stats;
+};
+
+}  // namespace md200

@@ -1,0 +1,1113 @@
+// kernels.cuh -- the engine's CUDA kernels (sm_100a).
+//
+// Pipeline per run (one stream, no host synchronisation between stages):
+//   prep_models   one warp per model: drop zero-thickness padding rows, prepare
+//                 reciprocals in FP64 and FP32 tables, search window, the
+//                 phase-count knot table that shapes the scan grid, seed points
+//   init_traces   trace list (period-major: the costly short periods first)
+//   scan<T>       persistent, one warp per trace: 32 grid points per step,
+//                 secular value + shape feature in precision T, sign changes
+//                 by warp ballot, compaction into bracket slots in velocity
+//                 order; a same-sign trough of the shape feature (a possible
+//                 hidden close pair) is zoomed into by the whole warp in FP64;
+//                 sign-uncertain FP32 samples are re-evaluated in FP64
+//   refine        one thread per bracket: FP64 endpoint confirmation (FP32
+//                 scans) and FP64 Brent refinement
+//   [FP32 only] collect_repairs + scan<double>/refine on the traces whose
+//                 FP32 brackets FP64 did not confirm
+//   assemble      one thread per trace: order, cap and write the roots, flags,
+//                 counts and group-velocity windows
+//   group         one thread per root: FP64 group velocity from forward-mode
+//                 derivatives dF/dk and dF/domega of the secular function
+#pragma once
+#include "engine.cuh"
+#include "secular.cuh"
+
+namespace md200 {
+
+// ---------------------------------------------------------------------------
+// helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned lanemask_lt() {
+  unsigned m;
+  asm volatile("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// 16-byte asynchronous global->shared copy (Ampere+ cp.async, bypassing L1).
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::);
+}
+
+template <class T>
+__device__ __forceinline__ const T *layer_table(const Dev &d, int b);
+template <>
+__device__ __forceinline__ const double *layer_table<double>(const Dev &d, int b) {
+  return d.layer64 + static_cast<size_t>(b) * ROWS * d.Ls;
+}
+template <>
+__device__ __forceinline__ const float *layer_table<float>(const Dev &d, int b) {
+  return d.layer32 + static_cast<size_t>(b) * ROWS * d.Ls;
+}
+
+template <class T>
+__device__ __forceinline__ LayerView<T> make_view(const T *tab, int Ls, int L, int water) {
+  LayerView<T> v;
+  v.h = tab;
+  v.ivp = tab + Ls;
+  v.ivs = tab + 2 * Ls;
+  v.vs2 = tab + 3 * Ls;
+  v.rho = tab + 4 * Ls;
+  v.irho = tab + 5 * Ls;
+  v.imu = tab + 6 * Ls;
+  v.L = L;
+  v.water = water;
+  return v;
+}
+
+// Layer recurrence steps of one evaluation.
+__device__ __forceinline__ int layer_steps(int L, int water) { return L - 1 - water; }
+
+// FP64 secular value (and shape feature) from a global-memory table.
+__device__ __forceinline__ double eval64(const LayerView<double> &m, int wave, double w, double c,
+                                         double *g) {
+  return secular<double, double>(m, wave, w / c, w, g);
+}
+
+// Out-of-line FP64 evaluation for the rare FP64 re-evaluations inside the FP32
+// scan, so their registers do not weigh on the single-precision loop.
+__device__ __noinline__ double eval64_outline(const LayerView<double> &m, int wave, double w, double c,
+                                              double *g, double *lm) {
+  return secular<double, double>(m, wave, w / c, w, g, lm);
+}
+
+// Rayleigh-wave speed of a homogeneous half-space by bisection of the
+// Rayleigh cubic (cpp/common/physics.hpp:140-144).
+__device__ double rayleigh_speed(double vp, double vs) {
+  const double ratio = (vs / vp) * (vs / vp);
+  double l = 0., h = 1.;
+  for (int j = 0; j < 56; ++j) {
+    const double x = (l + h) * .5;
+    const double f = ((x - 8.) * x + 24. - 16. * ratio) * x - 16. * (1. - ratio);
+    if (f < 0.) l = x; else h = x;
+  }
+  return vs * sqrt((l + h) * .5);
+}
+
+// Scholte-wave speed of a fluid over a solid half-space by bisection
+// (cpp/common/physics.hpp:146-156).
+__device__ double scholte_speed(double vf, double rf, double vp, double vs, double rs) {
+  const double ratio = (vs / vp) * (vs / vp), qf = (vs / vf) * (vs / vf);
+  double l = 0., h = fmax(0., fmin(1., vf / vs) * (1. - 1e-12));
+  for (int j = 0; j < 64; ++j) {
+    const double x = (l + h) * .5, x2 = x * x;
+    const double A = sqrt(fmax(0., 1. - ratio * x2)), B = sqrt(fmax(0., 1. - x2));
+    const double f = 4. * (1. + ratio - ratio * x2) / (1. + A * B) - 4. + x2 +
+                     (rf / rs) * x2 * A / sqrt(fmax(1e-30, 1. - qf * x2));
+    if (f < 0.) l = x; else h = x;
+  }
+  return vs * (l + h) * .5;
+}
+
+// Warp-cooperative bitonic sort of n2 (a power of two) keys with int payloads.
+__device__ void warp_bitonic(double *key, int *val, int n2, int lane) {
+  for (int size = 2; size <= n2; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int i = lane; i < (n2 >> 1); i += 32) {
+        const int lo = 2 * i - (i & (stride - 1));
+        const int hi = lo + stride;
+        const bool up = (lo & size) == 0;
+        const double a = key[lo], b = key[hi];
+        if ((a > b) == up) {
+          key[lo] = b;
+          key[hi] = a;
+          const int t = val[lo];
+          val[lo] = val[hi];
+          val[hi] = t;
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
+__device__ __forceinline__ int pow2_ceil(int n) {
+  int p = 1;
+  while (p < n) p <<= 1;
+  return p;
+}
+
+// Phase-count density N(c) = 2 sum_j h_j sqrt(1/v_j^2 - 1/c^2) over the finite
+// layers, S waves (and P waves for Rayleigh) (cpp/common/physics.hpp:130-138).
+__device__ double phase_count(const double *tab, int Ls, int L, int wave, double c) {
+  const double ic = 1. / (c * c);
+  double n = 0.;
+  for (int j = 0; j < L - 1; ++j) {
+    const double h = tab[j];
+    if (h == 0.) continue;
+    const double ivs = tab[2 * Ls + j], ivp = tab[Ls + j];
+    const double zs = ivs * ivs - ic;
+    if (zs > 0.) n += h * sqrt(zs);
+    if (!wave) {
+      const double zp = ivp * ivp - ic;
+      if (zp > 0.) n += h * sqrt(zp);
+    }
+  }
+  return 2. * n;
+}
+
+// ---------------------------------------------------------------------------
+// prep_models: one warp per model.
+// Shared memory per warp: 2 * sortcap doubles + 2 * sortcap ints.
+// ---------------------------------------------------------------------------
+__global__ void prep_models(Dev d, int sortcap, int automatic) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int b = blockIdx.x * (blockDim.x >> 5) + wib;
+  if (b >= d.B) return;
+  double *skey = reinterpret_cast<double *>(smem_raw) + static_cast<size_t>(wib) * sortcap;
+  int *sval = reinterpret_cast<int *>(reinterpret_cast<double *>(smem_raw) +
+                                      static_cast<size_t>(blockDim.x >> 5) * sortcap) +
+              static_cast<size_t>(wib) * sortcap;
+  const int Lmax = d.Lmax, Ls = d.Ls;
+  const size_t in = static_cast<size_t>(b) * Lmax;
+  double *t64 = d.layer64 + static_cast<size_t>(b) * ROWS * Ls;
+  float *t32 = d.layer32 + static_cast<size_t>(b) * ROWS * Ls;
+
+  // 1. keep row 0, the half-space and every layer of positive thickness; a
+  //    zero-thickness layer is an identity step of the recurrence.
+  int L = 0;
+  for (int base = 0; base < Lmax; base += 32) {
+    const int j = base + lane;
+    bool keep = false;
+    double hj = 0., vpj = 1., vsj = 0., rj = 1.;
+    if (j < Lmax) {
+      hj = d.h[in + j];
+      vpj = d.vp[in + j];
+      vsj = d.vs[in + j];
+      rj = d.rho[in + j];
+      keep = j == 0 || j == Lmax - 1 || hj > 0.;
+    }
+    const unsigned mask = __ballot_sync(FULL, keep);
+    if (keep) {
+      const int r = L + __popc(mask & lanemask_lt());
+      const double ivp = 1. / vpj, ivs = vsj > 0. ? 1. / vsj : 0.;
+      const double vals[ROWS] = {j == Lmax - 1 ? 0. : hj, ivp, ivs, vsj * vsj, rj, 1. / rj,
+                                 vsj > 0. ? 1. / (rj * vsj * vsj) : 0., vpj, vsj};
+#pragma unroll
+      for (int q = 0; q < ROWS; ++q) {
+        t64[q * Ls + r] = vals[q];
+        t32[q * Ls + r] = static_cast<float>(vals[q]);
+      }
+    }
+    L += __popc(mask);
+  }
+  __syncwarp();
+  const double *vpr = t64 + 7 * Ls, *vsr = t64 + 8 * Ls, *hr = t64, *rr = t64 + 4 * Ls;
+  const int water = vsr[0] == 0. ? 1 : 0;
+  const int top = water;
+  const int wave = d.wave;
+
+  // 2. search window (cpp/cpu/solver.cpp:781-790, cpp/common/physics.hpp:158-175).
+  //    A given window is used as is, except that a non-positive lower bound asks
+  //    for the automatic one and the upper bound never exceeds the half-space
+  //    shear velocity (exclusive).
+  double lo = d.bounds_in ? d.bounds_in[2 * b] : 0.;
+  double hi = d.bounds_in ? d.bounds_in[2 * b + 1] : INFINITY;
+  if (automatic || !(lo > 0.)) {
+    double best = 1e300;
+    for (int j = top + lane; j < L; j += 32) {
+      if (hr[j] == 0. && j < L - 1) continue;  // a zero-thickness row carries no waves
+      const double s = vsr[j], p = vpr[j];
+      double x = wave ? s : rayleigh_speed(p, s);
+      if (!wave && top) x = fmin(x, scholte_speed(vpr[0], rr[0], p, s, rr[j]));
+      best = fmin(best, x);
+    }
+    for (int o = 16; o; o >>= 1) best = fmin(best, __shfl_xor_sync(FULL, best, o));
+    lo = .125 * best;
+  }
+  hi = fmin(hi, nextafter(vsr[L - 1], 0.));
+  int state = hi > lo ? 0 : -4;
+  if (state == 0 && wave) {  // SH guide: a finite layer slower than the half-space
+    bool guide = false;
+    for (int j = top + lane; j < L - 1; j += 32) guide |= hr[j] > 0. && vsr[j] < vsr[L - 1];
+    if (!__any_sync(FULL, guide)) state = -3;
+  }
+  if (lane == 0) {
+    d.mL[b] = L;
+    d.mwater[b] = water;
+    d.mstate[b] = state;
+    d.mlo[b] = lo;
+    d.mhi[b] = hi;
+    if (d.bounds_out) {
+      d.bounds_out[2 * b] = lo;
+      d.bounds_out[2 * b + 1] = hi;
+    }
+  }
+  if (state) return;
+
+  // 3. knot table: log-spaced points over [lo, hi] plus every finite-layer body
+  //    velocity inside the window (kinks of N(c)), sorted.
+  const int nlog = d.nlog;
+  const double lspan = log(hi / lo);
+  int n = 0;
+  for (int i = lane; i <= nlog; i += 32) {
+    skey[i] = i == 0 ? lo : (i == nlog ? hi : lo * exp(lspan * i / nlog));
+    sval[i] = 0;
+  }
+  n = nlog + 1;
+  for (int base = top; base < L - 1; base += 32) {
+    const int j = base + lane;
+    bool ks = false, kp = false;
+    double s = 0., p = 0.;
+    if (j < L - 1 && hr[j] > 0.) {
+      s = vsr[j];
+      p = vpr[j];
+      ks = s > lo && s < hi;
+      kp = !wave && p > lo && p < hi;
+    }
+    const unsigned ms = __ballot_sync(FULL, ks), mp = __ballot_sync(FULL, kp);
+    if (ks) {
+      const int r = n + __popc(ms & lanemask_lt());
+      skey[r] = s;
+      sval[r] = 1;
+    }
+    n += __popc(ms);
+    if (kp) {
+      const int r = n + __popc(mp & lanemask_lt());
+      skey[r] = p;
+      sval[r] = 1;
+    }
+    n += __popc(mp);
+  }
+  int n2 = pow2_ceil(n);
+  for (int i = n + lane; i < n2; i += 32) {
+    skey[i] = INFINITY;
+    sval[i] = 0;
+  }
+  __syncwarp();
+  warp_bitonic(skey, sval, n2, lane);
+  // Keep the last element of each run of equal keys, merging kink marks.
+  int nk = 0;
+  double4 *kt = d.knot + static_cast<size_t>(b) * d.nkmax;
+  for (int base = 0; base < n; base += 32) {
+    const int i = base + lane;
+    bool keep = false;
+    double c = 0.;
+    int kink = 0;
+    if (i < n) {
+      c = skey[i];
+      keep = i + 1 >= n || skey[i + 1] != c;
+      kink = sval[i] | (i > 0 && skey[i - 1] == c ? sval[i - 1] : 0);
+    }
+    const unsigned mask = __ballot_sync(FULL, keep);
+    if (keep) {
+      const int r = nk + __popc(mask & lanemask_lt());
+      kt[r] = make_double4(c, 0., log(c), kink ? 1. : 0.);
+    }
+    nk += __popc(mask);
+  }
+  __syncwarp();
+  // N(c) at each knot, and the kink term of the interval starting at a kink.
+  for (int i = lane; i < nk; i += 32) {
+    double4 q = kt[i];
+    q.y = phase_count(t64, Ls, L, wave, q.x);
+    double kink = 0.;
+    if (q.w != 0. && i + 1 < nk) {
+      const double c1 = kt[i + 1].x, ic1 = 1. / (c1 * c1);
+      for (int j = top; j < L - 1; ++j) {
+        if (hr[j] == 0.) continue;
+        if (vsr[j] == q.x) kink += hr[j] * sqrt(fmax(0., 1. / (vsr[j] * vsr[j]) - ic1));
+        if (!wave && vpr[j] == q.x) kink += hr[j] * sqrt(fmax(0., 1. / (vpr[j] * vpr[j]) - ic1));
+      }
+    }
+    q.w = 2. * kink;
+    kt[i] = q;
+  }
+  __syncwarp();
+  if (lane == 0) {
+    d.nknot[b] = nk;
+    // log weight: background spacing ln(hi/lo)/log_points in ln c per scan step
+    d.malpha[b] = static_cast<double>(nlog) / (d.density * lspan);
+  }
+
+  // 4. seed points: the window ends, every body velocity and its +-1e-7 neighbours,
+  //    the top-layer Rayleigh/Love and Scholte speeds with nearby offsets
+  //    (the sampling seeds of cpp/cpu/solver.cpp:482-495).
+  __syncwarp();
+  n = 0;
+  const int seed_top = wave && water ? 1 : 0;
+  for (int base = seed_top; base < L; base += 32) {
+    const int j = base + lane;
+    double v[6];
+    int cnt = 0;
+    if (j < L) {
+      const double vv[2] = {vpr[j], vsr[j]};
+      for (int q = 0; q < 2; ++q)
+        for (int side = -1; side <= 1; ++side) {
+          const double c = vv[q] * (1. + side * 1e-7);
+          if (c > lo && c < hi) v[cnt++] = c;
+        }
+    }
+    int off = cnt;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(FULL, off, o);
+      if (lane >= o) off += y;
+    }
+    const int total = __shfl_sync(FULL, off, 31);
+    off -= cnt;
+    for (int q = 0; q < cnt; ++q) {
+      skey[n + off + q] = v[q];
+      sval[n + off + q] = 0;
+    }
+    n += total;
+  }
+  __syncwarp();
+  if (lane == 0) {
+    const double s0 = wave ? vsr[top] : rayleigh_speed(vpr[top], vsr[top]);
+    const double ws = (!wave && top) ? scholte_speed(vpr[0], rr[0], vpr[1], vsr[1], rr[1]) : NAN;
+    const double gaps[5] = {1e-7, 1e-6, 1e-5, 1e-4, 1e-3};
+    const double base[2] = {s0, ws};
+    skey[n++] = lo;
+    skey[n++] = hi;
+    for (int q = 0; q < 2; ++q) {
+      const double s = base[q];
+      const double cands[2] = {s, .9 * s};
+      for (int r = 0; r < 2; ++r)
+        if (cands[r] > lo && cands[r] < hi) skey[n++] = cands[r];
+      for (int g = 0; g < 5; ++g) {
+        const double a = s * (1. - gaps[g]), c = s * (1. + gaps[g]);
+        if (a > lo && a < hi) skey[n++] = a;
+        if (c > lo && c < hi) skey[n++] = c;
+      }
+    }
+  }
+  n = __shfl_sync(FULL, n, 0);
+  __syncwarp();
+  n2 = pow2_ceil(n);
+  for (int i = n + lane; i < n2; i += 32) skey[i] = INFINITY;
+  for (int i = lane; i < n2; i += 32) sval[i] = 0;
+  __syncwarp();
+  warp_bitonic(skey, sval, n2, lane);
+  int ns = 0;
+  double *sd = d.seed + static_cast<size_t>(b) * d.nsmax;
+  for (int base = 0; base < n; base += 32) {
+    const int i = base + lane;
+    const bool keep = i < n && (i == 0 || skey[i - 1] != skey[i]);
+    const unsigned mask = __ballot_sync(FULL, keep);
+    if (keep) sd[ns + __popc(mask & lanemask_lt())] = skey[i];
+    ns += __popc(mask);
+  }
+  if (lane == 0) d.nseed[b] = ns;
+}
+
+// ---------------------------------------------------------------------------
+// init_traces: the round-0 trace list (period-major) and per-trace resets.
+// ---------------------------------------------------------------------------
+__global__ void init_traces(Dev d) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= d.n_traces) return;
+  const int b = q % d.B, f = q / d.B;
+  const int t = b * d.T + f;
+  d.nbr[t] = 0;
+  d.tflags[t] = 0;
+  if (d.pred) d.pred[t] = 8u;  // searched independently (PredictionFlag.BYPASSED)
+  if (d.mstate[b] == 0) {
+    const int pos = atomicAdd(&d.ctr[C_NTRACE], 1);
+    d.trace_list[pos] = t;
+  }
+}
+
+// Position of scan point j (1 <= j <= J) of a trace: invert
+// u(c) = f N(c) + alpha ln c at u_lo + j / density through the knot table.  In
+// an interval that starts at a body velocity the kink term grows like
+// sqrt(c - c_i); the local model u = u_i + a sqrt(s) + b s (s the fractional
+// position) is inverted exactly.
+__device__ __forceinline__ double scan_point(const double4 *kt, int nk, double f, double alpha,
+                                             double target) {
+  int lo = 0, hi = nk - 1;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    const double4 q = kt[mid];
+    if (fma(f, q.y, alpha * q.z) <= target) lo = mid; else hi = mid;
+  }
+  const double4 q0 = kt[lo], q1 = kt[hi];
+  const double u0 = fma(f, q0.y, alpha * q0.z), u1 = fma(f, q1.y, alpha * q1.z);
+  const double dt = fmax(0., target - u0), du = u1 - u0;
+  const double a = f * q0.w, bs = fmax(0., du - a);
+  double s = 0.;
+  if (du > 0. && dt > 0.) {  // (dt = 0 would give 0/0 where the interval has no kink)
+    const double x = 2. * dt / (a + sqrt(a * a + 4. * bs * dt));
+    s = fmin(1., x * x);
+  }
+  return fma(q1.x - q0.x, s, q0.x);
+}
+
+// Index (0..32) of the first lane whose sorted value is >= x (or > x when
+// `inclusive`), over the warp's ascending per-lane values `v`.
+__device__ __forceinline__ int warp_rank(double v, double x, bool inclusive) {
+  int lo = 0, hi = 32;
+#pragma unroll
+  for (int it = 0; it < 6; ++it) {
+    const int mid = (lo + hi) >> 1;
+    const double m = __shfl_sync(FULL, v, mid & 31);
+    const bool less = inclusive ? (m <= x) : (m < x);
+    if (lo < hi) {
+      if (less) lo = mid + 1; else hi = mid;
+    }
+  }
+  return lo;
+}
+
+// Global-memory FP64 view of model b.
+__device__ __forceinline__ LayerView<double> global_view(const Dev &d, int b) {
+  return make_view<double>(layer_table<double>(d, b), d.Ls, d.mL[b], d.mwater[b]);
+}
+
+// Append one bracket to slot r of a trace (flo/fhi NaN: unknown in FP64).
+__device__ __forceinline__ void put_bracket(double *slot, int r, double lo, double hi, double flo,
+                                            double fhi) {
+  double *s = slot + static_cast<size_t>(r) * SLOT;
+  s[0] = lo;
+  s[1] = hi;
+  s[2] = flo;
+  s[3] = fhi;
+  s[4] = NAN;
+}
+
+// Could a same-sign local minimum (v at x1, neighbours u at x0 and z at x2, all
+// of one sign, s*g > 0) hide a root pair?  Close pairs show up in the shape
+// feature as a V whose flanks are nearly linear and whose bottom dips through
+// zero between samples; a smooth minimum well above zero does not.  The trough
+// is kept when a V with its vertex on zero fits the samples -- the linear
+// extension of either flank reaches zero before the far neighbour -- or when a
+// parabola through the three samples dips to zero.
+__device__ __forceinline__ bool trough_may_hide_roots(double x0, double x1, double x2, double u, double v,
+                                                      double z) {
+  if (!(v < u && v < z) || !(x0 < x1 && x1 < x2)) return false;
+  const double sl = (u - v) / (x1 - x0), sr = (z - v) / (x2 - x1);  // flank steepness (> 0)
+  if (x1 + v / sl < x2 + .25 * (x2 - x1) || x1 - v / sr > x0 - .25 * (x1 - x0)) return true;
+  const double d1 = -sl, d2 = sr, a2 = (d2 - d1) / (x2 - x0);
+  if (a2 > 0.) {
+    const double xs = .5 * (x0 + x1) - d1 / (2. * a2);
+    if (u + d1 * (xs - x0) + a2 * (xs - x0) * (xs - x1) <= 0.) return true;
+  }
+  return false;
+}
+
+// Depth (base-2 log units) of the middle sample's log-magnitude below the chord
+// of its neighbours: large where the whole unnormalised vector nearly vanishes,
+// which hides a root pair even where the shape feature stays smooth.
+constexpr double MDIP = 0.5;
+__device__ __forceinline__ double magnitude_dip(double x0, double x1, double x2, double m0, double m1,
+                                                double m2) {
+  if (!(x0 < x1 && x1 < x2) || !(m1 < m0 && m1 < m2)) return 0.;
+  const double t = (x1 - x0) / (x2 - x0);
+  return m0 + t * (m2 - m0) - m1;
+}
+
+// Warp-cooperative FP64 zoom into a same-sign trough of the shape feature:
+// 32 points inside (a, b) per step; a sign change among them yields brackets
+// (appended in order, FP64 values known); otherwise the window shrinks 16.5x
+// around the smallest s*g until the minimum is resolved above zero or the
+// window reaches the refinement width.  `sa`, `sb` are s*g at a and b.
+__device__ __noinline__ int zoom_trough(const LayerView<double> &m, int wave, double w, double a, double b,
+                                       double sa, double sb, double ma, double mb, double sgn, int mode,
+                                       double tol, double *slot, int nbr, int K, int lane,
+                                       unsigned long long &evals) {
+  const bool neg = sgn < 0.;
+  double Fa = NAN, Fb = NAN;  // FP64 values of the window ends once they are zoom points
+  for (int it = 0; it < 10; ++it) {
+    const double width = b - a;
+    if (!(width > fmax(4e-15 * b, .125 * tol * b))) break;
+    const double x = a + width * (lane + 1) * (1. / 33.);
+    double g, lm;
+    const double F = secular<double, double>(m, wave, w / x, w, &g, &lm);
+    evals += 32;
+    const bool opp = signbit(F) != neg;
+    const unsigned om = __ballot_sync(FULL, opp);
+    if (om) {
+      // brackets between consecutive points of a, x_0..x_31, b (a and b have sign sgn)
+      const double xl = __shfl_up_sync(FULL, x, 1), Fl = __shfl_up_sync(FULL, F, 1);
+      const bool opl = lane ? ((om >> (lane - 1)) & 1) != 0 : false;
+      const bool left = opp != opl;                    // change between element lane-1 (or a) and lane
+      const bool right = lane == 31 && opp;            // change between x_31 and b
+      const unsigned lm_ = __ballot_sync(FULL, left), rm = __ballot_sync(FULL, right);
+      if (left) {
+        const int r = nbr + __popc(lm_ & lanemask_lt());
+        if (r < K) put_bracket(slot, r, lane ? xl : a, x, lane ? Fl : Fa, F);
+      }
+      nbr += __popc(lm_);
+      if (right) {
+        if (nbr < K) put_bracket(slot, nbr, x, b, F, Fb);
+      }
+      nbr += __popc(rm);
+      return nbr < K ? nbr : K;
+    }
+    // no sign change: zoom on the lowest s*g (mode 0) or log-magnitude (mode 1)
+    const double v = sgn * g;
+    const double key = mode ? lm : v;
+    double best = key;
+    int arg = lane;
+    for (int o = 16; o; o >>= 1) {
+      const double ob = __shfl_xor_sync(FULL, best, o);
+      const int oa = __shfl_xor_sync(FULL, arg, o);
+      if (ob < best || (ob == best && oa < arg)) { best = ob; arg = oa; }
+    }
+    const int il = (arg - 1) & 31, ir = (arg + 1) & 31;
+    const double vl = arg ? __shfl_sync(FULL, v, il) : sa;
+    const double vr = arg < 31 ? __shfl_sync(FULL, v, ir) : sb;
+    const double ml = arg ? __shfl_sync(FULL, lm, il) : ma;
+    const double mr = arg < 31 ? __shfl_sync(FULL, lm, ir) : mb;
+    const double xlo = arg ? __shfl_sync(FULL, x, il) : a;
+    const double xhi = arg < 31 ? __shfl_sync(FULL, x, ir) : b;
+    const double Flo = arg ? __shfl_sync(FULL, F, il) : Fa;
+    const double Fhi = arg < 31 ? __shfl_sync(FULL, F, ir) : Fb;
+    const double xm = __shfl_sync(FULL, x, arg);
+    // stop once the lowest sample and its neighbours no longer admit a hidden pair
+    const bool go = mode ? magnitude_dip(xlo, xm, xhi, ml, __shfl_sync(FULL, lm, arg), mr) > MDIP
+                         : trough_may_hide_roots(xlo, xm, xhi, vl, __shfl_sync(FULL, v, arg), vr);
+    if (!go) break;
+    a = xlo; b = xhi; sa = vl; sb = vr; ma = ml; mb = mr; Fa = Flo; Fb = Fhi;
+  }
+  return nbr;
+}
+
+// ---------------------------------------------------------------------------
+// scan<T>: persistent, one warp per trace.
+// Shared memory per warp: EVAL_ROWS * Ls values of T (model table) + 32 doubles
+// (merge buffer).
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(128) scan(Dev d, const int *list, int cursor_id, int count_id) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const size_t tab_bytes = (static_cast<size_t>(EVAL_ROWS) * d.Ls * sizeof(T) + 15) & ~size_t(15);
+  unsigned char *mine = smem_raw + static_cast<size_t>(wib) * (tab_bytes + 32 * sizeof(double));
+  T *tab = reinterpret_cast<T *>(mine);
+  double *mbuf = reinterpret_cast<double *>(mine + tab_bytes);
+  unsigned long long evals = 0, evals32 = 0, steps = 0, steps32 = 0, brackets = 0, zooms = 0;
+  const int K = d.K, wave = d.wave;
+  const double density = d.density, step = 1. / density;
+  constexpr bool single = sizeof(T) == 4;
+
+  for (;;) {
+    int q = 0;
+    if (lane == 0) q = atomicAdd(&d.ctr[cursor_id], 1);
+    q = __shfl_sync(FULL, q, 0);
+    if (q >= *(volatile int *)&d.ctr[count_id]) break;
+    const int t = list[q];
+    const int b = t / d.T, f = t - b * d.T;
+    const double period = d.periods[f];
+    const double w = TWO_PI / period, fr = 1. / period;
+    const int L = d.mL[b], water = d.mwater[b];
+    // stage the model's recurrence rows (16-byte cp.async, coalesced)
+    {
+      const T *src = layer_table<T>(d, b);
+      const int n16 = static_cast<int>((static_cast<size_t>(EVAL_ROWS) * d.Ls * sizeof(T)) / 16);
+      for (int i = lane; i < n16; i += 32)
+        cp_async16(reinterpret_cast<unsigned char *>(tab) + 16 * i,
+                   reinterpret_cast<const unsigned char *>(src) + 16 * i);
+      cp_async_wait_all();
+      __syncwarp();
+    }
+    const LayerView<T> view = make_view<T>(tab, d.Ls, L, water);
+    // FP64 view for zooms and uncertain FP32 samples: shared memory in the FP64
+    // kernel, global memory (L1/L2-resident) in the FP32 kernel
+    LayerView<double> view64;
+    if constexpr (single) view64 = global_view(d, b);
+    else view64 = *reinterpret_cast<const LayerView<double> *>(&view);
+    const int nsteps = layer_steps(L, water);
+    const double4 *kt = d.knot + static_cast<size_t>(b) * d.nkmax;
+    const int nk = d.nknot[b];
+    const double alpha = d.malpha[b];
+    const double u_lo = fma(fr, kt[0].y, alpha * kt[0].z);
+    const double u_hi = fma(fr, kt[nk - 1].y, alpha * kt[nk - 1].z);
+    long long J = static_cast<long long>(ceil((u_hi - u_lo) * density)) - 1;
+    unsigned tfl = 0;
+    if (J < 0) J = 0;
+    if (J > JMAX) {
+      J = JMAX;
+      tfl |= TRACE_WORKSPACE_LIMIT;
+    }
+    const double *sd = d.seed + static_cast<size_t>(b) * d.nsmax;
+    const int ns = d.nseed[b];
+    const double hi = d.mhi[b];
+    double *slot = d.slot + static_cast<size_t>(t) * d.KB * SLOT;
+
+    long long gi = 1;
+    int si = 0, nbr = 0;
+    bool have1 = false, have2 = false;
+    double zoom_right = -INFINITY;  // right end of the last zoomed window (windows never overlap)
+    double c1 = 0., F1 = 0., g1 = 0., M1 = 0., c2 = 0., g2 = 0., F2 = 0., M2 = 0.;  // elements -1, -2
+    while (nbr < K) {
+      // ---- next 32 sample positions: merge scan points and seeds ----
+      const long long gj = gi + lane;
+      const double gv = gj <= J ? scan_point(kt, nk, fr, alpha, u_lo + static_cast<double>(gj) * step)
+                                : INFINITY;
+      const double sv = si + lane < ns ? sd[si + lane] : INFINITY;
+      const int rg = warp_rank(sv, gv, false);  // seeds strictly below this scan point
+      const int rs = warp_rank(gv, sv, true);   // scan points at or below this seed
+      const int pg = lane + rg, ps = lane + rs;
+      mbuf[lane] = INFINITY;
+      __syncwarp();
+      if (pg < 32) mbuf[pg] = gv;
+      if (ps < 32) mbuf[ps] = sv;
+      __syncwarp();
+      double c = mbuf[lane];
+      __syncwarp();
+      gi += __popc(__ballot_sync(FULL, pg < 32 && gv < INFINITY));
+      si += __popc(__ballot_sync(FULL, ps < 32 && sv < INFINITY));
+      const bool valid = c < INFINITY;
+      const unsigned vmask = __ballot_sync(FULL, valid);
+      if (!vmask) break;
+      const int nvalid = __popc(vmask);
+
+      // ---- secular value, shape feature and log-magnitude ----
+      double F = 0., g = 0., M = 0.;
+      bool exact = !single;  // value known in FP64
+      // near the half-space cutoff the start vector depends on the small radical
+      // sqrt(k^2 - kb^2) directly, which single precision resolves poorly: those
+      // samples are evaluated in FP64 only, at their exact positions
+      const bool near_cut = single && valid && c >= hi * (1. - 2e-3);
+      if (valid) {
+        if constexpr (single) {
+          float c32 = static_cast<float>(c);
+          if (static_cast<double>(c32) > hi) c32 = nextafterf(c32, 0.f);
+          if (!near_cut) c = static_cast<double>(c32);
+          float gg, mm;
+          const float w32 = static_cast<float>(w);
+          F = secular<float, float>(view, wave, w32 / c32, w32, &gg, &mm);
+          g = gg;
+          M = mm;
+        } else {
+          F = secular<double, double>(view, wave, w / c, w, &g, &M);
+        }
+      }
+      evals += nvalid;
+      steps += static_cast<unsigned long long>(nvalid) * nsteps;
+      if constexpr (single) {
+        evals32 += nvalid;
+        steps32 += static_cast<unsigned long long>(nvalid) * nsteps;
+        // sign-uncertain single-precision samples (small |g|) and the near-cutoff
+        // band are evaluated in FP64
+        const bool redo = valid && (!(fabs(g) > 2e-4) || near_cut);
+        const unsigned rm = __ballot_sync(FULL, redo);
+        if (rm) {
+          if (redo) {
+            F = eval64_outline(view64, wave, w, c, &g, &M);
+            exact = true;
+          }
+          evals += __popc(rm);
+          steps += static_cast<unsigned long long>(__popc(rm)) * nsteps;
+        }
+      }
+      if (__any_sync(FULL, valid && !(isfinite(F) && isfinite(g)))) {
+        tfl |= TRACE_NONFINITE | TRACE_SEARCH_UNCONVERGED;
+        break;
+      }
+      // ---- neighbours (elements i-1 and i-2) ----
+      double cl = __shfl_up_sync(FULL, c, 1), Fl = __shfl_up_sync(FULL, F, 1),
+             gl = __shfl_up_sync(FULL, g, 1);
+      double cll = __shfl_up_sync(FULL, c, 2), Fll = __shfl_up_sync(FULL, F, 2),
+             gll = __shfl_up_sync(FULL, g, 2);
+      double Ml = __shfl_up_sync(FULL, M, 1), Mll = __shfl_up_sync(FULL, M, 2);
+      bool exl = __shfl_up_sync(FULL, exact, 1);
+      const bool vl = lane >= 1 ? lane - 1 < nvalid : have1;
+      const bool vll = lane >= 2 ? lane - 2 < nvalid : (lane == 1 ? have1 : have2);
+      if (lane == 0) {
+        cl = c1; Fl = F1; gl = g1; Ml = M1;
+        cll = c2; Fll = F2; gll = g2; Mll = M2;
+        exl = false;
+      } else if (lane == 1) {
+        cll = c1; Fll = F1; gll = g1; Mll = M1;
+      }
+      // ---- events: sign changes (a +0 counts as positive) and same-sign troughs ----
+      const bool sc = valid && vl && (signbit(Fl) != signbit(F));
+      bool tr = false, trm_ = false;
+      if (valid && vl && vll && signbit(Fll) == signbit(Fl) && signbit(Fl) == signbit(F)) {
+        const double sgn = signbit(Fl) ? -1. : 1.;
+        tr = trough_may_hide_roots(cll, cl, c, sgn * gll, sgn * gl, sgn * g);
+        if (!tr) trm_ = magnitude_dip(cll, cl, c, Mll, Ml, M) > MDIP;
+        tr = tr || trm_;
+      }
+      const unsigned scm = __ballot_sync(FULL, sc), trm = __ballot_sync(FULL, tr);
+      const unsigned mmode = __ballot_sync(FULL, trm_);
+      unsigned events = scm | trm;
+      while (events && nbr < K) {
+        const int i = __ffs(events) - 1;
+        events &= events - 1;
+        if ((scm >> i) & 1u) {
+          if (lane == i) put_bracket(slot, nbr, cl, c, exl ? Fl : NAN, exact ? F : NAN);
+          ++nbr;
+          ++brackets;
+        } else {
+          double x0 = __shfl_sync(FULL, cll, i);
+          const double x2 = __shfl_sync(FULL, c, i);
+          const double sgn = signbit(__shfl_sync(FULL, Fl, i)) ? -1. : 1.;
+          double sa = sgn * __shfl_sync(FULL, gll, i);
+          const double sb = sgn * __shfl_sync(FULL, g, i);
+          double ma = __shfl_sync(FULL, Mll, i);
+          const double mb = __shfl_sync(FULL, M, i);
+          if (x0 < zoom_right) {  // overlaps the previous window: start at its middle sample
+            x0 = __shfl_sync(FULL, cl, i);
+            sa = sgn * __shfl_sync(FULL, gl, i);
+            ma = __shfl_sync(FULL, Ml, i);
+          }
+          zoom_right = x2;
+          unsigned long long ze = 0;
+          const int before = nbr;
+          nbr = zoom_trough(view64, wave, w, x0, x2, sa, sb, ma, mb, sgn, (mmode >> i) & 1u, d.tol, slot,
+                            nbr, K, lane, ze);
+          brackets += nbr - before;
+          evals += ze;
+          steps += ze * nsteps;
+          ++zooms;
+        }
+      }
+      // ---- carry the last two elements ----
+      const int last = nvalid - 1;
+      const double nc1 = __shfl_sync(FULL, c, last), nF1 = __shfl_sync(FULL, F, last),
+                   ng1 = __shfl_sync(FULL, g, last), nM1 = __shfl_sync(FULL, M, last);
+      if (nvalid >= 2) {
+        c2 = __shfl_sync(FULL, c, last - 1);
+        F2 = __shfl_sync(FULL, F, last - 1);
+        g2 = __shfl_sync(FULL, g, last - 1);
+        M2 = __shfl_sync(FULL, M, last - 1);
+        have2 = true;
+      } else {
+        c2 = c1; F2 = F1; g2 = g1; M2 = M1;
+        have2 = have1;
+      }
+      c1 = nc1; F1 = nF1; g1 = ng1; M1 = nM1;
+      have1 = true;
+    }
+    // ---- publish brackets ----
+    if (lane == 0) {
+      d.nbr[t] = nbr;
+      if (tfl) atomicOr(&d.tflags[t], tfl);
+    }
+    if (!(tfl & TRACE_SEARCH_UNCONVERGED)) {
+      int base = 0;
+      if (lane == 0) base = atomicAdd(&d.ctr[C_NREFINE], nbr);
+      base = __shfl_sync(FULL, base, 0);
+      for (int i = lane; i < nbr; i += 32) d.refine_list[base + i] = t * d.KB + i;
+    }
+    __syncwarp();
+  }
+  if (lane == 0 && d.stats) {
+    atomicAdd(&d.stats[0], evals);
+    atomicAdd(&d.stats[2], steps);
+    atomicAdd(&d.stats[1], evals32);
+    atomicAdd(&d.stats[3], steps32);
+    atomicAdd(&d.stats[5], zooms);
+  }
+}
+
+// Brent-Dekker bracketed refinement to the reference's stopping width
+// max(16 eps |x|, min(w/64, tol |x| / 8)) (cpp/common/refinement.hpp:341-396).
+__device__ double brent(const LayerView<double> &m, int wave, double w, double a, double b,
+                        double fa, double fb, double tol, int *evaluations) {
+  if (a == b) return fa == 0. ? a : NAN;
+  if (!isfinite(fa) || !isfinite(fb) || ((fa < 0.) == (fb < 0.) && fa != 0. && fb != 0.)) return NAN;
+  if (fa == 0.) return a;
+  if (fb == 0.) return b;
+  const double big = fmax(fabs(a), fabs(b));
+  const double stop = fmax(16. * 2.220446049250313e-16 * big, fmin((b - a) / 64., .125 * tol * big));
+  double c = b, fc = fb, dd = b - a, e = dd;
+  for (int it = 0; it < 160; ++it) {
+    if ((fb < 0.) == (fc < 0.)) {
+      c = a;
+      fc = fa;
+      e = dd = b - a;
+    }
+    if (fabs(fc) < fabs(fb)) {
+      a = b; fa = fb;
+      b = c; fb = fc;
+      c = a; fc = fa;
+    }
+    if (fb == 0.) return b;
+    const double mid = .5 * (c - b), half = .5 * stop;
+    if (fabs(c - b) <= stop) return .5 * (b + c);
+    if (fabs(e) >= half && fabs(fa) > fabs(fb)) {
+      const double s = fb / fa;
+      double p, q;
+      if (a == c) {
+        p = 2. * mid * s;
+        q = 1. - s;
+      } else {
+        const double qa = fa / fc, r = fb / fc;
+        p = s * (2. * mid * qa * (qa - r) - (b - a) * (r - 1.));
+        q = (qa - 1.) * (r - 1.) * (s - 1.);
+      }
+      if (p > 0.) q = -q; else p = -p;
+      const double old = e;
+      e = dd;
+      const double ratio = p / q;
+      if (isfinite(ratio) && 2. * p < fmin(3. * mid * q - fabs(half * q), fabs(old * q))) dd = ratio;
+      else { dd = mid; e = mid; }
+    } else {
+      dd = mid;
+      e = mid;
+    }
+    a = b;
+    fa = fb;
+    b += fabs(dd) > half ? dd : (mid > 0. ? half : -half);
+    fb = eval64(m, wave, w, b, nullptr);
+    ++*evaluations;
+    if (!isfinite(fb)) return NAN;
+  }
+  return NAN;
+}
+
+// ---------------------------------------------------------------------------
+// refine: one thread per bracket.
+// ---------------------------------------------------------------------------
+__global__ void refine(Dev d) {
+  const int begin = d.ctr[C_REFINE_BEGIN];
+  unsigned long long evals = 0, steps = 0, count = 0;
+  for (int i = begin + blockIdx.x * blockDim.x + threadIdx.x; i < *(volatile int *)&d.ctr[C_NREFINE];
+       i += gridDim.x * blockDim.x) {
+    const int id = d.refine_list[i];
+    const int t = id / d.KB;
+    const int b = t / d.T, f = t - b * d.T;
+    const LayerView<double> m = global_view(d, b);
+    const double w = TWO_PI / d.periods[f];
+    double *sl = d.slot + static_cast<size_t>(id) * SLOT;
+    const double lo = sl[0], hi = sl[1];
+    double flo = sl[2], fhi = sl[3];
+    int ev = 0;
+    if (!(isfinite(flo) && isfinite(fhi))) {  // FP32 scan bracket: confirm in FP64
+      if (!isfinite(flo)) { flo = eval64(m, d.wave, w, lo, nullptr); ++ev; }
+      if (!isfinite(fhi)) { fhi = eval64(m, d.wave, w, hi, nullptr); ++ev; }
+      if (signbit(flo) == signbit(fhi)) {
+        atomicOr(&d.tflags[t], INTERNAL_REPAIR);
+        sl[4] = NAN;
+        evals += ev;
+        steps += static_cast<unsigned long long>(ev) * layer_steps(m.L, m.water);
+        continue;
+      }
+    }
+    const double r = brent(m, d.wave, w, lo, hi, flo, fhi, d.tol, &ev);
+    sl[4] = r;
+    if (!isfinite(r)) atomicOr(&d.tflags[t], TRACE_REFINEMENT_FAILED);
+    evals += ev;
+    steps += static_cast<unsigned long long>(ev) * layer_steps(m.L, m.water);
+    ++count;
+  }
+  if (d.stats && (evals || count)) {
+    atomicAdd(&d.stats[0], evals);
+    atomicAdd(&d.stats[2], steps);
+    atomicAdd(&d.stats[4], count);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// collect_repairs: traces whose FP32 scan FP64 did not confirm.
+// ---------------------------------------------------------------------------
+__global__ void collect_repairs(Dev d) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t == 0) {
+    d.ctr[C_REFINE_BEGIN] = d.ctr[C_NREFINE];
+  }
+  if (t >= d.n_traces) return;
+  const unsigned fl = d.tflags[t];
+  if (fl & INTERNAL_REPAIR) {
+    const int pos = atomicAdd(&d.ctr[C_NREPAIR], 1);
+    d.repair_list[pos] = t;
+    d.tflags[t] = (fl & ~(INTERNAL_REPAIR | TRACE_REFINEMENT_FAILED)) | TRACE_FP64_REPAIR;
+    d.nbr[t] = 0;
+    if (d.stats) atomicAdd(&d.stats[7], 1ULL);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// assemble: one thread per trace.
+// ---------------------------------------------------------------------------
+__global__ void assemble(Dev d) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= d.n_traces) return;
+  const int b = t / d.T, f = t - b * d.T;
+  const int nm = d.nmodes, T = d.T;
+  const size_t out0 = static_cast<size_t>(b) * nm * T + f;
+  const int state = d.mstate[b];
+  if (state != 0) {
+    for (int m = 0; m < nm; ++m) d.vel[out0 + static_cast<size_t>(m) * T] = NAN;
+    d.oflags[t] = 0;
+    d.olevels[t] = state;
+    d.ocounts[t] = 0;
+    if (d.group)
+      for (int m = 0; m < nm; ++m) {
+        d.grp[out0 + static_cast<size_t>(m) * T] = NAN;
+        d.gflags[out0 + static_cast<size_t>(m) * T] = GROUP_MISSING_ROOT;
+      }
+    return;
+  }
+  unsigned fl = d.tflags[t];
+  const int nbr = d.nbr[t];
+  const double *slot = d.slot + static_cast<size_t>(t) * d.KB * SLOT;
+  // gather, order and cap at K (the K = nmodes + 2 smallest roots)
+  double r[64] = {};
+  int n = 0;
+  const int K = d.K;
+  const int cap = K < 64 ? K : 64;
+  bool failed = (fl & (TRACE_SEARCH_UNCONVERGED | INTERNAL_REPAIR)) != 0;
+  auto push = [&](double x) {
+    // insertion into the ascending list, keeping at most `cap` values
+    if (n == cap && !(x < r[n - 1])) return;
+    int i = n < cap ? n++ : n - 1;
+    while (i > 0 && r[i - 1] > x) {
+      r[i] = r[i - 1];
+      --i;
+    }
+    r[i] = x;
+  };
+  for (int s = 0; s < nbr && !failed; ++s) {
+    const double x = slot[static_cast<size_t>(s) * SLOT + 4];
+    if (!isfinite(x)) failed = true;
+    else push(x);
+  }
+  // exact duplicates (an exact zero shared by two brackets) collapse to one root
+  int u = 0;
+  for (int i = 0; i < n; ++i)
+    if (u == 0 || r[i] != r[u - 1]) r[u++] = r[i];
+  n = u;
+  const double lo = d.mlo[b], hi = d.mhi[b];
+  const LayerView<double> m = global_view(d, b);
+  const double vs_hs = layer_table<double>(d, b)[8 * d.Ls + m.L - 1];
+  const double w = TWO_PI / d.periods[f];
+  int level = d.fp32 ? ((fl & TRACE_FP64_REPAIR) ? LEVEL_REPAIRED : LEVEL_FP32) : LEVEL_FP64;
+  int count = n;
+  if (failed) {
+    fl |= TRACE_SEARCH_UNCONVERGED;
+    count = -1;
+    level = -1;
+    n = 0;
+  }
+  for (int i = 1; i < n; ++i)
+    if (r[i] - r[i - 1] <= d.close_rtol * r[i]) fl |= TRACE_CLOSE_ROOT_RISK;
+  for (int mo = 0; mo < nm; ++mo) {
+    double root = mo < n ? r[mo] : NAN;
+    if (isfinite(root) && root >= .99 * vs_hs) fl |= TRACE_NEAR_CUTOFF;
+    if (isfinite(root) && d.accept < 1.) {
+      const double v = eval64(m, d.wave, w, root, nullptr);
+      if (!isfinite(v) || fabs(v) > d.accept) {
+        root = NAN;
+        fl |= TRACE_F_REJECTED;
+      }
+    }
+    const size_t cell = out0 + static_cast<size_t>(mo) * T;
+    d.vel[cell] = root;
+    if (d.group) {
+      if (!isfinite(root)) {
+        d.grp[cell] = NAN;
+        d.gflags[cell] = GROUP_MISSING_ROOT;
+      } else {
+        // neighbour-midpoint window and close-root test (cpp/cpu/solver.cpp:96-103)
+        const double c = r[mo];
+        const double wl = mo ? .5 * (r[mo - 1] + c) : lo;
+        const double wh = mo + 1 < n ? .5 * (c + r[mo + 1]) : hi;
+        const bool close = (mo && c - r[mo - 1] <= d.close_rtol * c) ||
+                           (mo + 1 < n && r[mo + 1] - c <= d.close_rtol * r[mo + 1]);
+        d.gwin[2 * cell] = wl;
+        d.gwin[2 * cell + 1] = wh;
+        if (close) {
+          d.grp[cell] = NAN;
+          d.gflags[cell] = GROUP_CLOSE_ROOT;
+        } else {
+          d.gflags[cell] = 0;
+          const int pos = atomicAdd(&d.ctr[C_NGROUP], 1);
+          d.group_list[pos] = static_cast<int>(cell);
+        }
+      }
+    }
+  }
+  d.oflags[t] = fl & ~INTERNAL_MASK;
+  d.olevels[t] = level;
+  d.ocounts[t] = count;
+  if (d.stats) {
+    atomicAdd(&d.stats[11], 1ULL);
+    if (failed) atomicAdd(&d.stats[8], 1ULL);
+    int finite = 0;
+    for (int mo = 0; mo < nm && mo < n; ++mo) finite += isfinite(d.vel[out0 + static_cast<size_t>(mo) * T]);
+    if (finite) atomicAdd(&d.stats[10], static_cast<unsigned long long>(finite));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// group: one thread per root.  U = -F_k / F_omega from one forward-mode
+// evaluation (value + two directional derivatives) at the refined root.
+// ---------------------------------------------------------------------------
+__global__ void group_velocity(Dev d) {
+  const int n = d.ctr[C_NGROUP];
+  unsigned long long steps = 0, count = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int cell = d.group_list[i];
+    const int T = d.T, nm = d.nmodes;
+    const int b = cell / (nm * T);
+    const int f = cell % T;
+    const LayerView<double> m = global_view(d, b);
+    const double c = d.vel[cell];
+    const double w = TWO_PI / d.periods[f];
+    using D2 = Dual<double, 2>;
+    D2 k, wd;
+    k.v = w / c; k.d[0] = 1.; k.d[1] = 0.;
+    wd.v = w; wd.d[0] = 0.; wd.d[1] = 1.;
+    const D2 F = secular<D2, double>(m, d.wave, k, wd, nullptr);
+    const double fk = F.d[0], fw = F.d[1];
+    double u = -fk / fw;
+    unsigned flag = 0;
+    if (!isfinite(fk) || !isfinite(fw)) flag = GROUP_NONFINITE;
+    else if (fw == 0. || !isfinite(u) || !(u > 0.)) flag = GROUP_ILL_CONDITIONED;
+    d.grp[cell] = flag ? NAN : u;
+    d.gflags[cell] = flag;
+    steps += layer_steps(m.L, m.water);
+    ++count;
+  }
+  if (d.stats && count) {
+    atomicAdd(&d.stats[12], steps);
+    atomicAdd(&d.stats[9], count);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// group_roots: group velocities of one model's given ordered roots (the
+// reference's review-group bridge, cpp/common/review_groups.hpp:9-34).  `tab` is
+// a prepared [EVAL_ROWS][L] table.
+// ---------------------------------------------------------------------------
+__global__ void group_roots(const double *tab, int L, int water, int wave, double w,
+                            const double *roots, int known, int modes, double close_rtol,
+                            double *group, unsigned *flags) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= modes) return;
+  if (j >= known) {
+    group[j] = NAN;
+    flags[j] = GROUP_MISSING_ROOT;
+    return;
+  }
+  const double c = roots[j];
+  if ((j && c - roots[j - 1] <= close_rtol * c) ||
+      (j + 1 < known && roots[j + 1] - c <= close_rtol * roots[j + 1])) {
+    group[j] = NAN;
+    flags[j] = GROUP_CLOSE_ROOT;
+    return;
+  }
+  const LayerView<double> m = make_view<double>(tab, L, L, water);
+  using D2 = Dual<double, 2>;
+  D2 k, wd;
+  k.v = w / c; k.d[0] = 1.; k.d[1] = 0.;
+  wd.v = w; wd.d[0] = 0.; wd.d[1] = 1.;
+  const D2 F = secular<D2, double>(m, wave, k, wd, nullptr);
+  const double u = -F.d[0] / F.d[1];
+  unsigned flag = 0;
+  if (!isfinite(F.d[0]) || !isfinite(F.d[1])) flag = GROUP_NONFINITE;
+  else if (F.d[1] == 0. || !isfinite(u) || !(u > 0.)) flag = GROUP_ILL_CONDITIONED;
+  group[j] = flag ? NAN : u;
+  flags[j] = flag;
+}
+
+}  // namespace md200

@@ -1,0 +1,602 @@
+// secular.cuh -- device secular functions of the modisp_b200 engine.
+//
+// Rayleigh (P-SV): normalized Dunkin compound-matrix recurrence, the algebra of
+//   cpp/common/dunkin.hpp:82-159 (layer eigenfunction products),
+//   :171-221 (compound matrix) and :358-448 (half-space start, upward sweep,
+//   water top).  The 25 matrix entries are formed from their 15 distinct values
+//   and contracted directly with the 5-vector (same matrix, no storage).
+// Love (SH): 2-vector Thomson-Haskell recurrence of cpp/common/physics.hpp:33-53.
+//
+// Everything is generic over the number type N so one source serves the FP32
+// scan (N = float), the FP64 scan and refinement (N = double) and the
+// forward-mode derivatives used for group velocity and Jacobians
+// (N = Dual<double, ND>).  Branches test the value part only, and the per-layer
+// normalisation divides by a power of two taken from the value part: the sign
+// of F and every root are those of the reference function, and derivative parts
+// are the exact derivatives of the unnormalised function times the same positive
+// scale (so ratios of derivatives at a root are exact).
+#pragma once
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+
+// Device code by default; MD200_HOST_SECULAR builds the same recurrences for the
+// host (with libm in place of the device intrinsics) for CPU-side studies.
+#ifdef MD200_HOST_SECULAR
+#define MD200_FN __host__ __device__ __forceinline__
+#else
+#define MD200_FN __device__ __forceinline__
+#endif
+
+namespace md200 {
+
+// ---------------------------------------------------------------------------
+// Number-type helpers
+// ---------------------------------------------------------------------------
+template <class T, int ND>
+struct Dual {
+  T v;
+  T d[ND];
+};
+
+MD200_FN double val(double x) { return x; }
+MD200_FN float val(float x) { return x; }
+template <class T, int ND>
+MD200_FN T val(const Dual<T, ND> &x) { return x.v; }
+
+template <class T>
+struct Base { using type = T; };
+template <class T, int ND>
+struct Base<Dual<T, ND>> { using type = T; };
+
+// Constants of the number type.
+template <class N> struct Lift;
+template <> struct Lift<double> {
+  MD200_FN static double one() { return 1.0; }
+  MD200_FN static double zero() { return 0.0; }
+};
+template <> struct Lift<float> {
+  MD200_FN static float one() { return 1.0f; }
+  MD200_FN static float zero() { return 0.0f; }
+};
+template <class T, int ND> struct Lift<Dual<T, ND>> {
+  MD200_FN static Dual<T, ND> make(T x) {
+    Dual<T, ND> r;
+    r.v = x;
+#pragma unroll
+    for (int i = 0; i < ND; ++i) r.d[i] = T(0);
+    return r;
+  }
+  MD200_FN static Dual<T, ND> one() { return make(T(1)); }
+  MD200_FN static Dual<T, ND> zero() { return make(T(0)); }
+};
+template <class N> MD200_FN N lift_one() { return Lift<N>::one(); }
+template <class N> MD200_FN N lift_zero() { return Lift<N>::zero(); }
+
+#define MD200_DUAL_BINOP(OP, VALUE, DERIV)                                              \
+  template <class T, int ND>                                                            \
+  MD200_FN Dual<T, ND> operator OP(const Dual<T, ND> &a,              \
+                                                     const Dual<T, ND> &b) {            \
+    Dual<T, ND> r;                                                                      \
+    r.v = VALUE;                                                                        \
+    _Pragma("unroll") for (int i = 0; i < ND; ++i) r.d[i] = DERIV;                      \
+    return r;                                                                           \
+  }
+MD200_DUAL_BINOP(+, a.v + b.v, a.d[i] + b.d[i])
+MD200_DUAL_BINOP(-, a.v - b.v, a.d[i] - b.d[i])
+MD200_DUAL_BINOP(*, a.v * b.v, fma(a.d[i], b.v, a.v * b.d[i]))
+#undef MD200_DUAL_BINOP
+
+template <class T, int ND>
+MD200_FN Dual<T, ND> operator/(const Dual<T, ND> &a, const Dual<T, ND> &b) {
+  Dual<T, ND> r;
+  const T ib = T(1) / b.v;
+  r.v = a.v * ib;
+#pragma unroll
+  for (int i = 0; i < ND; ++i) r.d[i] = (a.d[i] - r.v * b.d[i]) * ib;
+  return r;
+}
+template <class T, int ND>
+MD200_FN Dual<T, ND> operator-(const Dual<T, ND> &a) {
+  Dual<T, ND> r;
+  r.v = -a.v;
+#pragma unroll
+  for (int i = 0; i < ND; ++i) r.d[i] = -a.d[i];
+  return r;
+}
+// Mixed with a base-type scalar
+template <class T, int ND>
+MD200_FN Dual<T, ND> operator*(const Dual<T, ND> &a, T s) {
+  Dual<T, ND> r;
+  r.v = a.v * s;
+#pragma unroll
+  for (int i = 0; i < ND; ++i) r.d[i] = a.d[i] * s;
+  return r;
+}
+template <class T, int ND>
+MD200_FN Dual<T, ND> operator*(T s, const Dual<T, ND> &a) { return a * s; }
+template <class T, int ND>
+MD200_FN Dual<T, ND> operator+(const Dual<T, ND> &a, T s) {
+  Dual<T, ND> r = a;
+  r.v += s;
+  return r;
+}
+template <class T, int ND>
+MD200_FN Dual<T, ND> operator+(T s, const Dual<T, ND> &a) { return a + s; }
+template <class T, int ND>
+MD200_FN Dual<T, ND> operator-(const Dual<T, ND> &a, T s) {
+  Dual<T, ND> r = a;
+  r.v -= s;
+  return r;
+}
+template <class T, int ND>
+MD200_FN Dual<T, ND> operator-(T s, const Dual<T, ND> &a) {
+  Dual<T, ND> r = -a;
+  r.v += s;
+  return r;
+}
+
+// --- elementary functions --------------------------------------------------
+// Double: IEEE libdevice routines.  Float: the accurate single-precision
+// routines for sin/cos (argument reduction matters, phases reach ~1e3 rad) and
+// the hardware approximations for exp and reciprocal square root, whose
+// relative errors (~1e-7) sit far below the scan's sign-decision threshold.
+#if defined(__CUDA_ARCH__)
+MD200_FN double m_rsqrt(double x) { return rsqrt(x); }
+MD200_FN float m_rsqrt(float x) { return rsqrtf(x); }
+MD200_FN void m_sincos(double x, double *s, double *c) { sincos(x, s, c); }
+MD200_FN void m_sincos(float x, float *s, float *c) { sincosf(x, s, c); }
+MD200_FN double m_exp(double x) { return exp(x); }
+MD200_FN float m_exp(float x) { return __expf(x); }
+MD200_FN float m_expm1(float x) { return expm1f(x); }
+MD200_FN double m_expm1(double x) { return expm1(x); }
+#else
+MD200_FN double m_rsqrt(double x) { return 1.0 / sqrt(x); }
+MD200_FN float m_rsqrt(float x) { return 1.0f / sqrtf(x); }
+MD200_FN void m_sincos(double x, double *s, double *c) { *s = sin(x); *c = cos(x); }
+MD200_FN void m_sincos(float x, float *s, float *c) { *s = sinf(x); *c = cosf(x); }
+MD200_FN double m_exp(double x) { return exp(x); }
+MD200_FN float m_exp(float x) { return expf(x); }
+MD200_FN float m_expm1(float x) { return expm1f(x); }
+MD200_FN double m_expm1(double x) { return expm1(x); }
+#endif
+MD200_FN double m_sqrt(double x) { return sqrt(x); }
+MD200_FN float m_sqrt(float x) { return sqrtf(x); }
+MD200_FN double m_abs(double x) { return fabs(x); }
+MD200_FN float m_abs(float x) { return fabsf(x); }
+
+template <class T, int ND>
+MD200_FN Dual<T, ND> m_rsqrt(const Dual<T, ND> &x) {
+  Dual<T, ND> r;
+  r.v = m_rsqrt(x.v);
+  const T k = T(-0.5) * r.v * r.v * r.v;
+#pragma unroll
+  for (int i = 0; i < ND; ++i) r.d[i] = k * x.d[i];
+  return r;
+}
+template <class T, int ND>
+MD200_FN void m_sincos(const Dual<T, ND> &x, Dual<T, ND> *s, Dual<T, ND> *c) {
+  T sv, cv;
+  m_sincos(x.v, &sv, &cv);
+  s->v = sv;
+  c->v = cv;
+#pragma unroll
+  for (int i = 0; i < ND; ++i) {
+    s->d[i] = cv * x.d[i];
+    c->d[i] = -sv * x.d[i];
+  }
+}
+template <class T, int ND>
+MD200_FN Dual<T, ND> m_exp(const Dual<T, ND> &x) {
+  Dual<T, ND> r;
+  r.v = m_exp(x.v);
+#pragma unroll
+  for (int i = 0; i < ND; ++i) r.d[i] = r.v * x.d[i];
+  return r;
+}
+template <class T, int ND>
+MD200_FN Dual<T, ND> m_sqrt(const Dual<T, ND> &x) {
+  Dual<T, ND> r;
+  r.v = m_sqrt(x.v);
+  const T k = T(0.5) / r.v;
+#pragma unroll
+  for (int i = 0; i < ND; ++i) r.d[i] = k * x.d[i];
+  return r;
+}
+template <class T, int ND>
+MD200_FN Dual<T, ND> m_abs(const Dual<T, ND> &x) {
+  return x.v < T(0) ? -x : x;
+}
+
+// Exact power-of-two reciprocal of the binade of x (x > 0, finite, normal):
+// for x = m * 2^E with m in [1, 2) it returns 2^-E, so x * r = m lies in [1, 2)
+// and the multiplication is exact.  The per-layer normalisation uses it instead
+// of a division: the normalised vector has max |e_i| in [1, 2), the sign of F
+// and the shape feature are unchanged.
+MD200_FN double pow2_inverse(double x) {
+  long long bits;
+  memcpy(&bits, &x, sizeof bits);
+  const long long e = (bits >> 52) & 0x7ff;
+  bits = (2046LL - e) << 52;
+  double r;
+  memcpy(&r, &bits, sizeof r);
+  return r;
+}
+MD200_FN float pow2_inverse(float x) {
+  int bits;
+  memcpy(&bits, &x, sizeof bits);
+  const int e = (bits >> 23) & 0xff;
+  bits = (254 - e) << 23;
+  float r;
+  memcpy(&r, &bits, sizeof r);
+  return r;
+}
+
+// Scale the vector by the exact power of two that brings its largest component
+// into [1, 2); returns the base-2 exponent removed (0 when nothing was done).
+MD200_FN int binade(double x) {
+  long long bits;
+  memcpy(&bits, &x, sizeof bits);
+  return static_cast<int>((bits >> 52) & 0x7ff) - 1023;
+}
+MD200_FN int binade(float x) {
+  int bits;
+  memcpy(&bits, &x, sizeof bits);
+  return ((bits >> 23) & 0xff) - 127;
+}
+template <class N>
+MD200_FN int scale_vector(N *e, int n, typename Base<N>::type tiny) {
+  using T = typename Base<N>::type;
+  T big = T(0);
+#pragma unroll
+  for (int i = 0; i < 5; ++i)
+    if (i < n) big = fmax(big, m_abs(val(e[i])));
+  if (big >= tiny && big < T(INFINITY)) {
+    const T r = pow2_inverse(big);
+#pragma unroll
+    for (int i = 0; i < 5; ++i)
+      if (i < n) e[i] = e[i] * r;
+    return binade(big);
+  }
+  return 0;
+}
+
+// sqrt((k + kv) |k - kv|) and its reciprocal, from one reciprocal square root.
+template <class N>
+MD200_FN void radical(const N &k, const N &kv, N *r, N *ir) {
+  using T = typename Base<N>::type;
+  N d = k - kv;
+  if (val(d) < T(0)) d = -d;
+  const N X = (k + kv) * d;
+  if (val(X) > T(0)) {
+    *ir = m_rsqrt(X);
+    *r = X * *ir;
+  } else {
+    *r = X;       // zero (with its derivative): the equal-velocity branch ignores it
+    *ir = X;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Model view: per-layer constants prepared once per model (in shared memory).
+// ---------------------------------------------------------------------------
+template <class T>
+struct LayerView {
+  const T *h;     // thickness
+  const T *ivp;   // 1 / vp
+  const T *ivs;   // 1 / vs (0 for a fluid layer)
+  const T *vs2;   // vs^2
+  const T *rho;   // density
+  const T *irho;  // 1 / rho
+  const T *imu;   // 1 / (rho vs^2) (0 for a fluid layer)
+  int L;          // rows including the half-space
+  int water;      // 1 when row 0 is a fluid (vs = 0) layer
+};
+
+// One upward Dunkin step through layer m: e <- e * Ca(m).
+// Returns the exponent P + Q (value part) that the scaled hyperbolic functions
+// of the evanescent branches factor out: the unscaled step is the scaled one
+// times exp(P + Q).
+template <class N, class T>
+MD200_FN typename Base<N>::type rayleigh_layer(N e[5], const N &k, const N &k2, const N &w,
+                                               const N &iw2, T h, T ivp, T vs2, T ivs, T rho,
+                                               T irho) {
+  using BT = typename Base<N>::type;
+  BT expo = BT(0);
+  const N ka = w * ivp, kb = w * ivs;
+  const N gammk = (iw2 * vs2) * T(2);
+  const N gam = gammk * k2;
+  N ra, ira, rb, irb;
+  radical(k, ka, &ra, &ira);
+  radical(k, kb, &rb, &irb);
+
+  N cosp, wv, xv, cosq, yv, zv;
+  N a0 = lift_one<N>();
+  if (val(k) < val(ka)) {
+    N sp;
+    m_sincos(ra * h, &sp, &cosp);
+    wv = sp * ira;
+    xv = -(ra * sp);
+  } else if (val(k) == val(ka)) {
+    cosp = lift_one<N>();
+    wv = lift_one<N>() * h;
+    xv = lift_zero<N>();
+  } else {
+    const N ep = m_exp(-(ra * h));
+    expo += val(ra) * h;
+    const N fac = ep * ep;
+    cosp = (fac + T(1)) * T(0.5);
+    const N sp = (T(1) - fac) * T(0.5);
+    wv = sp * ira;
+    xv = ra * sp;
+    a0 = ep;
+  }
+  if (val(k) < val(kb)) {
+    N sq;
+    m_sincos(rb * h, &sq, &cosq);
+    yv = sq * irb;
+    zv = -(rb * sq);
+  } else if (val(k) == val(kb)) {
+    cosq = lift_one<N>();
+    yv = lift_one<N>() * h;
+    zv = lift_zero<N>();
+  } else {
+    const N eq = m_exp(-(rb * h));
+    expo += val(rb) * h;
+    const N fac = eq * eq;
+    cosq = (fac + T(1)) * T(0.5);
+    const N sq = (T(1) - fac) * T(0.5);
+    yv = sq * irb;
+    zv = rb * sq;
+    a0 = a0 * eq;
+  }
+  const N cpcq = cosp * cosq, cpy = cosp * yv, cpz = cosp * zv;
+  const N cqw = cosq * wv, cqx = cosq * xv;
+  const N xy = xv * yv, xz = xv * zv, wy = wv * yv, wz = wv * zv;
+
+  const N gm1 = gam - T(1);
+  const N twgm1 = gam + gm1;
+  const N gmgmk = gam * gammk;
+  const N gmgm1 = gam * gm1;
+  const N gm1sq = gm1 * gm1;
+  const N a0pq = a0 - cpcq;
+  const T rho2 = rho * rho, irho2 = irho * irho;
+
+  // Distinct entries; the matrix is
+  //   [A D I C L; E B G M C; tJ tH K tG tI; F N H B D; O F J E A], t = -2 k^2.
+  const N A = cpcq - (gmgm1 * a0pq) * T(2) - gmgmk * xz - k2 * gm1sq * wy;
+  const N D = (k2 * cpy - cqx) * irho;
+  const N I = -(twgm1 * a0pq + gammk * xz + k2 * gm1 * wy) * irho;
+  const N C = (cpz - k2 * cqw) * irho;
+  const N Lm = -((k2 * a0pq) * T(2) + xz + k2 * k2 * wy) * irho2;
+  const N E = (gmgmk * cpz - gm1sq * cqw) * rho;
+  const N G = gammk * cpz - gm1 * cqw;
+  const N M = -wz;
+  const N Nn = -xy;
+  const N F = (gm1sq * cpy - gmgmk * cqx) * rho;
+  const N H = gm1 * cpy - gammk * cqx;
+  const N O = -((gmgmk * gm1sq * a0pq) * T(2) + gmgmk * gmgmk * xz + gm1sq * gm1sq * wy) * rho2;
+  const N J = -(gammk * gm1 * twgm1 * a0pq + gam * gammk * gammk * xz + gm1 * gm1sq * wy) * rho;
+  const N K = a0 + (cpcq - A) * T(2);
+  const N B = cpcq;
+
+  const N e0 = e[0], e1 = e[1], e4 = e[4], e3 = e[3];
+  const N e2t = e[2] * (k2 * T(-2));
+  e[0] = A * e0 + E * e1 + J * e2t + F * e3 + O * e4;
+  e[1] = D * e0 + B * e1 + H * e2t + Nn * e3 + F * e4;
+  e[2] = I * e0 + G * e1 + K * e[2] + H * e3 + J * e4;
+  e[3] = C * e0 + M * e1 + G * e2t + B * e3 + E * e4;
+  e[4] = Lm * e0 + C * e1 + I * e2t + D * e3 + A * e4;
+  return expo;
+}
+
+// The same layer step for a layer in which both waves are deeply evanescent
+// (c < vs/4), in single precision.  With u = (c/vp)^2, v = (c/vs)^2, p = sqrt(1-u),
+// s = sqrt(1-v), R = p s and g = 2/v (the standard form's gamma), the standard
+// entries are sums of terms growing like g^4 that cancel down to O(g^2); here each
+// entry is written through the exactly-computed differences 1 - R (loss),
+// v - u (contrast) and the exponential differences of the two phases, so no
+// cancellation occurs (the factorisation of cpp/common/dunkin.hpp:286-331).
+MD200_FN float rayleigh_layer_evanescent(float e[5], float k, float k2, float c, float h, float ivp,
+                                         float ivs, float rho, float irho) {
+  const float cp = c * ivp, cs = c * ivs, u = cp * cp, v = cs * cs;
+  const float p = sqrtf(1.f - u), s = sqrtf(1.f - v), R = p * s;
+  const float loss = (u + (1.f - u) * v) / (1.f + R);
+  const float g = 2.f / v, contrast = v - u;
+  const float kh = k * h, q = kh * s;
+  float sp = .5f, sq = .5f, a0 = 0.f, delta = 0.f, gap = 0.f;
+  if (q < 16.f) {
+    const float pq = kh * contrast / (p + s);  // P - Q, the phase difference
+    const float eq = m_exp(-q), diff = -eq * m_expm1(-pq);
+    sp = -.5f * m_expm1(-2.f * (q + pq));
+    sq = -.5f * m_expm1(-2.f * q);
+    a0 = eq * (eq - diff);
+    delta = -.5f * diff * (2.f * eq - diff);  // cos_p sin_q - cos_q sin_p (scaled)
+    gap = .5f * diff * diff;                  // cos_p cos_q - a0 - sin_p sin_q (scaled)
+  }
+  const float gm1 = g - 1.f, twgm1 = g + gm1;
+  const float gl = g * loss;
+  const float d1 = 1.f - gl, d2 = g * (2.f - gl) - 1.f;
+  const float ps = sp * sq, psr = ps / R, y = (1.f - sq) * sp, x = (1.f - sp) * sq;
+  const float q1 = 2.f * g * gm1 * gap, q2 = psr * d1 * d1;
+  const float kp = k / p, ks = k / s, ip = 1.f / (k * p), is = 1.f / (k * s);
+  const float rho2 = rho * rho, irho2 = irho * irho, ik2 = 1.f / k2;
+  const float B = (1.f - sp) * (1.f - sq), A = B + q1 - q2;
+  const float D = ks * (delta + loss * y) * irho, C = kp * (delta - loss * x) * irho;
+  const float G = (g * R * delta + d1 * y) * ip, H = (gm1 * delta - d1 * y) * is;
+  const float E = (g * g * R * delta + d2 * y) * ip * rho, F = (gm1 * gm1 * delta - d2 * y) * is * rho;
+  const float I = (twgm1 * gap + psr * loss * d1) * irho;
+  const float Lm = k2 * (2.f * gap - psr * loss * loss) * irho2;
+  const float J = (g * gm1 * twgm1 * gap - psr * d1 * d2) * rho * ik2;
+  const float O = (g * gm1 * q1 - psr * d2 * d2) * rho2 * ik2;
+  const float K = a0 + 2.f * (q2 - q1), M = -ps * (s / p), Nn = -ps * (p / s);
+  const float e0 = e[0], e1 = e[1], e3 = e[3], e4 = e[4];
+  const float e2t = e[2] * (-2.f * k2);
+  e[0] = A * e0 + E * e1 + J * e2t + F * e3 + O * e4;
+  e[1] = D * e0 + B * e1 + H * e2t + Nn * e3 + F * e4;
+  e[2] = I * e0 + G * e1 + K * e[2] + H * e3 + J * e4;
+  e[3] = C * e0 + M * e1 + G * e2t + B * e3 + E * e4;
+  e[4] = Lm * e0 + C * e1 + I * e2t + D * e3 + A * e4;
+  return kh * (p + s);  // P + Q
+}
+
+// Rayleigh secular value F(k, w) and shape feature g = F / |e| (water top: the
+// fluid form).  Units: k = w / c in rad/km, w in rad/s.  With `lmag`, also the
+// base-2 logarithm of the magnitude |e| of the unnormalised vector: it is smooth
+// across ordinary roots and dips logarithmically where the whole vector nearly
+// vanishes, the signature of a close root pair.
+template <class N, class T>
+MD200_FN N rayleigh_secular(const LayerView<T> &m, const N &k, const N &w, N *shape,
+                            typename Base<N>::type *lmag = nullptr) {
+  using B = typename Base<N>::type;
+  const B tiny = sizeof(B) == 4 ? B(1e-30) : B(1e-40);
+  const N k2 = k * k;
+  const N iw = lift_one<N>() / w;
+  const N iw2 = iw * iw;
+  const int last = m.L - 1;
+  N e[5];
+  {
+    const N ka = w * m.ivp[last], kb = w * m.ivs[last];
+    N ra, ira, rb, irb;
+    radical(k, ka, &ra, &ira);
+    radical(k, kb, &rb, &irb);
+    const N gammk = (iw2 * m.vs2[last]) * T(2);
+    const N gam = gammk * k2;
+    const N gm1 = gam - T(1);
+    const T rh = m.rho[last];
+    const N rarb = ra * rb;
+    e[0] = (gm1 * gm1 - gam * gammk * rarb) * (rh * rh);
+    e[1] = -(ra * rh);
+    e[2] = (gm1 - gammk * rarb) * rh;
+    e[3] = rb * rh;
+    e[4] = k2 - rarb;
+  }
+  if constexpr (sizeof(N) == sizeof(float)) {
+    // single precision: factored start and steps where c < vs/4
+    const float c = w / k;
+    const float ivs_l = m.ivs[last];
+    if (4.f * c * ivs_l < 1.f) {
+      const float cp = c * m.ivp[last], cs = c * ivs_l, u = cp * cp, v = cs * cs;
+      const float p = sqrtf(1.f - u), s = sqrtf(1.f - v), R = p * s;
+      const float loss = (u + (1.f - u) * v) / (1.f + R), g = 2.f / v;
+      const float d1 = 1.f - g * loss, rh = m.rho[last];
+      e[0] = rh * rh * (1.f - g * (1.f + d1));
+      e[1] = -rh * k * p;
+      e[2] = -rh * d1;
+      e[3] = rh * k * s;
+      e[4] = k2 * loss;
+    }
+    int ex = scale_vector(e, 5, tiny);
+    float ev = 0.f;
+    for (int l = m.L - 2; l >= m.water; --l) {
+      if (4.f * c * m.ivs[l] < 1.f)
+        ev += rayleigh_layer_evanescent(e, k, k2, c, m.h[l], m.ivp[l], m.ivs[l], m.rho[l], m.irho[l]);
+      else
+        ev += rayleigh_layer(e, k, k2, w, iw2, m.h[l], m.ivp[l], m.vs2[l], m.ivs[l], m.rho[l], m.irho[l]);
+      ex += scale_vector(e, 5, tiny);
+    }
+    if (lmag) *lmag = static_cast<float>(ex) + ev * 1.4426950408889634f;
+  } else {
+    int ex = scale_vector(e, 5, tiny);
+    B ev = B(0);
+    for (int l = m.L - 2; l >= m.water; --l) {
+      ev += rayleigh_layer(e, k, k2, w, iw2, m.h[l], m.ivp[l], m.vs2[l], m.ivs[l], m.rho[l], m.irho[l]);
+      ex += scale_vector(e, 5, tiny);
+    }
+    if (lmag) *lmag = static_cast<B>(ex) + ev * B(1.4426950408889634);
+  }
+  if (m.water) {
+    const N ka = w * m.ivp[0];
+    N rf, irf;
+    radical(k, ka, &rf, &irf);
+    const T h0 = m.h[0];
+    N cp, wv;
+    if (val(k) < val(ka)) {
+      N sn;
+      m_sincos(rf * h0, &sn, &cp);
+      wv = sn * irf;
+    } else if (val(k) == val(ka)) {
+      cp = lift_one<N>();
+      wv = lift_one<N>() * h0;
+    } else {
+      const N ez = m_exp(-(rf * h0));
+      const N z = ez * ez;
+      cp = (z + B(1)) * B(0.5);
+      wv = ((B(1) - z) * B(0.5)) * irf;
+    }
+    const N t0 = cp * e[0], t1 = wv * e[1] * m.rho[0];
+    N pair[2] = {t0, t1};
+    const int pex = scale_vector(pair, 2, tiny);
+    if (lmag) *lmag += static_cast<B>(pex);
+    const N u = pair[0], v = pair[1];
+    if (shape) *shape = (u - v) * m_rsqrt(u * u + v * v + lift_one<N>() * tiny);
+    if (lmag) *lmag += B(0.5) * log2(val(u * u + v * v) + tiny);
+    return u - v;
+  }
+  const N norm2 = e[0] * e[0] + e[1] * e[1] + e[2] * e[2] + e[3] * e[3] + e[4] * e[4];
+  if (shape) *shape = e[0] * m_rsqrt(norm2 + lift_one<N>() * tiny);
+  if (lmag) *lmag += B(0.5) * log2(val(norm2) + tiny);
+  return e[0];
+}
+
+// Love secular value (SH propagator) and shape feature.
+template <class N, class T>
+MD200_FN N love_secular(const LayerView<T> &m, const N &k, const N &w, N *shape,
+                        typename Base<N>::type *lmag = nullptr) {
+  using B = typename Base<N>::type;
+  const B tiny = sizeof(B) == 4 ? B(1e-30) : B(1e-40);
+  const int last = m.L - 1;
+  N e[2];
+  {
+    const N kb = w * m.ivs[last];
+    N r, ir;
+    radical(k, kb, &r, &ir);
+    e[0] = r * m.rho[last];
+    e[1] = lift_one<N>() * (m.ivs[last] * m.ivs[last]);
+  }
+  int ex = 0;
+  B ev = B(0);
+  for (int j = last - 1; j >= m.water; --j) {
+    const T h = m.h[j], mu = m.rho[j] * m.vs2[j], imu = m.imu[j];
+    const N kj = w * m.ivs[j];
+    N r, ir;
+    radical(k, kj, &r, &ir);
+    N cq, y, z;
+    if (val(k) < val(kj)) {
+      N sn;
+      m_sincos(r * h, &sn, &cq);
+      y = sn * ir;
+      z = -(r * sn);
+    } else if (val(k) == val(kj)) {
+      cq = lift_one<N>();
+      y = lift_one<N>() * h;
+      z = lift_zero<N>();
+    } else {
+      const N eq = m_exp(-(r * h));
+      ev += val(r) * h;
+      const N f = eq * eq;
+      cq = (f + B(1)) * B(0.5);
+      const N half = (B(1) - f) * B(0.5);
+      y = half * ir;
+      z = half * r;
+    }
+    const N u = e[0] * cq + e[1] * z * mu;
+    const N v = e[0] * y * imu + e[1] * cq;
+    e[0] = u;
+    e[1] = v;
+    ex += scale_vector(e, 2, tiny);
+  }
+  const N norm2 = e[0] * e[0] + e[1] * e[1];
+  if (shape) *shape = e[0] * m_rsqrt(norm2 + lift_one<N>() * tiny);
+  if (lmag) *lmag = static_cast<B>(ex) + ev * B(1.4426950408889634) + B(0.5) * log2(val(norm2) + tiny);
+  return e[0];
+}
+
+template <class N, class T>
+MD200_FN N secular(const LayerView<T> &m, int wave, const N &k, const N &w, N *shape,
+                   typename Base<N>::type *lmag = nullptr) {
+  return wave ? love_secular<N, T>(m, k, w, shape, lmag) : rayleigh_secular<N, T>(m, k, w, shape, lmag);
+}
+
+}  // namespace md200

@@ -1,0 +1,199 @@
+"""The oracle: CPU checkers for the modisp_b200 CUDA engine.
+
+TEST INFRASTRUCTURE ONLY.  Only ``tests/``, ``__graft_entry__.smoke()`` and the
+CPU-baseline / reference legs of ``bench.py`` import this package, and only to
+check or time against it.  The product package ``modisp_b200`` never imports it.
+
+Two checkers live here:
+
+* ``libmdoracle.so`` (``md_oracle.c``): a C restatement of the reference's FP64
+  numerics -- secular functions, search window, Brent refinement, a dense-grid
+  root search -- plus complex-step derivatives in long double for group
+  velocities and Jacobians.
+* ``_ref/_cpu*.so``: the reference's own CPU engine (``CpuSolver``), compiled
+  from its unmodified sources by ``oracle/Makefile``.  It is the root-set
+  oracle: mode counts, labels and masks are compared against it.
+
+Build both with ``make -C oracle`` (``__graft_entry__.build()`` does this).
+"""
+from __future__ import annotations
+
+import ctypes
+import glob
+import importlib.util
+import os
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+_LIB = None
+_REF = None
+
+TWO_PI = 6.283185307179586476925286766559
+
+
+def build(quiet: bool = True) -> None:
+    """Compile the C restatement and, where the reference tree exists, the reference engine."""
+    import subprocess
+    cmd = ["make", "-C", str(HERE), "all"]
+    subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL if quiet else None)
+
+
+def lib():
+    """ctypes handle of the C restatement (builds it on first use)."""
+    global _LIB
+    if _LIB is None:
+        path = HERE / "_build" / "libmdoracle.so"
+        if not path.exists():
+            build()
+        L = ctypes.CDLL(str(path))
+        d = ctypes.c_double
+        P = ctypes.POINTER(ctypes.c_double)
+        i = ctypes.c_int
+        L.mdo_secular.restype = d
+        L.mdo_secular.argtypes = [P, P, P, P, i, i, d, d, P]
+        L.mdo_love_phase.restype = d
+        L.mdo_love_phase.argtypes = [P, P, P, i, d, d]
+        L.mdo_bounds.restype = None
+        L.mdo_bounds.argtypes = [P, P, P, P, i, i, P, P]
+        L.mdo_refine.restype = d
+        L.mdo_refine.argtypes = [P, P, P, P, i, i, d, d, d, d, d, d, ctypes.POINTER(i)]
+        L.mdo_dense_roots.restype = i
+        L.mdo_dense_roots.argtypes = [P, P, P, P, i, i, d, d, d, i, d, P]
+        L.mdo_derivatives.restype = None
+        L.mdo_derivatives.argtypes = [P, P, P, P, i, i, d, d, P, P]
+        L.mdo_group.restype = i
+        L.mdo_group.argtypes = [P, P, P, P, i, i, d, d, d, d, P]
+        L.mdo_parameter_derivatives.restype = None
+        L.mdo_parameter_derivatives.argtypes = [P, P, P, P, i, i, d, d, P, P]
+        _LIB = L
+    return _LIB
+
+
+def reference():
+    """The reference's compiled CPU engine module (``_cpu``), or None if not built."""
+    global _REF
+    if _REF is None:
+        hits = sorted(glob.glob(str(HERE / "_ref" / "_cpu*.so")))
+        if not hits:
+            return None
+        spec = importlib.util.spec_from_file_location("_cpu", hits[0])
+        module = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(module)
+        _REF = module
+    return _REF
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _model(h, vp, vs, rho):
+    arrays = [np.ascontiguousarray(x, dtype=np.float64).ravel() for x in (h, vp, vs, rho)]
+    return arrays, arrays[0].size
+
+
+def secular(h, vp, vs, rho, period, velocity, wave=0, shape=False):
+    """F (and the shape feature g) at each velocity for one model and period."""
+    (h, vp, vs, rho), L = _model(h, vp, vs, rho)
+    c = np.atleast_1d(np.asarray(velocity, dtype=np.float64))
+    omega = TWO_PI / period
+    out = np.empty(c.size)
+    g = np.empty(c.size)
+    tmp = ctypes.c_double()
+    for j, x in enumerate(c):
+        out[j] = lib().mdo_secular(_ptr(h), _ptr(vp), _ptr(vs), _ptr(rho), L, int(wave), omega,
+                                   float(x), ctypes.byref(tmp))
+        g[j] = tmp.value
+    return (out, g) if shape else out
+
+
+def love_phase(h, vs, rho, period, velocity):
+    (h, _, vs, rho), L = _model(h, h, vs, rho)
+    omega = TWO_PI / period
+    return np.array([lib().mdo_love_phase(_ptr(h), _ptr(vs), _ptr(rho), L, omega, float(x))
+                     for x in np.atleast_1d(velocity)])
+
+
+def bounds(h, vp, vs, rho, wave=0):
+    """[B, 2] search windows for a [B, L] batch."""
+    h, vp, vs, rho = (np.atleast_2d(np.ascontiguousarray(x, dtype=np.float64)) for x in (h, vp, vs, rho))
+    out = np.empty((h.shape[0], 2))
+    lo, hi = ctypes.c_double(), ctypes.c_double()
+    for b in range(h.shape[0]):
+        row = [np.ascontiguousarray(x[b]) for x in (h, vp, vs, rho)]
+        lib().mdo_bounds(*(_ptr(r) for r in row), h.shape[1], int(wave), ctypes.byref(lo), ctypes.byref(hi))
+        out[b] = lo.value, hi.value
+    return out
+
+
+def dense_roots(h, vp, vs, rho, period, lo, hi, K, tol=1e-12, wave=0):
+    (h, vp, vs, rho), L = _model(h, vp, vs, rho)
+    roots = np.full(K, np.nan)
+    n = lib().mdo_dense_roots(_ptr(h), _ptr(vp), _ptr(vs), _ptr(rho), L, int(wave), float(period),
+                              float(lo), float(hi), int(K), float(tol), _ptr(roots))
+    return n, roots
+
+
+def derivatives(h, vp, vs, rho, period, c, wave=0):
+    (h, vp, vs, rho), L = _model(h, vp, vs, rho)
+    fk, fw = ctypes.c_double(), ctypes.c_double()
+    lib().mdo_derivatives(_ptr(h), _ptr(vp), _ptr(vs), _ptr(rho), L, int(wave), TWO_PI / period,
+                          float(c), ctypes.byref(fk), ctypes.byref(fw))
+    return fk.value, fw.value
+
+
+def group(h, vp, vs, rho, period, root, lower, upper, wave=0):
+    (h, vp, vs, rho), L = _model(h, vp, vs, rho)
+    u = ctypes.c_double()
+    rc = lib().mdo_group(_ptr(h), _ptr(vp), _ptr(vs), _ptr(rho), L, int(wave), TWO_PI / period,
+                         float(root), float(lower), float(upper), ctypes.byref(u))
+    return u.value if rc == 0 else np.nan
+
+
+def parameter_derivatives(h, vp, vs, rho, period, c, wave=0):
+    """(dF/dtheta [4, L] for h, vp, vs, rho; dF/dc) at one root, by complex step."""
+    (h, vp, vs, rho), L = _model(h, vp, vs, rho)
+    out = np.empty(4 * L)
+    fc = ctypes.c_double()
+    lib().mdo_parameter_derivatives(_ptr(h), _ptr(vp), _ptr(vs), _ptr(rho), L, int(wave),
+                                    TWO_PI / period, float(c), _ptr(out), ctypes.byref(fc))
+    return out.reshape(4, L), fc.value
+
+
+def group_windows(roots, lower, upper, close_rtol=0.005):
+    """Neighbour-midpoint windows and close-root flags (cpp/cpu/solver.cpp:96-103)."""
+    n = len(roots)
+    lo = np.empty(n)
+    hi = np.empty(n)
+    close = np.zeros(n, dtype=bool)
+    for j, c in enumerate(roots):
+        lo[j] = .5 * (roots[j - 1] + c) if j else lower
+        hi[j] = .5 * (c + roots[j + 1]) if j + 1 < n else upper
+        close[j] = (j and c - roots[j - 1] <= close_rtol * c) or (j + 1 < n and roots[j + 1] - c <= close_rtol * roots[j + 1])
+    return lo, hi, close
+
+
+def reference_solve(h, vp, vs, rho, periods, nmodes, wave=0, tol=1e-12, threads=None,
+                    group_velocity=False, group_rtol=1e-3, accuracy=0):
+    """Run the reference CPU engine on a [B, L] batch the way its Python wrapper does
+    for ``Solver(backend="cpu", accuracy="high", search_strategy="shape_adaptive",
+    secular="dunkin", refinement="brent", love_strategy="phase")``
+    (python/modisp/__init__.py:343,414-424)."""
+    ref = reference()
+    if ref is None:
+        raise RuntimeError("reference CPU engine not built (make -C oracle ref)")
+    h, vp, vs, rho = (np.atleast_2d(np.ascontiguousarray(x, dtype=np.float64)) for x in (h, vp, vs, rho))
+    periods = np.ascontiguousarray(periods, dtype=np.float64)
+    threads = threads or min(256, len(os.sched_getaffinity(0)))
+    bnd = ref.bounds(h, vp, vs, rho, int(wave), None, None)
+    solver = ref.CpuSolver(int(threads), int(accuracy), 0., .005, True, .001, 0, 1, 1)
+    out = solver.run(h, vp, vs, rho, periods, bnd, int(nmodes), int(wave), True, float(tol), 1.,
+                     False, bool(group_velocity), float(group_rtol), True)
+    velocity, flags, stats, levels, counts, extras = out
+    counts = counts.copy()
+    counts[(flags & 4) != 0] = -1
+    return dict(phase_velocity=velocity, trace_flags=flags, stats=stats, search_level=levels,
+                root_count=counts, group_velocity=extras["group_velocity"],
+                group_velocity_flags=extras["group_velocity_flags"], search_bounds=bnd)

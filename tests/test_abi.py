@@ -1,0 +1,106 @@
+"""The C-ABI library and the Python binding, without a GPU."""
+import ctypes
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+
+def _declared_functions():
+    text = (ROOT / "include" / "modisp_b200.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(md200_\w+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_function():
+    from modisp_b200 import _native
+    lib = _native.lib()
+    declared = _declared_functions()
+    assert len(declared) >= 12
+    for name in declared:
+        assert hasattr(lib, name), name
+    assert set(declared) == set(_native.EXPORTS)
+
+
+def test_library_is_built_for_sm100a():
+    from modisp_b200 import build
+    cmd = build.command()
+    assert "-gencode=arch=compute_100a,code=sm_100a" in cmd
+
+
+def test_options_struct_matches_header():
+    from modisp_b200 import _native
+    text = (ROOT / "include" / "modisp_b200.h").read_text()
+    body = text[text.index("typedef struct md200_options"):text.index("} md200_options;")]
+    fields = re.findall(r"^\s*(?:int|double)\s+(\w+);", body, flags=re.M)
+    assert fields == [f for f, _ in _native.Options._fields_]
+    o = _native.default_options()
+    assert o.close_root_rtol == .005 and o.refinement == 1 and o.anchor_stride == 4
+
+
+def test_no_device_is_reported_cleanly():
+    from modisp_b200 import _native, plugin
+    n = _native.device_count()
+    assert n >= 0
+    if n == 0:
+        assert not plugin.available(0)
+        with pytest.raises(RuntimeError):
+            _native.Engine(0, 4, 3, 2, 1, _native.default_options())
+        assert "CUDA" in _native.last_error() or "modisp_b200" in _native.last_error()
+
+
+def test_invalid_geometry_is_rejected_before_any_device_work():
+    from modisp_b200 import _native
+    with pytest.raises(RuntimeError, match="invalid engine geometry"):
+        _native.Engine(0, 0, 3, 2, 1, _native.default_options())
+    with pytest.raises(RuntimeError, match="invalid engine geometry"):
+        _native.Engine(0, 4, 300, 2, 1, _native.default_options())
+
+
+def test_plugin_contract_attributes():
+    import modisp_cuda
+    module = modisp_cuda.load()
+    assert modisp_cuda.__version__ == module.VERSION == "0.5.0"
+    assert module.ABI_VERSION == 9
+    for flag in ("SUPPORTS_FP32", "SUPPORTS_AUTO_ACCURACY", "SUPPORTS_CANONICAL_LOWER",
+                 "SUPPORTS_GROUP_VELOCITY", "SUPPORTS_CONTINUATION"):
+        assert getattr(module, flag) is True
+    for fn in ("available", "set_device", "memory_info", "device_name", "qe_kernel_report",
+               "love_phase_kernel_report", "_review_groups", "QeSolver"):
+        assert callable(getattr(module, fn))
+
+
+def test_solver_validation_matches_reference_rules():
+    import modisp_b200 as md
+    with pytest.raises(ValueError, match="backend"):
+        md.Solver(backend="cpu")
+    with pytest.raises(ValueError, match="group_rtol"):
+        md.Solver(group_rtol=2.)
+    with pytest.raises(ValueError, match="precision"):
+        md.Solver(precision="half")
+    with pytest.raises(ValueError, match="cmax must exceed cmin"):
+        md.Solver(cmin=2., cmax=1.)
+    from modisp_b200.api import _models
+    with pytest.raises(ValueError, match="sqrt"):
+        _models([1., 0.], [1., 5.], [1., 3.], [2., 2.])
+    with pytest.raises(ValueError, match="water"):
+        _models([1., 1., 0.], [1.5, 1.5, 5.], [0., 0., 3.], [1., 1., 2.])
+    with pytest.raises(ValueError, match="256"):
+        _models(np.ones(300), np.full(300, 5.), np.full(300, 3.), np.ones(300))
+
+
+def test_workloads_have_the_stated_shapes():
+    from modisp_b200 import workloads
+    batch, periods, nmodes = workloads.config2(64)
+    assert batch["thickness"].shape == (64, 21) and periods.size == 60 and nmodes == 5
+    assert np.all(batch["thickness"][:, -1] == 0.)
+    real = (batch["thickness"] > 0).sum(axis=1)
+    assert real.min() >= 8 and real.max() <= 20
+    assert np.all(batch["vp"] / batch["vs"] > 1.69)
+    lvz, _, _ = workloads.config3(200)
+    drops = np.any(lvz["vs"][:, 1:-1] < 0.81 * lvz["vs"][:, :-2], axis=1)
+    assert 0.15 < drops.mean() < 0.45
+    b4, p4, k4 = workloads.config4(16)
+    assert b4["thickness"].shape == (16, 13) and p4.size == 40 and k4 == 3

@@ -1,0 +1,212 @@
+"""GPU parity: the engine, called through its C ABI, against the oracle.
+
+Requirements (per trace and mode):
+* root counts, mode labels and validity masks identical to the reference CPU
+  engine's (bit-exact);
+* phase velocities within |dc|/c <= 1e-9 of the reference at c_tol_rel 1e-12;
+* group velocities within 1e-9 of the oracle's complex-step implicit derivative,
+  with the structural group flags (missing root, close root) identical.
+Both engine precisions are checked: FP64 throughout, and FP32 scan with FP64
+refinement.
+"""
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, load_golden
+
+pytestmark = pytest.mark.gpu
+
+PHASE_RTOL = 1e-9
+GROUP_RTOL = 1e-9
+ENGINE_TOL = 1e-10
+
+
+def engine_solve(g, single_precision, group=True, tol=ENGINE_TOL, bounds=None, **tuning):
+    from modisp_b200 import plugin
+    h, vp, vs, rho = (np.atleast_2d(g[k]) for k in ("thickness", "vp", "vs", "rho"))
+    periods = np.atleast_1d(g["periods"]).astype(np.float64)
+    nmodes = int(g["nmodes"])
+    solver = plugin.QeSolver(h.shape[0], h.shape[1], periods.size, nmodes, 0, 0., .005, True, .001, 0, 1, 1,
+                             single_precision, group, .001, False, 4, **tuning)
+    try:
+        bnd = g["search_bounds"] if bounds is None else bounds
+        v, flags, stats, levels, counts, extras = solver.run(h, vp, vs, rho, periods, bnd, tol, 1., int(g["wave"]))
+    finally:
+        solver.close()
+    if single_precision:
+        pass  # the plugin returns float32 in single precision, like the reference
+    return dict(phase_velocity=v, trace_flags=flags, stats=stats, search_level=levels, root_count=counts, **extras)
+
+
+def engine_solve64(g, single_precision, **kw):
+    """Mixed-precision engine results at full FP64 output precision."""
+    from modisp_b200 import _native
+    h, vp, vs, rho = (np.atleast_2d(g[k]) for k in ("thickness", "vp", "vs", "rho"))
+    periods = np.atleast_1d(g["periods"]).astype(np.float64)
+    o = _native.default_options()
+    o.single_precision = int(single_precision)
+    o.group_velocity = 1
+    for k, v in kw.items():
+        setattr(o, k, v)
+    e = _native.Engine(0, h.shape[0], h.shape[1], periods.size, int(g["nmodes"]), o)
+    try:
+        return e.run(h, vp, vs, rho, periods, g["search_bounds"], ENGINE_TOL, 1., int(g["wave"]), group=True)
+    finally:
+        e.close()
+
+
+def assert_root_parity(ref, out, where):
+    rv, ov = ref["phase_velocity"], out["velocity"] if "velocity" in out else out["phase_velocity"]
+    mask_ref, mask = np.isfinite(rv), np.isfinite(ov)
+    bad = np.argwhere(mask_ref != mask)
+    assert bad.size == 0, f"{where}: {len(bad)} mask mismatches, first {bad[:5].tolist()}"
+    counts = out["counts"] if "counts" in out else out["root_count"]
+    np.testing.assert_array_equal(counts, ref["root_count"], err_msg=f"{where}: root counts")
+    rel = np.abs(ov[mask] - rv[mask]) / rv[mask]
+    assert rel.max(initial=0.) <= PHASE_RTOL, f"{where}: max |dc|/c {rel.max():.3e}"
+    return rel.max(initial=0.)
+
+
+REF_CASES = sorted(p.stem for p in GOLDEN.glob("ref_*.npz"))
+
+
+@pytest.mark.parametrize("single_precision", [False, True], ids=["fp64", "fp32scan"])
+@pytest.mark.parametrize("name", REF_CASES)
+def test_matches_reference_engine(name, single_precision):
+    g = load_golden(name)
+    out = engine_solve64(g, single_precision)
+    assert_root_parity(g, out, name)
+    assert not np.any(out["flags"] & 4), "unconverged traces"
+
+
+@pytest.mark.parametrize("single_precision", [False, True], ids=["fp64", "fp32scan"])
+@pytest.mark.parametrize("name", ["ref_quickstart_rayleigh", "ref_quickstart_love", "ref_crustal48_rayleigh",
+                                  "ref_lvz48_love", "ref_water6_rayleigh"])
+def test_group_velocity_matches_complex_step_oracle(name, single_precision):
+    import oracle
+    g = load_golden(name)
+    out = engine_solve64(g, single_precision)
+    ref_flags = g["group_velocity_flags"]
+    gv, gf = out["group_velocity"], out["group_velocity_flags"]
+    # structural flags: missing root and close root are exact
+    for bit in (1, 16):
+        np.testing.assert_array_equal(gf & bit, ref_flags & bit)
+    wave = int(g["wave"])
+    rng = np.random.default_rng(0)
+    B, nm, T = gv.shape
+    cells = np.argwhere(gf == 0)
+    assert cells.size
+    pick = cells[rng.choice(len(cells), size=min(200, len(cells)), replace=False)]
+    worst = 0.
+    for b, m, f in pick:
+        v = out["velocity"][b, :, f]
+        roots = v[np.isfinite(v)]
+        lo, hi = g["search_bounds"][b]
+        wl, wh, _ = oracle.group_windows(roots, lo, hi)
+        u = oracle.group(g["thickness"][b], g["vp"][b], g["vs"][b], g["rho"][b], g["periods"][f], roots[m],
+                         wl[m], wh[m], wave)
+        worst = max(worst, abs(gv[b, m, f] - u) / u)
+    assert worst <= GROUP_RTOL, f"max group |dU|/U {worst:.3e}"
+    # the reference's own finite-difference estimator at its default group_rtol 1e-3
+    # deviates from the converged value by up to 3.3e-3 on these models (at 1e-4 it
+    # agrees with the oracle to 1e-7); it is a loose cross-check only
+    both = (gf == 0) & (ref_flags == 0)
+    rel = np.abs(gv[both] - g["group_velocity"][both]) / g["group_velocity"][both]
+    assert rel.max(initial=0.) < 5e-3
+
+
+@pytest.mark.parametrize("name", sorted(p.stem for p in GOLDEN.glob("fixture_witness_*.npz")))
+@pytest.mark.parametrize("single_precision", [False, True], ids=["fp64", "fp32scan"])
+def test_independent_witnesses(name, single_precision):
+    """FP64 CPS/disba and QEDispInv witness roots, including near-kissing pairs."""
+    import oracle
+    g = load_golden(name)
+    expected = g["reference_hi"].ravel()
+    case = dict(thickness=g["thickness"], vp=g["vp"], vs=g["vs"], rho=g["rho"], periods=g["periods"],
+                nmodes=expected.size, wave=0,
+                search_bounds=oracle.bounds(g["thickness"], g["vp"], g["vs"], g["rho"], 0))
+    out = engine_solve64(case, single_precision)
+    np.testing.assert_allclose(out["velocity"].ravel(), expected, rtol=2e-6)
+
+
+@pytest.mark.parametrize("name", sorted(p.stem for p in GOLDEN.glob("fixture_0*.npz")))
+def test_reference_frozen_fixtures(name):
+    """The reference suite's frozen high-accuracy cases: same masks and counts, roots to 1e-6."""
+    g = load_golden(name)
+    case = dict(g)
+    case["wave"] = 1 if str(g["wave"]) == "love" else 0
+    out = engine_solve64(case, False)
+    np.testing.assert_array_equal(np.isfinite(out["velocity"]), g["mode_mask"])
+    np.testing.assert_array_equal(out["counts"], g["root_count"])
+    m = g["mode_mask"]
+    np.testing.assert_allclose(out["velocity"][m], g["phase_velocity"][m], rtol=1e-6)
+
+
+@pytest.mark.parametrize("wave", [0, 1])
+def test_live_reference_on_fresh_lvz_batch(wave):
+    """A batch the fixtures never saw, against the reference engine run live on the host."""
+    import oracle
+    from modisp_b200 import workloads
+    if oracle.reference() is None:
+        pytest.skip("reference CPU engine not built")
+    batch = workloads.crustal_batch(64, seed=99 + wave, lvz_fraction=0.5)
+    periods = np.geomspace(0.5, 50., 24)
+    ref = oracle.reference_solve(batch["thickness"], batch["vp"], batch["vs"], batch["rho"], periods, 5,
+                                 wave=wave, tol=1e-12)
+    case = dict(batch, periods=periods, nmodes=5, wave=wave, search_bounds=ref["search_bounds"])
+    for sp in (False, True):
+        assert_root_parity(ref, engine_solve64(case, sp), f"live wave={wave} fp32={sp}")
+
+
+def test_automatic_window_matches_reference_bounds():
+    """The engine's on-device window (no bounds passed) equals the reference's."""
+    from modisp_b200 import _native
+    g = load_golden("ref_crustal48_rayleigh")
+    h = g["thickness"]
+    o = _native.default_options()
+    e = _native.Engine(0, h.shape[0], h.shape[1], g["periods"].size, int(g["nmodes"]), o)
+    try:
+        out = e.run(h, g["vp"], g["vs"], g["rho"], g["periods"], None, ENGINE_TOL, 1., 0)
+    finally:
+        e.close()
+    np.testing.assert_array_equal(out["bounds"], g["search_bounds"])
+    assert_root_parity(g, out, "automatic window")
+
+
+def test_solver_api_end_to_end():
+    """modisp's public API on the engine: DispersionBatch fields and masks."""
+    import modisp_b200 as md
+    g = load_golden("ref_quickstart_rayleigh")
+    with md.Solver(accuracy="high", c_tol_rel=ENGINE_TOL, group_velocity=True) as s:
+        r = s(g["thickness"][0], g["vp"][0], g["vs"][0], g["rho"][0], g["periods"], nmodes=2)
+    assert r.backend_used == "cuda"
+    np.testing.assert_array_equal(r.mode_mask, np.isfinite(g["phase_velocity"]))
+    np.testing.assert_array_equal(r.root_count, g["root_count"])
+    np.testing.assert_array_equal(r.search_bounds, g["search_bounds"])
+    m = r.mode_mask
+    assert np.max(np.abs(r.phase_velocity[m] - g["phase_velocity"][m]) / g["phase_velocity"][m]) <= PHASE_RTOL
+    assert r.group_velocity_mask.sum() > 0
+    # unsorted periods are deduplicated and restored like the reference wrapper does
+    per = g["periods"][[5, 2, 2, 9]]
+    with md.Solver(accuracy="high", c_tol_rel=ENGINE_TOL) as s:
+        r2 = s(g["thickness"][0], g["vp"][0], g["vs"][0], g["rho"][0], per, nmodes=2)
+    np.testing.assert_allclose(r2.phase_velocity[0, :, 1], r2.phase_velocity[0, :, 2])
+    np.testing.assert_allclose(r2.phase_velocity[0, :, 0], r.phase_velocity[0, :, 5], rtol=1e-12)
+
+
+def test_review_groups_bridge():
+    import oracle
+    from modisp_b200 import plugin
+    g = load_golden("ref_quickstart_love")
+    f = 3
+    roots = g["phase_velocity"][0, :, f]
+    roots = roots[np.isfinite(roots)]
+    packed = np.concatenate([g[k][0] for k in ("thickness", "vp", "vs", "rho")] + [roots])
+    lo, hi = g["search_bounds"][0]
+    vel, flags, n = plugin._review_groups(packed, 2, 3, 1, 0, g["periods"][f], lo, hi, 1e-3, .005)
+    assert flags[2] == 1 and np.isnan(vel[2])
+    for m in range(2):
+        wl, wh, _ = oracle.group_windows(roots, lo, hi)
+        u = oracle.group(g["thickness"][0], g["vp"][0], g["vs"][0], g["rho"][0], g["periods"][f], roots[m],
+                         wl[m], wh[m], 1)
+        assert abs(vel[m] - u) / u < GROUP_RTOL
