@@ -1,0 +1,355 @@
+"""Benchmark: multimode Rayleigh + Love dispersion roots/s on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one "step"): the batched crustal configuration -- 10,000 seeded random
+models with 8-20 layers over a half-space (padded to 21 rows), 60 periods
+geomspaced 0.5-50 s, 5 modes, Rayleigh and Love, group velocity on -- solved to
+c_tol_rel 1e-10 (|dc|/c <= 1e-11, inside the 1e-9 parity bar).  Each rank solves
+its own batch (weak scaling; ranks exchange nothing but the timing reduction).
+
+Printed JSON (rank 0, one line):
+  value      roots/s of the FP32-scan / FP64-refinement engine, device-resident
+             inputs, CUDA events on the launching stream, L2 flushed between steps
+  e2e        the same metric through the plugin's QeSolver.run (C ABI host path,
+             host arrays, host<->device copies inside the timed region)
+  fp64       the plain FP64 engine on the same protocol (the denominator of the
+             FP32-scan speed-up)
+  roofline   the scan kernel's algorithmic FP32 flop rate against the measured
+             non-tensor FP32 FMA peak of this GPU
+  cpu_baseline  the reference CPU engine (oracle/_ref, built from the reference
+             sources) on a bounded sample of the same batch, all host cores
+--impl reference times that reference CPU engine alone (rank 0 only).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "roots/s at |dc/c|<=1e-9 (FP32-scan+FP64-refine engine; plain FP64 alongside)"
+TOL = 1e-10
+MODELS = 10_000
+WORKLOAD = "crustal batch: 10000 models x 8-20 layers, 60 periods 0.5-50 s, 5 modes, Rayleigh+Love, group velocity"
+# Algorithmic floating-point operations of one layer step of the secular
+# recurrences, counted from modisp_b200/csrc/secular.cuh (adds and multiplies
+# each 1, an FMA 2; the elementary functions counted separately: 2 rsqrt and
+# 2 sin/cos-or-exp per Rayleigh step, 1 rsqrt and 1 sin/cos-or-exp per Love step).
+FLOPS_PER_STEP = {0: 170, 1: 24}
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    p.add_argument("--models", type=int, default=MODELS)
+    p.add_argument("--cpu-sample", type=int, default=128, help="models in the CPU-baseline sample")
+    p.add_argument("--no-cpu", action="store_true")
+    return p.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    return rank, world, local
+
+
+def workload(rank, models):
+    from modisp_b200 import workloads
+    batch = workloads.crustal_batch(models, seed=workloads.SEED + 2 + 1000 * rank)
+    return batch, np.geomspace(0.5, 50., 60), 5
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    def __init__(self, index):
+        self.index, self.proc, self.lines = index, None, []
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in self.lines:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[4:8]):
+                if flag.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(batch, periods, nmodes, sample):
+    """The reference CPU engine (built from the reference sources) on a bounded sample."""
+    import oracle
+    ref = oracle.reference()
+    if ref is None:
+        return None
+    sub = {k: v[:sample] for k, v in batch.items()}
+    cores = len(os.sched_getaffinity(0))
+    threads = min(256, cores)
+    roots, elapsed = 0, 0.
+    for wave in (0, 1):
+        oracle.reference_solve(sub["thickness"][:4], sub["vp"][:4], sub["vs"][:4], sub["rho"][:4], periods, nmodes,
+                               wave=wave, tol=TOL, threads=threads, group_velocity=True)  # warm-up
+        t = time.perf_counter()
+        out = oracle.reference_solve(sub["thickness"], sub["vp"], sub["vs"], sub["rho"], periods, nmodes,
+                                     wave=wave, tol=TOL, threads=threads, group_velocity=True)
+        elapsed += time.perf_counter() - t
+        roots += int(np.isfinite(out["phase_velocity"]).sum())
+    return {"value": roots / elapsed, "unit": "roots/s", "cores": threads, "kind": "reference",
+            "sample": f"{sample} models of the same batch x 60 periods x 5 modes, Rayleigh+Love, group velocity, "
+                      f"accuracy=high shape-adaptive, c_tol_rel={TOL:g}; {roots} roots in {elapsed:.2f} s"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    batch, periods, nmodes = workload(0, args.models)
+    sample = args.cpu_sample
+    vals = []
+    for step in range(args.warmup + args.steps):
+        res = cpu_baseline(batch, periods, nmodes, sample)
+        if res is None:
+            print(json.dumps({"impl": "reference", "unavailable": "reference CPU engine not built (make -C oracle)"}))
+            return
+        if step >= args.warmup:
+            vals.append(res["value"])
+    value = statistics.median(vals)
+    line = {"metric": METRIC, "value": value, "unit": "roots/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "impl": "reference",
+            "config": {"workload": WORKLOAD, "models_per_step": sample, "periods": 60, "nmodes": 5,
+                       "c_tol_rel": TOL},
+            "cpu_baseline": {"value": value, "unit": "roots/s", "cores": res["cores"], "kind": "reference",
+                             "sample": res["sample"]},
+            "e2e": {"value": value, "unit": "roots/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def device_run(torch, eng, tens, B, wave, stream):
+    """Enqueue one engine run on device-resident tensors."""
+    eng.run_device(tens["h"].data_ptr(), tens["vp"].data_ptr(), tens["vs"].data_ptr(), tens["rho"].data_ptr(), B,
+                   tens["per"].data_ptr(), 0, TOL, 1., wave, tens["vel"][wave].data_ptr(),
+                   tens["flags"][wave].data_ptr(), tens["levels"][wave].data_ptr(), tens["counts"][wave].data_ptr(),
+                   tens["grp"][wave].data_ptr(), tens["gfl"][wave].data_ptr(), None, None,
+                   tens["stats"][wave].data_ptr(), stream)
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    import torch
+    from modisp_b200 import _native, plugin
+
+    torch.cuda.set_device(local)
+    # a dedicated stream: the engine's kernels and the timing events share it
+    work_stream = torch.cuda.Stream()
+    torch.cuda.set_stream(work_stream)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    batch, periods, nmodes = workload(rank, args.models)
+    B, L = batch["thickness"].shape
+    T = periods.size
+    dev = torch.device("cuda", local)
+    f64 = torch.float64
+    tens = {k: torch.tensor(batch[k], dtype=f64, device=dev) for k in ("thickness", "vp", "vs", "rho")}
+    tens = {"h": tens["thickness"], "vp": tens["vp"], "vs": tens["vs"], "rho": tens["rho"],
+            "per": torch.tensor(periods, dtype=f64, device=dev),
+            "vel": [torch.empty((B, nmodes, T), dtype=f64, device=dev) for _ in range(2)],
+            "grp": [torch.empty((B, nmodes, T), dtype=f64, device=dev) for _ in range(2)],
+            "gfl": [torch.empty((B, nmodes, T), dtype=torch.int32, device=dev) for _ in range(2)],
+            "flags": [torch.empty((B, T), dtype=torch.int32, device=dev) for _ in range(2)],
+            "levels": [torch.empty((B, T), dtype=torch.int32, device=dev) for _ in range(2)],
+            "counts": [torch.empty((B, T), dtype=torch.int32, device=dev) for _ in range(2)],
+            "stats": [torch.zeros(16, dtype=torch.int64, device=dev) for _ in range(2)]}
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # 256 MiB > 126 MB L2
+
+    def engine(single):
+        o = _native.default_options()
+        o.single_precision = int(single)
+        o.group_velocity = 1
+        return _native.Engine(local, B, L, T, nmodes, o)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    def timed(eng, steps, warmup):
+        stream = torch.cuda.current_stream().cuda_stream
+        for _ in range(warmup):
+            for wave in (0, 1):
+                device_run(torch, eng, tens, B, wave, stream)
+        barrier()
+        total = 0.
+        for _ in range(steps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            for wave in (0, 1):
+                device_run(torch, eng, tens, B, wave, stream)
+            b.record()
+            b.synchronize()
+            total += a.elapsed_time(b)
+        barrier()
+        roots = sum(int(torch.isfinite(tens["vel"][w]).sum()) for w in (0, 1))
+        return total, roots
+
+    def reduce_max(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    def reduce_sum(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t)
+        return float(t.item())
+
+    # ---- FP32-scan engine: the headline ----
+    e32 = engine(True)
+    with ClockSampler(local) as clocks:
+        ms32, roots32 = timed(e32, args.steps, args.warmup)
+    ms32 = reduce_max(ms32)
+    roots_all = reduce_sum(roots32)
+    value = roots_all * args.steps / (ms32 * 1e-3)
+    # per-stage device times of one more run per wave (scan kernel = dominant)
+    stream = torch.cuda.current_stream().cuda_stream
+    stage = {}
+    scan_flops = 0.
+    for wave in (0, 1):
+        flush.zero_()
+        device_run(torch, e32, tens, B, wave, stream)
+        st = e32.stage_times()
+        stats = tens["stats"][wave].cpu().numpy()
+        stage[wave] = st
+        scan_flops += float(stats[3]) * FLOPS_PER_STEP[wave]  # FP32 layer steps (scan kernel)
+    scan_ms = sum(stage[w]["scan"] for w in (0, 1))
+    launches = e32.kernel_launches() * 2 * args.steps
+    e32_stats = {w: tens["stats"][w].cpu().numpy().tolist() for w in (0, 1)}
+
+    # ---- plain FP64 engine ----
+    e64 = engine(False)
+    ms64, roots64 = timed(e64, max(2, args.steps // 2), 1)
+    ms64 = reduce_max(ms64)
+    value64 = reduce_sum(roots64) * max(2, args.steps // 2) / (ms64 * 1e-3)
+    e64.close()
+
+    # ---- end to end through the plugin (host arrays) ----
+    h2d = d2h = 0
+    e2e_value = None
+    if True:
+        solver = plugin.QeSolver(B, L, T, nmodes, 0, 0., .005, True, .001, 0, 1, 1, True, True, .001, False, 4,
+                                 device=local)
+        bounds = np.zeros((B, 2))
+        bounds[:, 1] = np.inf
+        host = [np.ascontiguousarray(batch[k]) for k in ("thickness", "vp", "vs", "rho")]
+        for _ in range(max(1, args.warmup - 1)):
+            for wave in (0, 1):
+                solver.run(*host, periods, bounds, TOL, 1., wave)
+        barrier()
+        t0 = time.perf_counter()
+        roots_e2e = 0
+        for _ in range(args.steps):
+            for wave in (0, 1):
+                out = solver.run(*host, periods, bounds, TOL, 1., wave)
+                roots_e2e += int(np.isfinite(out[0]).sum())
+        barrier()
+        wall = reduce_max(time.perf_counter() - t0)
+        e2e_value = reduce_sum(roots_e2e) / wall
+        per_wave_in = sum(a.nbytes for a in host) + periods.nbytes + bounds.nbytes
+        per_wave_out = B * nmodes * T * (8 + 8 + 4) + B * T * 4 * 3 + B * 16 + 16 * 8
+        h2d, d2h = 2 * per_wave_in, 2 * per_wave_out
+        solver.close()
+
+    peak32 = _native.measure_peak(local, fp64=False)
+    peak64 = _native.measure_peak(local, fp64=True)
+    achieved = scan_flops / (scan_ms * 1e-3)
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        cpu = cpu_baseline(batch, periods, nmodes, args.cpu_sample)
+    e32.close()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "roots/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms32 / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded crustal models)",
+            "config": {"workload": WORKLOAD, "models_per_gpu": B, "layers_padded": L, "periods": T, "nmodes": nmodes,
+                       "waves": ["rayleigh", "love"], "c_tol_rel": TOL, "l2": "flushed between steps (256 MiB write)",
+                       "parallelism": f"model-sharded x{world}"},
+            "fp64": {"value": value64, "unit": "roots/s", "ms_per_step": ms64 / max(2, args.steps // 2),
+                     "fp32_scan_speedup": value / value64},
+            "e2e": {"value": e2e_value, "unit": "roots/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "roofline": {"bound": "fp32-cuda-core", "kernel": "scan<float>", "achieved": achieved / 1e12,
+                         "peak": peak32 / 1e12, "unit": "TFLOP/s", "frac": achieved / peak32, "traffic": None,
+                         "peak_kind": "measured FMA throughput (md200_measure_peak), not MEASURED_PEAKS.json",
+                         "fp64_peak": peak64 / 1e12, "scan_ms_per_step": scan_ms,
+                         "stage_ms": {("rayleigh" if w == 0 else "love"): stage[w] for w in (0, 1)}},
+            "cpu_baseline": cpu,
+            "gpu_launches": launches,
+            "clocks": clocks.summary(),
+            "engine_stats": {"rayleigh": e32_stats[0], "love": e32_stats[1]},
+        }
+        print(json.dumps(line))
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -100,7 +100,7 @@ int md200_run(md200_engine *engine, const double *thickness, const double *vp, c
               int nstats);
 
 /* As md200_run, but every array is a device pointer and the work is enqueued on
- * `stream` (a cudaStream_t, or NULL for the engine's own stream) without a host
+ * `stream` (a cudaStream_t; NULL selects the engine's own stream) without a host
  * synchronisation.  stats, if given, is a device array of MD200_STAT_COUNT
  * counters. */
 int md200_run_device(md200_engine *engine, const double *thickness, const double *vp,
@@ -109,6 +109,16 @@ int md200_run_device(md200_engine *engine, const double *thickness, const double
                      double *velocity, unsigned *flags, int *levels, int *counts, double *group,
                      unsigned *group_flags, unsigned *prediction_flags, double *bounds_out,
                      unsigned long long *stats, void *stream);
+
+/* Device time (ms) of each stage of the engine's last run, from cudaEvent pairs
+ * recorded on the run's stream (the reference's profile timings,
+ * cpp/cuda/qe.cu:853-864): [0] model preparation, [1] trace list, [2] scan,
+ * [3] refinement, [4] repair selection, [5] FP64 re-scan, [6] re-scan
+ * refinement, [7] assembly, [8] group velocity.  Waits for the run to finish. */
+int md200_stage_times(md200_engine *engine, double *ms, int n);
+
+/* Number of kernel launches one md200_run of this engine enqueues. */
+int md200_kernel_launches(md200_engine *engine);
 
 /* Replaces QeSolver.close() (cpp/cuda/qe.cu:1039-1059). */
 void md200_destroy(md200_engine *engine);
@@ -126,6 +136,11 @@ int md200_device_name(int device, char *name, int length);
 /* Kernel attributes of the engine's kernels (cpp/cuda/qe.cu:1143-1164): writes a
  * JSON object describing registers, shared memory and occupancy to `json`. */
 int md200_kernel_report(int layers, int single_precision, char *json, int length);
+
+/* Measurement helper with no counterpart in the reference: sustained non-tensor
+ * FMA throughput of `device` in flop/s (FMA = 2), FP64 when fp64 != 0 else FP32
+ * -- the roofline denominator for the engine's CUDA-core kernels. */
+int md200_measure_peak(int device, int fp64, double *flops);
 
 /* Group velocities of one model's known ordered roots (guards included), for a
  * trace repaired outside the engine: replaces the plugin's _review_groups

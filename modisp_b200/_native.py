@@ -67,7 +67,12 @@ EXPORTS = {
     "md200_device_name": (_I, [_I, ctypes.c_char_p, _I]),
     "md200_kernel_report": (_I, [_I, _I, ctypes.c_char_p, _I]),
     "md200_group_roots": (_I, [_P, _P, _P, _P, _I, _I, _D, _P, _I, _I, _D, _P, _P]),
+    "md200_stage_times": (_I, [_P, ctypes.POINTER(ctypes.c_double), _I]),
+    "md200_kernel_launches": (_I, [_P]),
+    "md200_measure_peak": (_I, [_I, _I, ctypes.POINTER(ctypes.c_double)]),
 }
+STAGES = ("prep", "trace_list", "scan", "refine", "repair_select", "repair_scan", "repair_refine",
+          "assemble", "group_velocity")
 
 
 def lib():
@@ -158,15 +163,25 @@ class Engine:
     def run_device(self, h, vp, vs, rho, models, periods, bounds, tol, accept, wave, velocity, flags,
                    levels, counts, group=None, group_flags=None, prediction=None, bounds_out=None,
                    stats=None, stream=None):
-        """Device-pointer run (integer addresses), enqueued on `stream` (cudaStream_t address)."""
+        """Device-pointer run (integer addresses), enqueued on `stream` (a cudaStream_t
+        address; None selects the engine's own stream, 0 the legacy default stream)."""
         c = ctypes.c_void_p
         status = lib().md200_run_device(
             self.handle, c(h), c(vp), c(vs), c(rho), int(models), c(periods), c(bounds) if bounds else None,
             float(tol), float(accept), int(wave), c(velocity), c(flags), c(levels), c(counts),
             c(group) if group else None, c(group_flags) if group_flags else None,
             c(prediction) if prediction else None, c(bounds_out) if bounds_out else None,
-            c(stats) if stats else None, c(stream) if stream else None)
+            c(stats) if stats else None, c(stream) if stream is not None else None)
         check(status)
+
+    def stage_times(self) -> dict:
+        """Device milliseconds per stage of the last run (waits for it)."""
+        ms = (ctypes.c_double * len(STAGES))()
+        check(lib().md200_stage_times(self.handle, ms, len(STAGES)))
+        return dict(zip(STAGES, list(ms)))
+
+    def kernel_launches(self) -> int:
+        return int(lib().md200_kernel_launches(self.handle))
 
     def close(self):
         if getattr(self, "_handle", None):
@@ -202,6 +217,13 @@ def device_name(device: int = 0) -> str:
     buf = ctypes.create_string_buffer(256)
     check(lib().md200_device_name(int(device), buf, 256))
     return buf.value.decode()
+
+
+def measure_peak(device: int = 0, fp64: bool = False) -> float:
+    """Sustained FMA throughput of the device in flop/s (FP64 or FP32, non-tensor)."""
+    out = ctypes.c_double()
+    check(lib().md200_measure_peak(int(device), int(bool(fp64)), ctypes.byref(out)))
+    return float(out.value)
 
 
 def group_roots(h, vp, vs, rho, wave, period, roots, modes, close_rtol=.005):

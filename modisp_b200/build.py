@@ -30,7 +30,10 @@ def nvcc() -> str:
 
 
 def command(output: Path = LIBRARY, verbose_ptxas: bool = False) -> list[str]:
-    cmd = [nvcc(), ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
+    # single-precision division and square root as hardware approximations, and
+    # FP32 denormals flushed: the FP32 scan only decides signs (FP64 is untouched)
+    cmd = [nvcc(), ARCH, "-lineinfo", "-O3", "-std=c++17", "-prec-div=false", "-prec-sqrt=false", "-ftz=true",
+           "-Xcompiler", "-fPIC", "-shared",
            f"-I{ROOT / 'include'}", str(CSRC / "engine.cu"), "-o", str(output)]
     if verbose_ptxas:
         cmd.insert(1, "-Xptxas=-v")

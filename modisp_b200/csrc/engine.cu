@@ -13,7 +13,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/modisp_b200.h"
+#include "modisp_b200.h"
 #include "kernels.cuh"
 
 using namespace md200;
@@ -62,6 +62,10 @@ struct md200_engine {
   unsigned char *pinned = nullptr;
   size_t pinned_bytes = 0;
   std::vector<void *> owned;
+  // per-stage timing (cudaEvent pairs on the run's stream)
+  static constexpr int NSTAGE = 9;
+  cudaEvent_t ev[NSTAGE + 1] = {};
+  bool profiling = false;
 };
 
 namespace {
@@ -82,6 +86,8 @@ void release(md200_engine *e) {
   for (void *p : e->owned) cudaFree(p);
   e->owned.clear();
   if (e->pinned) cudaFreeHost(e->pinned);
+  for (auto &x : e->ev)
+    if (x) cudaEventDestroy(x);
   if (e->stream) cudaStreamDestroy(e->stream);
   cudaSetDevice(prev);
 }
@@ -112,6 +118,7 @@ int setup(md200_engine *e) {
   const size_t nt = static_cast<size_t>(B) * T;
   if (own_alloc(e, &d.mL, B) || own_alloc(e, &d.mwater, B) || own_alloc(e, &d.mstate, B) ||
       own_alloc(e, &d.mlo, B) || own_alloc(e, &d.mhi, B) || own_alloc(e, &d.malpha, B) ||
+      own_alloc(e, &d.mtail, 2 * static_cast<size_t>(B)) || own_alloc(e, &d.tail, 2 * nt) ||
       own_alloc(e, &d.layer64, static_cast<size_t>(B) * ROWS * d.Ls) ||
       own_alloc(e, &d.layer32, static_cast<size_t>(B) * ROWS * d.Ls) ||
       own_alloc(e, &d.knot, static_cast<size_t>(B) * d.nkmax) || own_alloc(e, &d.nknot, B) ||
@@ -145,14 +152,16 @@ int setup(md200_engine *e) {
   e->scan_warps = e->o.warps_per_block > 0 ? std::min(4, e->o.warps_per_block) : 4;
   e->scan_smem64 = scan_smem(e->scan_warps, d.Ls, sizeof(double));
   e->scan_smem32 = scan_smem(e->scan_warps, d.Ls, sizeof(float));
-  MD200_CK(cudaFuncSetAttribute(scan<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                static_cast<int>(std::max<size_t>(e->scan_smem64, 1024))));
-  MD200_CK(cudaFuncSetAttribute(scan<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                static_cast<int>(std::max<size_t>(e->scan_smem32, 1024))));
+  for (auto fn : {scan<double, 0>, scan<double, 1>})
+    MD200_CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(std::max<size_t>(e->scan_smem64, 1024))));
+  for (auto fn : {scan<float, 0>, scan<float, 1>})
+    MD200_CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(std::max<size_t>(e->scan_smem32, 1024))));
   int occ64 = 0, occ32 = 0;
-  MD200_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ64, scan<double>, 32 * e->scan_warps,
+  MD200_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ64, scan<double, 0>, 32 * e->scan_warps,
                                                          e->scan_smem64));
-  MD200_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ32, scan<float>, 32 * e->scan_warps,
+  MD200_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ32, scan<float, 0>, 32 * e->scan_warps,
                                                          e->scan_smem32));
   if (e->o.blocks_per_sm > 0) {
     occ64 = std::min(occ64, e->o.blocks_per_sm);
@@ -167,6 +176,7 @@ int setup(md200_engine *e) {
   e->sortcap = cap2;
   e->prep_warps = 4;
   e->prep_smem = static_cast<size_t>(e->prep_warps) * cap2 * (sizeof(double) + sizeof(int));
+  for (auto &x : e->ev) MD200_CK(cudaEventCreate(&x));
   MD200_CK(cudaFuncSetAttribute(prep_models, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(std::max<size_t>(e->prep_smem, 1024))));
   return 0;
@@ -213,35 +223,82 @@ int enqueue(md200_engine *e, const double *h, const double *vp, const double *vs
   const int nt = d.n_traces;
   MD200_CK(cudaMemsetAsync(d.ctr, 0, sizeof(int) * C_COUNT, s));
   if (stats) MD200_CK(cudaMemsetAsync(stats, 0, sizeof(unsigned long long) * MD200_STAT_COUNT, s));
+  // stage marks: 0 prep, 1 init, 2 scan, 3 refine, 4 repair collect, 5 repair scan,
+  // 6 repair refine, 7 assemble, 8 group (empty stages record back-to-back events)
+  auto mark = [&](int i) { return cudaEventRecord(e->ev[i], s); };
+  MD200_CK(mark(0));
   const int pw = e->prep_warps;
   prep_models<<<(B + pw - 1) / pw, 32 * pw, e->prep_smem, s>>>(d, e->sortcap, 0);
   MD200_CK(cudaGetLastError());
+  MD200_CK(mark(1));
   init_traces<<<(nt + 255) / 256, 256, 0, s>>>(d);
   MD200_CK(cudaGetLastError());
   if (d.fp32) {
-    scan<float><<<e->scan_blocks32, 32 * e->scan_warps, e->scan_smem32, s>>>(d, d.trace_list,
-                                                                            C_SCAN_CURSOR, C_NTRACE);
-  } else {
-    scan<double><<<e->scan_blocks64, 32 * e->scan_warps, e->scan_smem64, s>>>(d, d.trace_list,
-                                                                              C_SCAN_CURSOR, C_NTRACE);
-  }
-  MD200_CK(cudaGetLastError());
-  refine<<<e->list_blocks, 128, 0, s>>>(d);
-  MD200_CK(cudaGetLastError());
-  if (d.fp32) {
-    collect_repairs<<<(nt + 255) / 256, 256, 0, s>>>(d);
-    scan<double><<<e->scan_blocks64, 32 * e->scan_warps, e->scan_smem64, s>>>(d, d.repair_list,
-                                                                              C_REPAIR_CURSOR, C_NREPAIR);
-    refine<<<e->list_blocks, 128, 0, s>>>(d);
+    tail_values<<<(nt + 127) / 128, 128, 0, s>>>(d);
     MD200_CK(cudaGetLastError());
   }
+  MD200_CK(mark(2));
+  {
+    const dim3 grid(d.fp32 ? e->scan_blocks32 : e->scan_blocks64), block(32 * e->scan_warps);
+    const size_t sm = d.fp32 ? e->scan_smem32 : e->scan_smem64;
+    if (d.fp32 && wave == 0) scan<float, 0><<<grid, block, sm, s>>>(d, d.trace_list, C_SCAN_CURSOR, C_NTRACE);
+    else if (d.fp32) scan<float, 1><<<grid, block, sm, s>>>(d, d.trace_list, C_SCAN_CURSOR, C_NTRACE);
+    else if (wave == 0) scan<double, 0><<<grid, block, sm, s>>>(d, d.trace_list, C_SCAN_CURSOR, C_NTRACE);
+    else scan<double, 1><<<grid, block, sm, s>>>(d, d.trace_list, C_SCAN_CURSOR, C_NTRACE);
+  }
+  MD200_CK(cudaGetLastError());
+  MD200_CK(mark(3));
+  refine<<<e->list_blocks, 128, 0, s>>>(d);
+  MD200_CK(cudaGetLastError());
+  MD200_CK(mark(4));
+  if (d.fp32) {
+    collect_repairs<<<(nt + 255) / 256, 256, 0, s>>>(d);
+    MD200_CK(mark(5));
+    if (wave == 0)
+      scan<double, 0><<<e->scan_blocks64, 32 * e->scan_warps, e->scan_smem64, s>>>(d, d.repair_list,
+                                                                                 C_REPAIR_CURSOR, C_NREPAIR);
+    else
+      scan<double, 1><<<e->scan_blocks64, 32 * e->scan_warps, e->scan_smem64, s>>>(d, d.repair_list,
+                                                                                 C_REPAIR_CURSOR, C_NREPAIR);
+    MD200_CK(mark(6));
+    refine<<<e->list_blocks, 128, 0, s>>>(d);
+    MD200_CK(cudaGetLastError());
+  } else {
+    MD200_CK(mark(5));
+    MD200_CK(mark(6));
+  }
+  MD200_CK(mark(7));
   assemble<<<(nt + 255) / 256, 256, 0, s>>>(d);
   MD200_CK(cudaGetLastError());
+  MD200_CK(mark(8));
   if (d.group) {
     group_velocity<<<e->list_blocks, 128, 0, s>>>(d);
     MD200_CK(cudaGetLastError());
   }
+  MD200_CK(mark(9));
+  e->profiling = true;
   return 0;
+}
+
+}  // namespace
+
+namespace {
+// Sustained non-tensor FMA throughput (flop/s, an FMA counted as 2): 8 independent
+// dependent-FMA chains per thread over every SM; the roofline denominator of the
+// scan and refinement kernels.
+template <class T>
+__global__ void fma_chains(T *out, int iters, T a, T b) {
+  T x[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) x[j] = static_cast<T>(threadIdx.x + j);
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) x[j] = fma(x[j], a, b);
+  }
+  T sum = 0;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) sum += x[j];
+  if (sum == static_cast<T>(-1.2345)) out[0] = sum;  // keeps the chains live
 }
 
 }  // namespace
@@ -382,6 +439,22 @@ int md200_run(md200_engine *e, const double *h, const double *vp, const double *
   return 0;
 }
 
+int md200_stage_times(md200_engine *e, double *ms, int n) {
+  if (!e || !e->profiling) return fail("modisp_b200: no run to report");
+  MD200_CK(cudaEventSynchronize(e->ev[md200_engine::NSTAGE]));
+  for (int i = 0; i < n && i < md200_engine::NSTAGE; ++i) {
+    float t = 0.f;
+    MD200_CK(cudaEventElapsedTime(&t, e->ev[i], e->ev[i + 1]));
+    ms[i] = t;
+  }
+  return 0;
+}
+
+int md200_kernel_launches(md200_engine *e) {
+  if (!e) return -1;
+  return 6 + (e->d.fp32 ? 4 : 0) - (e->d.group ? 0 : 1);
+}
+
 void md200_destroy(md200_engine *e) {
   if (!e) return;
   release(e);
@@ -434,8 +507,10 @@ int md200_kernel_report(int layers, int single_precision, char *json, int length
   };
   const Entry entries[] = {
       {"prep_models", reinterpret_cast<const void *>(prep_models)},
-      {"scan_fp64", reinterpret_cast<const void *>(scan<double>)},
-      {"scan_fp32", reinterpret_cast<const void *>(scan<float>)},
+      {"scan_fp64", reinterpret_cast<const void *>(scan<double, 0>)},
+      {"scan_fp32", reinterpret_cast<const void *>(scan<float, 0>)},
+      {"scan_fp64_love", reinterpret_cast<const void *>(scan<double, 1>)},
+      {"scan_fp32_love", reinterpret_cast<const void *>(scan<float, 1>)},
       {"refine", reinterpret_cast<const void *>(refine)},
       {"assemble", reinterpret_cast<const void *>(assemble)},
       {"group_velocity", reinterpret_cast<const void *>(group_velocity)},
@@ -510,6 +585,36 @@ int md200_group_roots(const double *h, const double *vp, const double *vs, const
   cudaFree(dgrp);
   cudaFree(dfl);
   if (err != cudaSuccess) return fail(std::string("modisp_b200 CUDA: ") + cudaGetErrorString(err));
+  return 0;
+}
+
+int md200_measure_peak(int device, int fp64, double *flops) {
+  MD200_CK(cudaSetDevice(device));
+  int sms = 0;
+  MD200_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  void *out = nullptr;
+  MD200_CK(cudaMalloc(&out, 64));
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  const int blocks = sms * 8, threads = 256, iters = fp64 ? 4096 : 16384;
+  float best = 1e30f;
+  for (int rep = 0; rep < 4; ++rep) {
+    cudaEventRecord(a);
+    if (fp64) fma_chains<double><<<blocks, threads>>>(static_cast<double *>(out), iters, 0.999999, 1e-7);
+    else fma_chains<float><<<blocks, threads>>>(static_cast<float *>(out), iters, 0.999999f, 1e-7f);
+    cudaEventRecord(b);
+    cudaEventSynchronize(b);
+    float t = 0.f;
+    cudaEventElapsedTime(&t, a, b);
+    if (rep) best = std::min(best, t);  // the first launch warms up
+  }
+  const cudaError_t err = cudaGetLastError();
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(out);
+  if (err != cudaSuccess) return fail(std::string("modisp_b200 CUDA: ") + cudaGetErrorString(err));
+  *flops = 2.0 * 8.0 * iters * static_cast<double>(blocks) * threads / (best * 1e-3);
   return 0;
 }
 

@@ -54,6 +54,9 @@ struct Dev {
   // prepared models
   int *mL, *mwater, *mstate;
   double *mlo, *mhi, *malpha;
+  double *mtail;    // [B][2]: the two near-cutoff sample positions every scan that
+                    // reaches the window end evaluates (hi, and vs_hs (1 - 1e-7))
+  double4 *tail;    // [n_traces][2]: FP64 (c, F, g, log-magnitude) at those positions
   double *layer64;  // [B][ROWS][Ls]
   float *layer32;   // [B][ROWS][Ls]
   double4 *knot;    // [B][nkmax]: c, N(c), ln c, kink part of N over [c_i, c_i+1]

@@ -57,16 +57,22 @@ __device__ __forceinline__ const float *layer_table<float>(const Dev &d, int b) 
 template <class T>
 __device__ __forceinline__ LayerView<T> make_view(const T *tab, int Ls, int L, int water) {
   LayerView<T> v;
-  v.h = tab;
-  v.ivp = tab + Ls;
-  v.ivs = tab + 2 * Ls;
-  v.vs2 = tab + 3 * Ls;
-  v.rho = tab + 4 * Ls;
-  v.irho = tab + 5 * Ls;
-  v.imu = tab + 6 * Ls;
+  v.base = tab;
+  v.Ls = Ls;
   v.L = L;
   v.water = water;
   return v;
+}
+
+// Out-of-line secular evaluation for the scan: the scan's bookkeeping is saved
+// once per 32-sample step around the call instead of competing with the layer
+// recurrence for registers.
+template <class T, int WAVE, int S>
+__device__ __noinline__ void scan_eval(const LayerView<T> view, T w, const T *c, T *F, T *g, T *lm) {
+  T k[S];
+#pragma unroll
+  for (int s = 0; s < S; ++s) k[s] = w / c[s];
+  secular_multi<T, T, S, WAVE>(view, k, w, F, g, lm);
 }
 
 // Layer recurrence steps of one evaluation.
@@ -243,6 +249,8 @@ __global__ void prep_models(Dev d, int sortcap, int automatic) {
     d.mstate[b] = state;
     d.mlo[b] = lo;
     d.mhi[b] = hi;
+    d.mtail[2 * b] = hi;
+    d.mtail[2 * b + 1] = vsr[L - 1] * (1. + -1 * 1e-7);  // the -1e-7 seed of the half-space row
     if (d.bounds_out) {
       d.bounds_out[2 * b] = lo;
       d.bounds_out[2 * b + 1] = hi;
@@ -422,6 +430,26 @@ __global__ void init_traces(Dev d) {
   }
 }
 
+// FP64 values at the two near-cutoff positions of every trace, for the FP32
+// scan (one thread per trace, all lanes busy): near the half-space cutoff the
+// start vector depends on the small radical sqrt(k^2 - kb^2) directly, which
+// single precision resolves poorly.
+__global__ void tail_values(Dev d) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= *(volatile int *)&d.ctr[C_NTRACE]) return;
+  const int t = d.trace_list[q];
+  const int b = t / d.T, f = t - b * d.T;
+  const double w = TWO_PI / d.periods[f];
+  const LayerView<double> m = make_view<double>(d.layer64 + static_cast<size_t>(b) * ROWS * d.Ls, d.Ls,
+                                                d.mL[b], d.mwater[b]);
+  for (int i = 0; i < 2; ++i) {
+    const double c = d.mtail[2 * b + i];
+    double g = 0., lm = 0., F = NAN;
+    if (c > d.mlo[b]) F = secular<double, double>(m, d.wave, w / c, w, &g, &lm);
+    d.tail[2 * static_cast<size_t>(t) + i] = make_double4(c, F, g, lm);
+  }
+}
+
 // Position of scan point j (1 <= j <= J) of a trace: invert
 // u(c) = f N(c) + alpha ln c at u_lo + j / density through the knot table.  In
 // an interval that starts at a body velocity the kink term grows like
@@ -437,14 +465,15 @@ __device__ __forceinline__ double scan_point(const double4 *kt, int nk, double f
   }
   const double4 q0 = kt[lo], q1 = kt[hi];
   const double u0 = fma(f, q0.y, alpha * q0.z), u1 = fma(f, q1.y, alpha * q1.z);
-  const double dt = fmax(0., target - u0), du = u1 - u0;
-  const double a = f * q0.w, bs = fmax(0., du - a);
-  double s = 0.;
-  if (du > 0. && dt > 0.) {  // (dt = 0 would give 0/0 where the interval has no kink)
-    const double x = 2. * dt / (a + sqrt(a * a + 4. * bs * dt));
-    s = fmin(1., x * x);
+  // the fractional position within the knot interval needs only single precision
+  const float dt = static_cast<float>(fmax(0., target - u0)), du = static_cast<float>(u1 - u0);
+  const float a = static_cast<float>(f * q0.w), bs = fmaxf(0.f, du - a);
+  float s = 0.f;
+  if (du > 0.f && dt > 0.f) {  // (dt = 0 would give 0/0 where the interval has no kink)
+    const float x = 2.f * dt / (a + sqrtf(a * a + 4.f * bs * dt));
+    s = fminf(1.f, x * x);
   }
-  return fma(q1.x - q0.x, s, q0.x);
+  return fma(q1.x - q0.x, static_cast<double>(s), q0.x);
 }
 
 // Index (0..32) of the first lane whose sorted value is >= x (or > x when
@@ -486,15 +515,19 @@ __device__ __forceinline__ void put_bracket(double *slot, int r, double lo, doub
 // is kept when a V with its vertex on zero fits the samples -- the linear
 // extension of either flank reaches zero before the far neighbour -- or when a
 // parabola through the three samples dips to zero.
-__device__ __forceinline__ bool trough_may_hide_roots(double x0, double x1, double x2, double u, double v,
-                                                      double z) {
-  if (!(v < u && v < z) || !(x0 < x1 && x1 < x2)) return false;
-  const double sl = (u - v) / (x1 - x0), sr = (z - v) / (x2 - x1);  // flank steepness (> 0)
-  if (x1 + v / sl < x2 + .25 * (x2 - x1) || x1 - v / sr > x0 - .25 * (x1 - x0)) return true;
-  const double d1 = -sl, d2 = sr, a2 = (d2 - d1) / (x2 - x0);
-  if (a2 > 0.) {
-    const double xs = .5 * (x0 + x1) - d1 / (2. * a2);
-    if (u + d1 * (xs - x0) + a2 * (xs - x0) * (xs - x1) <= 0.) return true;
+__device__ __forceinline__ bool trough_may_hide_roots(double x0, double x1, double x2, float u, float v, float z,
+                                                      float noise = 1e-7f) {
+  // both flanks must rise by more than the evaluation's rounding noise
+  if (!(v + noise < u && v + noise < z) || !(x0 < x1 && x1 < x2)) return false;
+  // single precision suffices for the slope test: spacings are differences of
+  // exact positions, well above float resolution
+  const float h0 = static_cast<float>(x1 - x0), h1 = static_cast<float>(x2 - x1);
+  const float sl = (u - v) / h0, sr = (z - v) / h1;  // flank steepness (> 0)
+  if (v / sl < 1.25f * h1 || v / sr < 1.25f * h0) return true;
+  const float d1 = -sl, d2 = sr, a2 = (d2 - d1) / (h0 + h1);
+  if (a2 > 0.f) {
+    const float xs = .5f * h0 - d1 / (2.f * a2);  // vertex offset from x0
+    if (u + d1 * xs + a2 * xs * (xs - h0) <= 0.f) return true;
   }
   return false;
 }
@@ -503,10 +536,9 @@ __device__ __forceinline__ bool trough_may_hide_roots(double x0, double x1, doub
 // of its neighbours: large where the whole unnormalised vector nearly vanishes,
 // which hides a root pair even where the shape feature stays smooth.
 constexpr double MDIP = 0.5;
-__device__ __forceinline__ double magnitude_dip(double x0, double x1, double x2, double m0, double m1,
-                                                double m2) {
-  if (!(x0 < x1 && x1 < x2) || !(m1 < m0 && m1 < m2)) return 0.;
-  const double t = (x1 - x0) / (x2 - x0);
+__device__ __forceinline__ float magnitude_dip(double x0, double x1, double x2, float m0, float m1, float m2) {
+  if (!(x0 < x1 && x1 < x2) || !(m1 < m0 && m1 < m2)) return 0.f;
+  const float t = static_cast<float>((x1 - x0) / (x2 - x0));
   return m0 + t * (m2 - m0) - m1;
 }
 
@@ -515,7 +547,8 @@ __device__ __forceinline__ double magnitude_dip(double x0, double x1, double x2,
 // (appended in order, FP64 values known); otherwise the window shrinks 16.5x
 // around the smallest s*g until the minimum is resolved above zero or the
 // window reaches the refinement width.  `sa`, `sb` are s*g at a and b.
-__device__ __noinline__ int zoom_trough(const LayerView<double> &m, int wave, double w, double a, double b,
+template <int WAVE>
+__device__ __noinline__ int zoom_trough(const LayerView<double> &m, double w, double a, double b,
                                        double sa, double sb, double ma, double mb, double sgn, int mode,
                                        double tol, double *slot, int nbr, int K, int lane,
                                        unsigned long long &evals) {
@@ -526,7 +559,7 @@ __device__ __noinline__ int zoom_trough(const LayerView<double> &m, int wave, do
     if (!(width > fmax(4e-15 * b, .125 * tol * b))) break;
     const double x = a + width * (lane + 1) * (1. / 33.);
     double g, lm;
-    const double F = secular<double, double>(m, wave, w / x, w, &g, &lm);
+    const double F = secular<double, double>(m, WAVE, w / x, w, &g, &lm);
     evals += 32;
     const bool opp = signbit(F) != neg;
     const unsigned om = __ballot_sync(FULL, opp);
@@ -577,23 +610,96 @@ __device__ __noinline__ int zoom_trough(const LayerView<double> &m, int wave, do
   return nbr;
 }
 
+// Single-precision screen of a trough window, run before the FP64 zoom in the
+// FP32 scan: up to two 32-point steps in FP32 (the model table in shared
+// memory).  Returns true when the window is dismissed -- no sample changes sign
+// or comes near zero (|g| <= 2e-4), and the lowest sample no longer admits a
+// hidden pair -- so only troughs that stay suspicious pay for FP64.
+template <int WAVE>
+__device__ __noinline__ bool screen_trough32(const LayerView<float> &m, float w, double a, double b, double sa,
+                                             double sb, double ma, double mb, double sgn, int mode, int lane,
+                                             unsigned long long &evals) {
+  const bool neg = sgn < 0.;
+  for (int it = 0; it < 2; ++it) {
+    const double width = b - a;
+    if (!(width > 1e-5 * b)) return false;  // below single-precision resolution
+    const double x = a + width * (lane + 1) * (1. / 33.);
+    const float x32 = static_cast<float>(x);
+    float g, lm;
+    const float F = secular<float, float>(m, WAVE, w / x32, w, &g, &lm);
+    evals += 32;
+    const bool doubt = signbit(F) != neg || !(fabsf(g) > 2e-4f) || !isfinite(F);
+    if (__any_sync(FULL, doubt)) return false;
+    const double v = sgn * g;
+    const double key = mode ? lm : v;
+    double best = key;
+    int arg = lane;
+    for (int o = 16; o; o >>= 1) {
+      const double ob = __shfl_xor_sync(FULL, best, o);
+      const int oa = __shfl_xor_sync(FULL, arg, o);
+      if (ob < best || (ob == best && oa < arg)) { best = ob; arg = oa; }
+    }
+    const int il = (arg - 1) & 31, ir = (arg + 1) & 31;
+    const double vl = arg ? __shfl_sync(FULL, v, il) : sa, vr = arg < 31 ? __shfl_sync(FULL, v, ir) : sb;
+    const double ml = arg ? __shfl_sync(FULL, static_cast<double>(lm), il) : ma;
+    const double mr = arg < 31 ? __shfl_sync(FULL, static_cast<double>(lm), ir) : mb;
+    const double xlo = arg ? __shfl_sync(FULL, x, il) : a, xhi = arg < 31 ? __shfl_sync(FULL, x, ir) : b;
+    const double xm = __shfl_sync(FULL, x, arg);
+    const bool go = mode ? magnitude_dip(xlo, xm, xhi, ml, __shfl_sync(FULL, static_cast<double>(lm), arg), mr) > MDIP
+                         : trough_may_hide_roots(xlo, xm, xhi, vl, __shfl_sync(FULL, v, arg), vr, 1e-5f);
+    if (!go) return true;
+    a = xlo; b = xhi; sa = vl; sb = vr; ma = ml; mb = mr;
+  }
+  return false;
+}
+
 // ---------------------------------------------------------------------------
-// scan<T>: persistent, one warp per trace.
+// scan<T, WAVE>: persistent, one warp per trace.
 // Shared memory per warp: EVAL_ROWS * Ls values of T (model table) + 32 doubles
 // (merge buffer).
+//
+// Trough tests look only at "regular" samples -- a sample within 1e-6 of its
+// left neighbour (the +-1e-7 seeds that straddle a body velocity, where the
+// shape feature has a square-root kink) takes part in sign-change bracketing
+// but not in slope estimates -- and a trough window must lie inside one sign
+// segment (no sign change anywhere between its ends), so a zoom never revisits
+// a root the brackets already hold.
 // ---------------------------------------------------------------------------
-template <class T>
-__global__ void __launch_bounds__(128) scan(Dev d, const int *list, int cursor_id, int count_id) {
+// A sample as the trough tests see it: position, shape feature and log-magnitude
+// (single precision suffices for slopes and dips), sign segment and sign.
+struct Sample {
+  double c;
+  float g, M;
+  int seg;  // running sign-change count, with the sign of F in bit 30
+};
+
+__device__ __forceinline__ Sample shfl_sample(const Sample &s, int src) {
+  Sample r;
+  r.c = __shfl_sync(FULL, s.c, src);
+  r.g = __shfl_sync(FULL, s.g, src);
+  r.M = __shfl_sync(FULL, s.M, src);
+  r.seg = __shfl_sync(FULL, s.seg, src);
+  return r;
+}
+__device__ __forceinline__ double sample_sign(const Sample &s) { return (s.seg >> 30) & 1 ? -1. : 1.; }
+__device__ __forceinline__ int sample_segment(const Sample &s) { return s.seg & 0x3fffffff; }
+
+#ifndef MD200_SCAN_MIN_BLOCKS
+#define MD200_SCAN_MIN_BLOCKS 4
+#endif
+template <class T, int WAVE>
+__global__ void __launch_bounds__(128, MD200_SCAN_MIN_BLOCKS) scan(Dev d, const int *list, int cursor_id, int count_id) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const size_t tab_bytes = (static_cast<size_t>(EVAL_ROWS) * d.Ls * sizeof(T) + 15) & ~size_t(15);
   unsigned char *mine = smem_raw + static_cast<size_t>(wib) * (tab_bytes + 32 * sizeof(double));
   T *tab = reinterpret_cast<T *>(mine);
   double *mbuf = reinterpret_cast<double *>(mine + tab_bytes);
-  unsigned long long evals = 0, evals32 = 0, steps = 0, steps32 = 0, brackets = 0, zooms = 0;
-  const int K = d.K, wave = d.wave;
+  unsigned long long evals = 0, evals32 = 0, steps = 0, steps32 = 0, zooms = 0;
+  const int K = d.K;
   const double density = d.density, step = 1. / density;
   constexpr bool single = sizeof(T) == 4;
+  const unsigned lt = lanemask_lt(), le = lt | (1u << lane);
 
   for (;;) {
     int q = 0;
@@ -616,8 +722,8 @@ __global__ void __launch_bounds__(128) scan(Dev d, const int *list, int cursor_i
       __syncwarp();
     }
     const LayerView<T> view = make_view<T>(tab, d.Ls, L, water);
-    // FP64 view for zooms and uncertain FP32 samples: shared memory in the FP64
-    // kernel, global memory (L1/L2-resident) in the FP32 kernel
+    // FP64 view for zooms and FP64 samples of the single-precision scan (global
+    // memory, L1/L2-resident); the FP64 scan reads its shared-memory copy
     LayerView<double> view64;
     if constexpr (single) view64 = global_view(d, b);
     else view64 = *reinterpret_cast<const LayerView<double> *>(&view);
@@ -638,153 +744,227 @@ __global__ void __launch_bounds__(128) scan(Dev d, const int *list, int cursor_i
     const int ns = d.nseed[b];
     const double hi = d.mhi[b];
     double *slot = d.slot + static_cast<size_t>(t) * d.KB * SLOT;
+    const double4 *tail = d.tail + 2 * static_cast<size_t>(t);
 
     long long gi = 1;
-    int si = 0, nbr = 0;
-    bool have1 = false, have2 = false;
+    int si = 0, nbr = 0, nseg = 0;
+    // carries: the last element (for bracketing) and the last two regular elements
+    bool have1 = false, hr1 = false, hr2 = false, ex1 = false;
+    double c1 = 0., F1 = 0.;
+    Sample R1{0., 0.f, 0.f, 0}, R2{0., 0.f, 0.f, 0};
     double zoom_right = -INFINITY;  // right end of the last zoomed window (windows never overlap)
-    double c1 = 0., F1 = 0., g1 = 0., M1 = 0., c2 = 0., g2 = 0., F2 = 0., M2 = 0.;  // elements -1, -2
-    while (nbr < K) {
-      // ---- next 32 sample positions: merge scan points and seeds ----
-      const long long gj = gi + lane;
-      const double gv = gj <= J ? scan_point(kt, nk, fr, alpha, u_lo + static_cast<double>(gj) * step)
-                                : INFINITY;
-      const double sv = si + lane < ns ? sd[si + lane] : INFINITY;
-      const int rg = warp_rank(sv, gv, false);  // seeds strictly below this scan point
-      const int rs = warp_rank(gv, sv, true);   // scan points at or below this seed
-      const int pg = lane + rg, ps = lane + rs;
-      mbuf[lane] = INFINITY;
-      __syncwarp();
-      if (pg < 32) mbuf[pg] = gv;
-      if (ps < 32) mbuf[ps] = sv;
-      __syncwarp();
-      double c = mbuf[lane];
-      __syncwarp();
-      gi += __popc(__ballot_sync(FULL, pg < 32 && gv < INFINITY));
-      si += __popc(__ballot_sync(FULL, ps < 32 && sv < INFINITY));
-      const bool valid = c < INFINITY;
-      const unsigned vmask = __ballot_sync(FULL, valid);
-      if (!vmask) break;
-      const int nvalid = __popc(vmask);
+    // one 32-sample step per iteration (S > 1 interleaves S independent
+    // recurrences per lane; measured slower on B200: instruction-cache bound)
+    constexpr int S = 1;
+    bool finished = false;
+    while (nbr < K && !finished) {
+      // ---- next S x 32 sample positions: merge scan points and seeds ----
+      double cs[S];
+      unsigned vm[S];
+#pragma unroll
+      for (int h = 0; h < S; ++h) {
+        const long long gj = gi + lane;
+        const double gv = gj <= J ? scan_point(kt, nk, fr, alpha, u_lo + static_cast<double>(gj) * step)
+                                  : INFINITY;
+        const double sv = si + lane < ns ? sd[si + lane] : INFINITY;
+        const int rg = warp_rank(sv, gv, false);  // seeds strictly below this scan point
+        const int rs = warp_rank(gv, sv, true);   // scan points at or below this seed
+        const int pg = lane + rg, ps = lane + rs;
+        mbuf[lane] = INFINITY;
+        __syncwarp();
+        if (pg < 32) mbuf[pg] = gv;
+        if (ps < 32) mbuf[ps] = sv;
+        __syncwarp();
+        cs[h] = mbuf[lane];
+        __syncwarp();
+        gi += __popc(__ballot_sync(FULL, pg < 32 && gv < INFINITY));
+        si += __popc(__ballot_sync(FULL, ps < 32 && sv < INFINITY));
+        vm[h] = __ballot_sync(FULL, cs[h] < INFINITY);
+      }
+      if (!vm[0]) break;
 
-      // ---- secular value, shape feature and log-magnitude ----
-      double F = 0., g = 0., M = 0.;
-      bool exact = !single;  // value known in FP64
-      // near the half-space cutoff the start vector depends on the small radical
-      // sqrt(k^2 - kb^2) directly, which single precision resolves poorly: those
-      // samples are evaluated in FP64 only, at their exact positions
-      const bool near_cut = single && valid && c >= hi * (1. - 2e-3);
-      if (valid) {
-        if constexpr (single) {
-          float c32 = static_cast<float>(c);
-          if (static_cast<double>(c32) > hi) c32 = nextafterf(c32, 0.f);
-          if (!near_cut) c = static_cast<double>(c32);
-          float gg, mm;
-          const float w32 = static_cast<float>(w);
-          F = secular<float, float>(view, wave, w32 / c32, w32, &gg, &mm);
-          g = gg;
-          M = mm;
-        } else {
-          F = secular<double, double>(view, wave, w / c, w, &g, &M);
-        }
-      }
-      evals += nvalid;
-      steps += static_cast<unsigned long long>(nvalid) * nsteps;
+      // ---- secular values, shape features and log-magnitudes ----
+      double Fs[S], gs[S], Ms[S];
+      bool exs[S];
       if constexpr (single) {
-        evals32 += nvalid;
-        steps32 += static_cast<unsigned long long>(nvalid) * nsteps;
-        // sign-uncertain single-precision samples (small |g|) and the near-cutoff
-        // band are evaluated in FP64
-        const bool redo = valid && (!(fabs(g) > 2e-4) || near_cut);
-        const unsigned rm = __ballot_sync(FULL, redo);
-        if (rm) {
-          if (redo) {
-            F = eval64_outline(view64, wave, w, c, &g, &M);
-            exact = true;
-          }
-          evals += __popc(rm);
-          steps += static_cast<unsigned long long>(__popc(rm)) * nsteps;
+        float c32[S], F32[S], g32[S], M32[S];
+        bool near_cut[S];
+#pragma unroll
+        for (int h = 0; h < S; ++h) {
+          const bool valid = cs[h] < INFINITY;
+          // near the half-space cutoff the start vector depends on the small radical
+          // sqrt(k^2 - kb^2) directly, which single precision resolves poorly: those
+          // samples are evaluated in FP64 only, at their exact positions
+          near_cut[h] = valid && cs[h] >= hi * (1. - 1e-4);
+          float x = valid ? static_cast<float>(cs[h]) : 1.f;
+          if (valid && static_cast<double>(x) > hi) x = nextafterf(x, 0.f);
+          if (valid && !near_cut[h]) cs[h] = static_cast<double>(x);
+          c32[h] = x;
         }
-      }
-      if (__any_sync(FULL, valid && !(isfinite(F) && isfinite(g)))) {
-        tfl |= TRACE_NONFINITE | TRACE_SEARCH_UNCONVERGED;
-        break;
-      }
-      // ---- neighbours (elements i-1 and i-2) ----
-      double cl = __shfl_up_sync(FULL, c, 1), Fl = __shfl_up_sync(FULL, F, 1),
-             gl = __shfl_up_sync(FULL, g, 1);
-      double cll = __shfl_up_sync(FULL, c, 2), Fll = __shfl_up_sync(FULL, F, 2),
-             gll = __shfl_up_sync(FULL, g, 2);
-      double Ml = __shfl_up_sync(FULL, M, 1), Mll = __shfl_up_sync(FULL, M, 2);
-      bool exl = __shfl_up_sync(FULL, exact, 1);
-      const bool vl = lane >= 1 ? lane - 1 < nvalid : have1;
-      const bool vll = lane >= 2 ? lane - 2 < nvalid : (lane == 1 ? have1 : have2);
-      if (lane == 0) {
-        cl = c1; Fl = F1; gl = g1; Ml = M1;
-        cll = c2; Fll = F2; gll = g2; Mll = M2;
-        exl = false;
-      } else if (lane == 1) {
-        cll = c1; Fll = F1; gll = g1; Mll = M1;
-      }
-      // ---- events: sign changes (a +0 counts as positive) and same-sign troughs ----
-      const bool sc = valid && vl && (signbit(Fl) != signbit(F));
-      bool tr = false, trm_ = false;
-      if (valid && vl && vll && signbit(Fll) == signbit(Fl) && signbit(Fl) == signbit(F)) {
-        const double sgn = signbit(Fl) ? -1. : 1.;
-        tr = trough_may_hide_roots(cll, cl, c, sgn * gll, sgn * gl, sgn * g);
-        if (!tr) trm_ = magnitude_dip(cll, cl, c, Mll, Ml, M) > MDIP;
-        tr = tr || trm_;
-      }
-      const unsigned scm = __ballot_sync(FULL, sc), trm = __ballot_sync(FULL, tr);
-      const unsigned mmode = __ballot_sync(FULL, trm_);
-      unsigned events = scm | trm;
-      while (events && nbr < K) {
-        const int i = __ffs(events) - 1;
-        events &= events - 1;
-        if ((scm >> i) & 1u) {
-          if (lane == i) put_bracket(slot, nbr, cl, c, exl ? Fl : NAN, exact ? F : NAN);
-          ++nbr;
-          ++brackets;
-        } else {
-          double x0 = __shfl_sync(FULL, cll, i);
-          const double x2 = __shfl_sync(FULL, c, i);
-          const double sgn = signbit(__shfl_sync(FULL, Fl, i)) ? -1. : 1.;
-          double sa = sgn * __shfl_sync(FULL, gll, i);
-          const double sb = sgn * __shfl_sync(FULL, g, i);
-          double ma = __shfl_sync(FULL, Mll, i);
-          const double mb = __shfl_sync(FULL, M, i);
-          if (x0 < zoom_right) {  // overlaps the previous window: start at its middle sample
-            x0 = __shfl_sync(FULL, cl, i);
-            sa = sgn * __shfl_sync(FULL, gl, i);
-            ma = __shfl_sync(FULL, Ml, i);
+        scan_eval<float, WAVE, S>(view, static_cast<float>(w), c32, F32, g32, M32);
+#pragma unroll
+        for (int h = 0; h < S; ++h) {
+          const bool valid = cs[h] < INFINITY;
+          const int nv = __popc(vm[h]);
+          Fs[h] = F32[h];
+          gs[h] = g32[h];
+          Ms[h] = M32[h];
+          exs[h] = false;
+          evals += nv;
+          evals32 += nv;
+          steps += static_cast<unsigned long long>(nv) * nsteps;
+          steps32 += static_cast<unsigned long long>(nv) * nsteps;
+          // the near-cutoff band takes the precomputed FP64 values where it can
+          bool have_tail = false;
+          if (near_cut[h]) {
+            const double4 t0 = tail[0], t1 = tail[1];
+            const double4 tv = cs[h] == t0.x ? t0 : t1;
+            if (cs[h] == tv.x && isfinite(tv.y)) {
+              Fs[h] = tv.y;
+              gs[h] = tv.z;
+              Ms[h] = tv.w;
+              exs[h] = true;
+              have_tail = true;
+            }
           }
-          zoom_right = x2;
-          unsigned long long ze = 0;
-          const int before = nbr;
-          nbr = zoom_trough(view64, wave, w, x0, x2, sa, sb, ma, mb, sgn, (mmode >> i) & 1u, d.tol, slot,
-                            nbr, K, lane, ze);
-          brackets += nbr - before;
-          evals += ze;
-          steps += ze * nsteps;
-          ++zooms;
+          // sign-uncertain single-precision samples (small |g|) and the rest of the
+          // near-cutoff band are evaluated in FP64 here
+          const bool redo = valid && !have_tail && (!(fabs(gs[h]) > 2e-4) || near_cut[h]);
+          const unsigned rm = __ballot_sync(FULL, redo);
+          if (rm) {
+            if (redo) {
+              Fs[h] = eval64_outline(view64, WAVE, w, cs[h], &gs[h], &Ms[h]);
+              exs[h] = true;
+            }
+            evals += __popc(rm);
+            steps += static_cast<unsigned long long>(__popc(rm)) * nsteps;
+          }
         }
-      }
-      // ---- carry the last two elements ----
-      const int last = nvalid - 1;
-      const double nc1 = __shfl_sync(FULL, c, last), nF1 = __shfl_sync(FULL, F, last),
-                   ng1 = __shfl_sync(FULL, g, last), nM1 = __shfl_sync(FULL, M, last);
-      if (nvalid >= 2) {
-        c2 = __shfl_sync(FULL, c, last - 1);
-        F2 = __shfl_sync(FULL, F, last - 1);
-        g2 = __shfl_sync(FULL, g, last - 1);
-        M2 = __shfl_sync(FULL, M, last - 1);
-        have2 = true;
       } else {
-        c2 = c1; F2 = F1; g2 = g1; M2 = M1;
-        have2 = have1;
+        double c64 = cs[0] < INFINITY ? cs[0] : 1.;
+        scan_eval<double, WAVE, 1>(view, w, &c64, Fs, gs, Ms);
+        exs[0] = true;
+        const int nv = __popc(vm[0]);
+        evals += nv;
+        steps += static_cast<unsigned long long>(nv) * nsteps;
       }
-      c1 = nc1; F1 = nF1; g1 = ng1; M1 = nM1;
-      have1 = true;
+
+#pragma unroll
+      for (int h = 0; h < S; ++h) {
+        if (nbr >= K) break;
+        if (!vm[h]) {
+          finished = true;
+          break;
+        }
+        const double c = cs[h], F = Fs[h], g = gs[h], M = Ms[h];
+        const bool exact = exs[h];
+        const bool valid = c < INFINITY;
+        const int nvalid = __popc(vm[h]);
+        if (__any_sync(FULL, valid && !(isfinite(F) && isfinite(g)))) {
+          tfl |= TRACE_NONFINITE | TRACE_SEARCH_UNCONVERGED;
+          finished = true;
+          break;
+        }
+        // ---- sign changes against the immediate left neighbour ----
+        double cl = __shfl_up_sync(FULL, c, 1), Fl = __shfl_up_sync(FULL, F, 1);
+        bool exl = __shfl_up_sync(FULL, exact, 1);
+        const bool vl = lane >= 1 ? lane - 1 < nvalid : have1;
+        if (lane == 0) {
+          cl = c1;
+          Fl = F1;
+          exl = ex1;
+        }
+        const bool sc = valid && vl && (signbit(Fl) != signbit(F));  // +0 counts as positive
+        const unsigned scm = __ballot_sync(FULL, sc);
+        const int myseg = nseg + __popc(scm & le);
+        Sample me{c, static_cast<float>(g), static_cast<float>(M), myseg | (signbit(F) ? (1 << 30) : 0)};
+        // ---- regular samples and their two regular predecessors ----
+        const bool reg = valid && !(vl && c - cl < 1e-6 * c);
+        const unsigned rmask = __ballot_sync(FULL, reg);
+        const unsigned m1 = rmask & lt;
+        const int j1 = m1 ? 31 - __clz(m1) : -1;
+        const unsigned m2 = j1 >= 0 ? (m1 & ~(1u << j1)) : 0u;
+        const int j2 = m2 ? 31 - __clz(m2) : -1;
+        Sample P1 = shfl_sample(me, j1 & 31), P2 = shfl_sample(me, j2 & 31);
+        bool hp1 = j1 >= 0, hp2 = j2 >= 0;
+        if (j1 < 0) {
+          P1 = R1; hp1 = hr1;
+          P2 = R2; hp2 = hr2;
+        } else if (j2 < 0) {
+          P2 = R1; hp2 = hr1;
+        }
+        // ---- same-sign troughs: V-shaped shape-feature minima, log-magnitude dips ----
+        bool tr = false, trm_ = false;
+        if (reg && hp1 && hp2 && sample_segment(P2) == myseg && sample_segment(P1) == myseg) {
+          const double sgn = sample_sign(P1);
+          tr = trough_may_hide_roots(P2.c, P1.c, c, sgn * P2.g, sgn * P1.g, sgn * static_cast<float>(g),
+                                     single ? 1e-5f : 1e-7f);
+          if (!tr) trm_ = magnitude_dip(P2.c, P1.c, c, P2.M, P1.M, static_cast<float>(M)) > MDIP;
+          tr = tr || trm_;
+        }
+        const unsigned trm = __ballot_sync(FULL, tr), mmode = __ballot_sync(FULL, trm_);
+        unsigned events = scm | trm;
+        while (events && nbr < K) {
+          const int i = __ffs(events) - 1;
+          events &= events - 1;
+          if ((scm >> i) & 1u) {
+            if (lane == i) put_bracket(slot, nbr, cl, c, exl ? Fl : NAN, exact ? F : NAN);
+            ++nbr;
+          } else {
+            double x0 = __shfl_sync(FULL, P2.c, i), x1 = __shfl_sync(FULL, P1.c, i);
+            const double x2 = __shfl_sync(FULL, c, i);
+            const double sgn = (__shfl_sync(FULL, P1.seg, i) >> 30) & 1 ? -1. : 1.;
+            double sa = sgn * __shfl_sync(FULL, P2.g, i), ma = __shfl_sync(FULL, P2.M, i);
+            const double sb = sgn * __shfl_sync(FULL, g, i), mb = __shfl_sync(FULL, M, i);
+            if (x0 < zoom_right) {  // overlaps the previous window: start at its middle sample
+              x0 = x1;
+              sa = sgn * __shfl_sync(FULL, P1.g, i);
+              ma = __shfl_sync(FULL, P1.M, i);
+            }
+            zoom_right = x2;
+            const int mode = (mmode >> i) & 1u;
+            bool dismissed = false;
+            if constexpr (single) {
+              unsigned long long se = 0;
+              dismissed = screen_trough32<WAVE>(view, static_cast<float>(w), x0, x2, sa, sb, ma, mb, sgn, mode,
+                                                lane, se);
+              evals += se;
+              evals32 += se;
+              steps += se * nsteps;
+              steps32 += se * nsteps;
+            }
+            if (!dismissed) {
+              unsigned long long ze = 0;
+              nbr = zoom_trough<WAVE>(view64, w, x0, x2, sa, sb, ma, mb, sgn, mode, d.tol, slot, nbr, K, lane, ze);
+              evals += ze;
+              steps += ze * nsteps;
+              ++zooms;
+            }
+          }
+        }
+        // ---- carries ----
+        nseg += __popc(scm);
+        const int last = nvalid - 1;
+        c1 = __shfl_sync(FULL, c, last);
+        F1 = __shfl_sync(FULL, F, last);
+        ex1 = __shfl_sync(FULL, exact, last);
+        have1 = true;
+        if (rmask) {
+          const int h1 = 31 - __clz(rmask);
+          const unsigned rest = rmask & ~(1u << h1);
+          const Sample n1 = shfl_sample(me, h1);
+          const Sample n2 = shfl_sample(me, rest ? 31 - __clz(rest) : 0);
+          if (rest) {
+            R2 = n2;
+            hr2 = true;
+          } else {
+            R2 = R1;
+            hr2 = hr1;
+          }
+          R1 = n1;
+          hr1 = true;
+        }
+      }
     }
     // ---- publish brackets ----
     if (lane == 0) {

@@ -146,7 +146,15 @@ MD200_FN Dual<T, ND> operator-(T s, const Dual<T, ND> &a) {
 MD200_FN double m_rsqrt(double x) { return rsqrt(x); }
 MD200_FN float m_rsqrt(float x) { return rsqrtf(x); }
 MD200_FN void m_sincos(double x, double *s, double *c) { sincos(x, s, c); }
-MD200_FN void m_sincos(float x, float *s, float *c) { sincosf(x, s, c); }
+// Single precision: reduce by 2 pi with a two-constant Cody-Waite split (exact
+// for the |x| < 2^12 rad phases of the recurrences) and evaluate with the
+// special-function unit; absolute error ~4e-7, far below the scan's
+// sign-decision threshold (|g| < 2e-4 samples are re-evaluated in FP64).
+MD200_FN void m_sincos(float x, float *s, float *c) {
+  const float n = rintf(x * 0.15915494309189535f);
+  const float r = fmaf(n, -1.7484555e-07f, fmaf(n, -6.28318548f, x));
+  __sincosf(r, s, c);
+}
 MD200_FN double m_exp(double x) { return exp(x); }
 MD200_FN float m_exp(float x) { return __expf(x); }
 MD200_FN float m_expm1(float x) { return expm1f(x); }
@@ -165,6 +173,10 @@ MD200_FN double m_sqrt(double x) { return sqrt(x); }
 MD200_FN float m_sqrt(float x) { return sqrtf(x); }
 MD200_FN double m_abs(double x) { return fabs(x); }
 MD200_FN float m_abs(float x) { return fabsf(x); }
+MD200_FN double m_max(double a, double b) { return fmax(a, b); }
+MD200_FN float m_max(float a, float b) { return fmaxf(a, b); }
+MD200_FN double m_log2(double x) { return log2(x); }
+MD200_FN float m_log2(float x) { return log2f(x); }
 
 template <class T, int ND>
 MD200_FN Dual<T, ND> m_rsqrt(const Dual<T, ND> &x) {
@@ -251,7 +263,7 @@ MD200_FN int scale_vector(N *e, int n, typename Base<N>::type tiny) {
   T big = T(0);
 #pragma unroll
   for (int i = 0; i < 5; ++i)
-    if (i < n) big = fmax(big, m_abs(val(e[i])));
+    if (i < n) big = m_max(big, m_abs(val(e[i])));
   if (big >= tiny && big < T(INFINITY)) {
     const T r = pow2_inverse(big);
 #pragma unroll
@@ -283,15 +295,19 @@ MD200_FN void radical(const N &k, const N &kv, N *r, N *ir) {
 // ---------------------------------------------------------------------------
 template <class T>
 struct LayerView {
-  const T *h;     // thickness
-  const T *ivp;   // 1 / vp
-  const T *ivs;   // 1 / vs (0 for a fluid layer)
-  const T *vs2;   // vs^2
-  const T *rho;   // density
-  const T *irho;  // 1 / rho
-  const T *imu;   // 1 / (rho vs^2) (0 for a fluid layer)
-  int L;          // rows including the half-space
-  int water;      // 1 when row 0 is a fluid (vs = 0) layer
+  // rows of one model, each Ls long: h, 1/vp, 1/vs (0 for a fluid layer), vs^2,
+  // rho, 1/rho, 1/(rho vs^2) (0 for a fluid layer)
+  const T *base;
+  int Ls;
+  int L;      // rows including the half-space
+  int water;  // 1 when row 0 is a fluid (vs = 0) layer
+  MD200_FN T h(int j) const { return base[j]; }
+  MD200_FN T ivp(int j) const { return base[Ls + j]; }
+  MD200_FN T ivs(int j) const { return base[2 * Ls + j]; }
+  MD200_FN T vs2(int j) const { return base[3 * Ls + j]; }
+  MD200_FN T rho(int j) const { return base[4 * Ls + j]; }
+  MD200_FN T irho(int j) const { return base[5 * Ls + j]; }
+  MD200_FN T imu(int j) const { return base[6 * Ls + j]; }
 };
 
 // One upward Dunkin step through layer m: e <- e * Ca(m).
@@ -391,8 +407,65 @@ MD200_FN typename Base<N>::type rayleigh_layer(N e[5], const N &k, const N &k2, 
   return expo;
 }
 
+// Branch-free single-precision form of rayleigh_layer: both the trigonometric
+// (propagating) and the scaled hyperbolic (evanescent) forms of each wave are
+// evaluated with the special-function unit and selected, so the lanes of a warp
+// at different velocities do not diverge.  Same matrix, same return value.
+MD200_FN float rayleigh_layer_f32(float e[5], float k, float k2, float w, float iw2, float h, float ivp,
+                                  float vs2, float ivs, float rho, float irho) {
+  const float ka = w * ivp, kb = w * ivs;
+  const float gammk = (iw2 * vs2) * 2.f;
+  const float gam = gammk * k2;
+  // radicals and reciprocals (zero where k equals the wavenumber exactly)
+  const float Xa = (k + ka) * fabsf(k - ka), Xb = (k + kb) * fabsf(k - kb);
+  const float ira = Xa > 0.f ? rsqrtf(Xa) : 0.f, irb = Xb > 0.f ? rsqrtf(Xb) : 0.f;
+  const float ra = Xa * ira, rb = Xb * irb;
+  const float p = ra * h, q = rb * h;
+  const bool pp = k < ka, pq = k < kb;  // propagating P / S
+  float sp, cp, sq, cq;
+  m_sincos(p, &sp, &cp);
+  m_sincos(q, &sq, &cq);
+  const float ep = m_exp(-p), eq = m_exp(-q);
+  const float fp = ep * ep, fq = eq * eq;
+  const float cosp = pp ? cp : .5f * (1.f + fp), sinp = pp ? sp : .5f * (1.f - fp);
+  const float cosq = pq ? cq : .5f * (1.f + fq), sinq = pq ? sq : .5f * (1.f - fq);
+  // sin(r h)/r -> h as r -> 0
+  const float wv = Xa > 0.f ? sinp * ira : h, xv = pp ? -(ra * sinp) : ra * sinp;
+  const float yv = Xb > 0.f ? sinq * irb : h, zv = pq ? -(rb * sinq) : rb * sinq;
+  const float a0 = (pp ? 1.f : ep) * (pq ? 1.f : eq);
+  const float expo = (pp ? 0.f : p) + (pq ? 0.f : q);
+  const float cpcq = cosp * cosq, cpy = cosp * yv, cpz = cosp * zv;
+  const float cqw = cosq * wv, cqx = cosq * xv;
+  const float xy = xv * yv, xz = xv * zv, wy = wv * yv, wz = wv * zv;
+  const float gm1 = gam - 1.f, twgm1 = gam + gm1, gmgmk = gam * gammk, gmgm1 = gam * gm1, gm1sq = gm1 * gm1;
+  const float a0pq = a0 - cpcq;
+  const float rho2 = rho * rho, irho2 = irho * irho;
+  const float A = cpcq - (gmgm1 * a0pq) * 2.f - gmgmk * xz - k2 * gm1sq * wy;
+  const float D = (k2 * cpy - cqx) * irho;
+  const float I = -(twgm1 * a0pq + gammk * xz + k2 * gm1 * wy) * irho;
+  const float C = (cpz - k2 * cqw) * irho;
+  const float Lm = -((k2 * a0pq) * 2.f + xz + k2 * k2 * wy) * irho2;
+  const float E = (gmgmk * cpz - gm1sq * cqw) * rho;
+  const float G = gammk * cpz - gm1 * cqw;
+  const float M = -wz, Nn = -xy;
+  const float F = (gm1sq * cpy - gmgmk * cqx) * rho;
+  const float H = gm1 * cpy - gammk * cqx;
+  const float O = -((gmgmk * gm1sq * a0pq) * 2.f + gmgmk * gmgmk * xz + gm1sq * gm1sq * wy) * rho2;
+  const float J = -(gammk * gm1 * twgm1 * a0pq + gam * gammk * gammk * xz + gm1 * gm1sq * wy) * rho;
+  const float K = a0 + (cpcq - A) * 2.f;
+  const float B = cpcq;
+  const float e0 = e[0], e1 = e[1], e3 = e[3], e4 = e[4];
+  const float e2t = e[2] * (k2 * -2.f);
+  e[0] = A * e0 + E * e1 + J * e2t + F * e3 + O * e4;
+  e[1] = D * e0 + B * e1 + H * e2t + Nn * e3 + F * e4;
+  e[2] = I * e0 + G * e1 + K * e[2] + H * e3 + J * e4;
+  e[3] = C * e0 + M * e1 + G * e2t + B * e3 + E * e4;
+  e[4] = Lm * e0 + C * e1 + I * e2t + D * e3 + A * e4;
+  return expo;
+}
+
 // The same layer step for a layer in which both waves are deeply evanescent
-// (c < vs/4), in single precision.  With u = (c/vp)^2, v = (c/vs)^2, p = sqrt(1-u),
+// (c well below vs), in single precision.  With u = (c/vp)^2, v = (c/vs)^2, p = sqrt(1-u),
 // s = sqrt(1-v), R = p s and g = 2/v (the standard form's gamma), the standard
 // entries are sums of terms growing like g^4 that cancel down to O(g^2); here each
 // entry is written through the exactly-computed differences 1 - R (loss),
@@ -441,156 +514,222 @@ MD200_FN float rayleigh_layer_evanescent(float e[5], float k, float k2, float c,
   return kh * (p + s);  // P + Q
 }
 
-// Rayleigh secular value F(k, w) and shape feature g = F / |e| (water top: the
-// fluid form).  Units: k = w / c in rad/km, w in rad/s.  With `lmag`, also the
-// base-2 logarithm of the magnitude |e| of the unnormalised vector: it is smooth
-// across ordinary roots and dips logarithmically where the whole vector nearly
-// vanishes, the signature of a close root pair.
-template <class N, class T>
-MD200_FN N rayleigh_secular(const LayerView<T> &m, const N &k, const N &w, N *shape,
-                            typename Base<N>::type *lmag = nullptr) {
+// Single-precision layers switch to the factored step where c < vs / RATIO.
+// Measured against the FP64 oracle on crustal and low-velocity-layer models,
+// the standard step keeps every FP32 sign down to c = vs/16 and loses signs
+// below about vs/64; the factored step costs ~3x a standard one, so it is used
+// only where needed.
+#ifndef MD200_EVANESCENT_RATIO
+#define MD200_EVANESCENT_RATIO 16.f
+#endif
+
+// Rayleigh secular values F(k_s, w) of S samples at one frequency, with shape
+// features g = F / |e| (water top: the fluid form).  Units: k = w / c in rad/km,
+// w in rad/s.  The S recurrences are independent and interleaved layer by layer
+// (instruction-level parallelism for latency-bound single-precision scans).
+// With `lmag`, also the base-2 logarithm of the magnitude |e| of the
+// unnormalised vector: it is smooth across ordinary roots and dips
+// logarithmically where the whole vector nearly vanishes, the signature of a
+// close root pair.
+template <class N, class T, int S>
+MD200_FN void rayleigh_multi(const LayerView<T> &m, const N *k, const N &w, N *F, N *shape,
+                             typename Base<N>::type *lmag) {
   using B = typename Base<N>::type;
   const B tiny = sizeof(B) == 4 ? B(1e-30) : B(1e-40);
-  const N k2 = k * k;
   const N iw = lift_one<N>() / w;
   const N iw2 = iw * iw;
   const int last = m.L - 1;
-  N e[5];
-  {
-    const N ka = w * m.ivp[last], kb = w * m.ivs[last];
+  N e[S][5], k2[S];
+  int ex[S];
+  B ev[S];
+#pragma unroll
+  for (int s = 0; s < S; ++s) {
+    k2[s] = k[s] * k[s];
+    const N ka = w * m.ivp(last), kb = w * m.ivs(last);
     N ra, ira, rb, irb;
-    radical(k, ka, &ra, &ira);
-    radical(k, kb, &rb, &irb);
-    const N gammk = (iw2 * m.vs2[last]) * T(2);
-    const N gam = gammk * k2;
+    radical(k[s], ka, &ra, &ira);
+    radical(k[s], kb, &rb, &irb);
+    const N gammk = (iw2 * m.vs2(last)) * T(2);
+    const N gam = gammk * k2[s];
     const N gm1 = gam - T(1);
-    const T rh = m.rho[last];
+    const T rh = m.rho(last);
     const N rarb = ra * rb;
-    e[0] = (gm1 * gm1 - gam * gammk * rarb) * (rh * rh);
-    e[1] = -(ra * rh);
-    e[2] = (gm1 - gammk * rarb) * rh;
-    e[3] = rb * rh;
-    e[4] = k2 - rarb;
+    e[s][0] = (gm1 * gm1 - gam * gammk * rarb) * (rh * rh);
+    e[s][1] = -(ra * rh);
+    e[s][2] = (gm1 - gammk * rarb) * rh;
+    e[s][3] = rb * rh;
+    e[s][4] = k2[s] - rarb;
+    if constexpr (sizeof(N) == sizeof(float)) {
+      // single precision: the factored start vector well below the shear velocity
+      const float c = w / k[s];
+      const float ivs_l = m.ivs(last);
+      if (MD200_EVANESCENT_RATIO * c * ivs_l < 1.f) {
+        const float cp = c * m.ivp(last), cs = c * ivs_l, u = cp * cp, v = cs * cs;
+        const float p = sqrtf(1.f - u), sh = sqrtf(1.f - v), R = p * sh;
+        const float loss = (u + (1.f - u) * v) / (1.f + R), g = 2.f / v;
+        const float d1 = 1.f - g * loss;
+        e[s][0] = rh * rh * (1.f - g * (1.f + d1));
+        e[s][1] = -rh * k[s] * p;
+        e[s][2] = -rh * d1;
+        e[s][3] = rh * k[s] * sh;
+        e[s][4] = k2[s] * loss;
+      }
+    }
+    ex[s] = scale_vector(e[s], 5, tiny);
+    ev[s] = B(0);
   }
-  if constexpr (sizeof(N) == sizeof(float)) {
-    // single precision: factored start and steps where c < vs/4
-    const float c = w / k;
-    const float ivs_l = m.ivs[last];
-    if (4.f * c * ivs_l < 1.f) {
-      const float cp = c * m.ivp[last], cs = c * ivs_l, u = cp * cp, v = cs * cs;
-      const float p = sqrtf(1.f - u), s = sqrtf(1.f - v), R = p * s;
-      const float loss = (u + (1.f - u) * v) / (1.f + R), g = 2.f / v;
-      const float d1 = 1.f - g * loss, rh = m.rho[last];
-      e[0] = rh * rh * (1.f - g * (1.f + d1));
-      e[1] = -rh * k * p;
-      e[2] = -rh * d1;
-      e[3] = rh * k * s;
-      e[4] = k2 * loss;
+  for (int l = m.L - 2; l >= m.water; --l) {
+    const T h = m.h(l), ivp = m.ivp(l), vs2 = m.vs2(l), ivs = m.ivs(l), rho = m.rho(l), irho = m.irho(l);
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+      if constexpr (sizeof(N) == sizeof(float)) {
+        const float c = w / k[s];
+        if (MD200_EVANESCENT_RATIO * c * ivs < 1.f)
+          ev[s] += rayleigh_layer_evanescent(e[s], k[s], k2[s], c, h, ivp, ivs, rho, irho);
+        else
+          ev[s] += rayleigh_layer_f32(e[s], k[s], k2[s], w, iw2, h, ivp, vs2, ivs, rho, irho);
+      } else {
+        ev[s] += rayleigh_layer(e[s], k[s], k2[s], w, iw2, h, ivp, vs2, ivs, rho, irho);
+      }
+      ex[s] += scale_vector(e[s], 5, tiny);
     }
-    int ex = scale_vector(e, 5, tiny);
-    float ev = 0.f;
-    for (int l = m.L - 2; l >= m.water; --l) {
-      if (4.f * c * m.ivs[l] < 1.f)
-        ev += rayleigh_layer_evanescent(e, k, k2, c, m.h[l], m.ivp[l], m.ivs[l], m.rho[l], m.irho[l]);
-      else
-        ev += rayleigh_layer(e, k, k2, w, iw2, m.h[l], m.ivp[l], m.vs2[l], m.ivs[l], m.rho[l], m.irho[l]);
-      ex += scale_vector(e, 5, tiny);
-    }
-    if (lmag) *lmag = static_cast<float>(ex) + ev * 1.4426950408889634f;
-  } else {
-    int ex = scale_vector(e, 5, tiny);
-    B ev = B(0);
-    for (int l = m.L - 2; l >= m.water; --l) {
-      ev += rayleigh_layer(e, k, k2, w, iw2, m.h[l], m.ivp[l], m.vs2[l], m.ivs[l], m.rho[l], m.irho[l]);
-      ex += scale_vector(e, 5, tiny);
-    }
-    if (lmag) *lmag = static_cast<B>(ex) + ev * B(1.4426950408889634);
   }
-  if (m.water) {
-    const N ka = w * m.ivp[0];
-    N rf, irf;
-    radical(k, ka, &rf, &irf);
-    const T h0 = m.h[0];
-    N cp, wv;
-    if (val(k) < val(ka)) {
-      N sn;
-      m_sincos(rf * h0, &sn, &cp);
-      wv = sn * irf;
-    } else if (val(k) == val(ka)) {
-      cp = lift_one<N>();
-      wv = lift_one<N>() * h0;
+#pragma unroll
+  for (int s = 0; s < S; ++s) {
+    if (lmag) lmag[s] = static_cast<B>(ex[s]) + ev[s] * B(1.4426950408889634);
+    if (m.water) {
+      const N ka = w * m.ivp(0);
+      N rf, irf;
+      radical(k[s], ka, &rf, &irf);
+      const T h0 = m.h(0);
+      N cp, wv;
+      if (val(k[s]) < val(ka)) {
+        N sn;
+        m_sincos(rf * h0, &sn, &cp);
+        wv = sn * irf;
+      } else if (val(k[s]) == val(ka)) {
+        cp = lift_one<N>();
+        wv = lift_one<N>() * h0;
+      } else {
+        const N ez = m_exp(-(rf * h0));
+        const N z = ez * ez;
+        cp = (z + B(1)) * B(0.5);
+        wv = ((B(1) - z) * B(0.5)) * irf;
+      }
+      const N t0 = cp * e[s][0], t1 = wv * e[s][1] * m.rho(0);
+      N pair[2] = {t0, t1};
+      const int pex = scale_vector(pair, 2, tiny);
+      const N u = pair[0], v = pair[1];
+      if (shape) shape[s] = (u - v) * m_rsqrt(u * u + v * v + lift_one<N>() * tiny);
+      if (lmag) lmag[s] += static_cast<B>(pex) + B(0.5) * m_log2(val(u * u + v * v) + tiny);
+      F[s] = u - v;
     } else {
-      const N ez = m_exp(-(rf * h0));
-      const N z = ez * ez;
-      cp = (z + B(1)) * B(0.5);
-      wv = ((B(1) - z) * B(0.5)) * irf;
+      const N norm2 = e[s][0] * e[s][0] + e[s][1] * e[s][1] + e[s][2] * e[s][2] + e[s][3] * e[s][3] +
+                      e[s][4] * e[s][4];
+      if (shape) shape[s] = e[s][0] * m_rsqrt(norm2 + lift_one<N>() * tiny);
+      if (lmag) lmag[s] += B(0.5) * m_log2(val(norm2) + tiny);
+      F[s] = e[s][0];
     }
-    const N t0 = cp * e[0], t1 = wv * e[1] * m.rho[0];
-    N pair[2] = {t0, t1};
-    const int pex = scale_vector(pair, 2, tiny);
-    if (lmag) *lmag += static_cast<B>(pex);
-    const N u = pair[0], v = pair[1];
-    if (shape) *shape = (u - v) * m_rsqrt(u * u + v * v + lift_one<N>() * tiny);
-    if (lmag) *lmag += B(0.5) * log2(val(u * u + v * v) + tiny);
-    return u - v;
   }
-  const N norm2 = e[0] * e[0] + e[1] * e[1] + e[2] * e[2] + e[3] * e[3] + e[4] * e[4];
-  if (shape) *shape = e[0] * m_rsqrt(norm2 + lift_one<N>() * tiny);
-  if (lmag) *lmag += B(0.5) * log2(val(norm2) + tiny);
-  return e[0];
 }
 
-// Love secular value (SH propagator) and shape feature.
 template <class N, class T>
-MD200_FN N love_secular(const LayerView<T> &m, const N &k, const N &w, N *shape,
-                        typename Base<N>::type *lmag = nullptr) {
+MD200_FN N rayleigh_secular(const LayerView<T> &m, const N &k, const N &w, N *shape,
+                            typename Base<N>::type *lmag = nullptr) {
+  N F;
+  rayleigh_multi<N, T, 1>(m, &k, w, &F, shape, lmag);
+  return F;
+}
+
+// Love secular values (SH propagator) and shape features of S samples.
+template <class N, class T, int S>
+MD200_FN void love_multi(const LayerView<T> &m, const N *k, const N &w, N *F, N *shape,
+                         typename Base<N>::type *lmag) {
   using B = typename Base<N>::type;
   const B tiny = sizeof(B) == 4 ? B(1e-30) : B(1e-40);
   const int last = m.L - 1;
-  N e[2];
-  {
-    const N kb = w * m.ivs[last];
+  N e[S][2];
+  int ex[S];
+  B ev[S];
+#pragma unroll
+  for (int s = 0; s < S; ++s) {
+    const N kb = w * m.ivs(last);
     N r, ir;
-    radical(k, kb, &r, &ir);
-    e[0] = r * m.rho[last];
-    e[1] = lift_one<N>() * (m.ivs[last] * m.ivs[last]);
+    radical(k[s], kb, &r, &ir);
+    e[s][0] = r * m.rho(last);
+    e[s][1] = lift_one<N>() * (m.ivs(last) * m.ivs(last));
+    ex[s] = 0;
+    ev[s] = B(0);
   }
-  int ex = 0;
-  B ev = B(0);
   for (int j = last - 1; j >= m.water; --j) {
-    const T h = m.h[j], mu = m.rho[j] * m.vs2[j], imu = m.imu[j];
-    const N kj = w * m.ivs[j];
-    N r, ir;
-    radical(k, kj, &r, &ir);
-    N cq, y, z;
-    if (val(k) < val(kj)) {
-      N sn;
-      m_sincos(r * h, &sn, &cq);
-      y = sn * ir;
-      z = -(r * sn);
-    } else if (val(k) == val(kj)) {
-      cq = lift_one<N>();
-      y = lift_one<N>() * h;
-      z = lift_zero<N>();
-    } else {
-      const N eq = m_exp(-(r * h));
-      ev += val(r) * h;
-      const N f = eq * eq;
-      cq = (f + B(1)) * B(0.5);
-      const N half = (B(1) - f) * B(0.5);
-      y = half * ir;
-      z = half * r;
+    const T h = m.h(j), mu = m.rho(j) * m.vs2(j), imu = m.imu(j), ivs = m.ivs(j);
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+      const N kj = w * ivs;
+      N r, ir;
+      radical(k[s], kj, &r, &ir);
+      N cq, y, z;
+      if constexpr (sizeof(N) == sizeof(float)) {
+        // branch-free single precision: both forms, selected
+        const float q = r * h;
+        float sn, cs;
+        m_sincos(q, &sn, &cs);
+        const float eq = m_exp(-q), f = eq * eq;
+        const bool prop = k[s] < kj;
+        cq = prop ? cs : .5f * (1.f + f);
+        const float half = prop ? sn : .5f * (1.f - f);
+        y = ir > 0.f ? half * ir : h;
+        z = prop ? -(r * half) : r * half;
+        ev[s] += prop ? 0.f : q;
+      } else if (val(k[s]) < val(kj)) {
+        N sn;
+        m_sincos(r * h, &sn, &cq);
+        y = sn * ir;
+        z = -(r * sn);
+      } else if (val(k[s]) == val(kj)) {
+        cq = lift_one<N>();
+        y = lift_one<N>() * h;
+        z = lift_zero<N>();
+      } else {
+        const N eq = m_exp(-(r * h));
+        ev[s] += val(r) * h;
+        const N f = eq * eq;
+        cq = (f + B(1)) * B(0.5);
+        const N half = (B(1) - f) * B(0.5);
+        y = half * ir;
+        z = half * r;
+      }
+      const N u = e[s][0] * cq + e[s][1] * z * mu;
+      const N v = e[s][0] * y * imu + e[s][1] * cq;
+      e[s][0] = u;
+      e[s][1] = v;
+      ex[s] += scale_vector(e[s], 2, tiny);
     }
-    const N u = e[0] * cq + e[1] * z * mu;
-    const N v = e[0] * y * imu + e[1] * cq;
-    e[0] = u;
-    e[1] = v;
-    ex += scale_vector(e, 2, tiny);
   }
-  const N norm2 = e[0] * e[0] + e[1] * e[1];
-  if (shape) *shape = e[0] * m_rsqrt(norm2 + lift_one<N>() * tiny);
-  if (lmag) *lmag = static_cast<B>(ex) + ev * B(1.4426950408889634) + B(0.5) * log2(val(norm2) + tiny);
-  return e[0];
+#pragma unroll
+  for (int s = 0; s < S; ++s) {
+    const N norm2 = e[s][0] * e[s][0] + e[s][1] * e[s][1];
+    if (shape) shape[s] = e[s][0] * m_rsqrt(norm2 + lift_one<N>() * tiny);
+    if (lmag)
+      lmag[s] = static_cast<B>(ex[s]) + ev[s] * B(1.4426950408889634) + B(0.5) * m_log2(val(norm2) + tiny);
+    F[s] = e[s][0];
+  }
+}
+
+template <class N, class T>
+MD200_FN N love_secular(const LayerView<T> &m, const N &k, const N &w, N *shape,
+                        typename Base<N>::type *lmag = nullptr) {
+  N F;
+  love_multi<N, T, 1>(m, &k, w, &F, shape, lmag);
+  return F;
+}
+
+// S samples at once (WAVE: 0 Rayleigh, 1 Love).
+template <class N, class T, int S, int WAVE>
+MD200_FN void secular_multi(const LayerView<T> &m, const N *k, const N &w, N *F, N *shape,
+                            typename Base<N>::type *lmag) {
+  if constexpr (WAVE) love_multi<N, T, S>(m, k, w, F, shape, lmag);
+  else rayleigh_multi<N, T, S>(m, k, w, F, shape, lmag);
 }
 
 template <class N, class T>
