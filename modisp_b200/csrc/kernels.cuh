@@ -92,31 +92,40 @@ __device__ __noinline__ double eval64_outline(const LayerView<double> &m, int wa
 }
 
 // Rayleigh-wave speed of a homogeneous half-space by bisection of the
-// Rayleigh cubic (cpp/common/physics.hpp:140-144).
+// Rayleigh cubic (cpp/common/physics.hpp:140-144).  Every operation is rounded
+// separately (no FMA contraction), matching the reference's -ffp-contract=off
+// build bit for bit: the search window is reported and compared exactly.
 __device__ double rayleigh_speed(double vp, double vs) {
-  const double ratio = (vs / vp) * (vs / vp);
+  const double q = __ddiv_rn(vs, vp), ratio = __dmul_rn(q, q);
   double l = 0., h = 1.;
   for (int j = 0; j < 56; ++j) {
-    const double x = (l + h) * .5;
-    const double f = ((x - 8.) * x + 24. - 16. * ratio) * x - 16. * (1. - ratio);
+    const double x = __dmul_rn(__dadd_rn(l, h), .5);
+    const double a = __dadd_rn(__dmul_rn(__dadd_rn(x, -8.), x), 24.);
+    const double f = __dadd_rn(__dmul_rn(__dadd_rn(a, -__dmul_rn(16., ratio)), x),
+                               -__dmul_rn(16., __dadd_rn(1., -ratio)));
     if (f < 0.) l = x; else h = x;
   }
-  return vs * sqrt((l + h) * .5);
+  return __dmul_rn(vs, __dsqrt_rn(__dmul_rn(__dadd_rn(l, h), .5)));
 }
 
 // Scholte-wave speed of a fluid over a solid half-space by bisection
-// (cpp/common/physics.hpp:146-156).
+// (cpp/common/physics.hpp:146-156), separately rounded like rayleigh_speed.
 __device__ double scholte_speed(double vf, double rf, double vp, double vs, double rs) {
-  const double ratio = (vs / vp) * (vs / vp), qf = (vs / vf) * (vs / vf);
-  double l = 0., h = fmax(0., fmin(1., vf / vs) * (1. - 1e-12));
+  const double q1 = __ddiv_rn(vs, vp), ratio = __dmul_rn(q1, q1);
+  const double q2 = __ddiv_rn(vs, vf), qf = __dmul_rn(q2, q2);
+  double l = 0., h = fmax(0., __dmul_rn(fmin(1., __ddiv_rn(vf, vs)), __dadd_rn(1., -1e-12)));
   for (int j = 0; j < 64; ++j) {
-    const double x = (l + h) * .5, x2 = x * x;
-    const double A = sqrt(fmax(0., 1. - ratio * x2)), B = sqrt(fmax(0., 1. - x2));
-    const double f = 4. * (1. + ratio - ratio * x2) / (1. + A * B) - 4. + x2 +
-                     (rf / rs) * x2 * A / sqrt(fmax(1e-30, 1. - qf * x2));
+    const double x = __dmul_rn(__dadd_rn(l, h), .5), x2 = __dmul_rn(x, x);
+    const double A = __dsqrt_rn(fmax(0., __dadd_rn(1., -__dmul_rn(ratio, x2))));
+    const double B = __dsqrt_rn(fmax(0., __dadd_rn(1., -x2)));
+    const double num = __dmul_rn(4., __dadd_rn(__dadd_rn(1., ratio), -__dmul_rn(ratio, x2)));
+    const double t1 = __ddiv_rn(num, __dadd_rn(1., __dmul_rn(A, B)));
+    const double t2 = __ddiv_rn(__dmul_rn(__dmul_rn(__ddiv_rn(rf, rs), x2), A),
+                                __dsqrt_rn(fmax(1e-30, __dadd_rn(1., -__dmul_rn(qf, x2)))));
+    const double f = __dadd_rn(__dadd_rn(__dadd_rn(t1, -4.), x2), t2);
     if (f < 0.) l = x; else h = x;
   }
-  return vs * (l + h) * .5;
+  return __dmul_rn(vs, __dmul_rn(__dadd_rn(l, h), .5));
 }
 
 // Warp-cooperative bitonic sort of n2 (a power of two) keys with int payloads.
