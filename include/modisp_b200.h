@@ -152,6 +152,23 @@ int md200_group_roots(const double *thickness, const double *vp, const double *v
                       const double *roots, int known, int modes, double close_rtol,
                       double *group, unsigned *group_flags);
 
+/* md200_group_roots without any device allocation.  No counterpart in the
+ * reference: it exists for callers that cannot call cudaMalloc -- code whose GPU
+ * memory is owned by another allocator (a framework's caching allocator that has
+ * reserved the device), and repair loops that must not pay the device-wide
+ * synchronisation of cudaFree on every trace.  Same arguments and results as
+ * md200_group_roots; the scratch is a static 16 KiB device array (2048 doubles,
+ * held by every GPU that loads the library until exit) that must hold
+ * 7*layers + known + modes + ceil(modes/2) doubles (e.g. 256 layers with up to
+ * 100 roots and modes); larger requests fail with a message and touch nothing.  The first
+ * call on a device looks up the array's address (cudaGetSymbolAddress) -- make it
+ * before any stream capture.  Calls share the array: calls that overlap on the
+ * GPU (from several host threads or processes sharing a context) race. */
+int md200_group_roots_static(const double *thickness, const double *vp, const double *vs,
+                             const double *rho, int layers, int wave, double period,
+                             const double *roots, int known, int modes, double close_rtol,
+                             double *group, unsigned *group_flags);
+
 #ifdef __cplusplus
 }
 #endif

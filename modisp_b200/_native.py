@@ -67,6 +67,7 @@ EXPORTS = {
     "md200_device_name": (_I, [_I, ctypes.c_char_p, _I]),
     "md200_kernel_report": (_I, [_I, _I, ctypes.c_char_p, _I]),
     "md200_group_roots": (_I, [_P, _P, _P, _P, _I, _I, _D, _P, _I, _I, _D, _P, _P]),
+    "md200_group_roots_static": (_I, [_P, _P, _P, _P, _I, _I, _D, _P, _I, _I, _D, _P, _P]),
     "md200_stage_times": (_I, [_P, ctypes.POINTER(ctypes.c_double), _I]),
     "md200_kernel_launches": (_I, [_P]),
     "md200_measure_peak": (_I, [_I, _I, ctypes.POINTER(ctypes.c_double)]),
