@@ -190,7 +190,7 @@ def main():
         run_reference(args, rank, world)
         return
     import torch
-    from modisp_b200 import _native, plugin
+    from modisp_b200 import _native, plugin, sharding
 
     torch.cuda.set_device(local)
     # a dedicated stream: the engine's kernels and the timing events share it
@@ -249,18 +249,10 @@ def main():
         return total, roots
 
     def reduce_max(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
+        return sharding.reduce_max(x, dev)
 
     def reduce_sum(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t)
-        return float(t.item())
+        return sharding.reduce_sum(x, dev)
 
     # ---- FP32-scan engine: the headline ----
     e32 = engine(True)
