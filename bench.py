@@ -58,6 +58,7 @@ def parse():
     p.add_argument("--models", type=int, default=MODELS)
     p.add_argument("--cpu-sample", type=int, default=128, help="models in the CPU-baseline sample")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-jacobian", action="store_true")
     return p.parse_args()
 
 
@@ -172,6 +173,75 @@ def run_reference(args, rank, world):
                              "sample": res["sample"]},
             "e2e": {"value": value, "unit": "roots/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
+
+
+def jacobian_bench(torch, local, steps, warmup, flush):
+    """Differentiation workload: forward solve, full phase/group Jacobians and the
+    misfit gradient (vector-Jacobian product) of 4096 12-layer models, 40 periods
+    1-40 s, 3 modes, Rayleigh, timed separately with CUDA events."""
+    from modisp_b200 import _native, workloads
+    batch, periods, nmodes = workloads.config4(4096)
+    B, L = batch["thickness"].shape
+    T = periods.size
+    dev = torch.device("cuda", local)
+    f64 = torch.float64
+    x = {k: torch.tensor(batch[k], dtype=f64, device=dev) for k in ("thickness", "vp", "vs", "rho")}
+    per = torch.tensor(periods, dtype=f64, device=dev)
+    vel = torch.empty((B, nmodes, T), dtype=f64, device=dev)
+    grp = torch.empty_like(vel)
+    gfl = torch.empty((B, nmodes, T), dtype=torch.int32, device=dev)
+    i32 = [torch.empty((B, T), dtype=torch.int32, device=dev) for _ in range(3)]
+    jc = torch.empty((B, nmodes, T, 4, L), dtype=f64, device=dev)
+    ju = torch.empty_like(jc)
+    grad = torch.empty((4, B, L), dtype=f64, device=dev)
+    w = torch.ones_like(vel)
+    o = _native.default_options()
+    o.single_precision = 1
+    o.group_velocity = 1
+    eng = _native.Engine(local, B, L, T, nmodes, o)
+    stream = torch.cuda.current_stream().cuda_stream
+    ptrs = [x[k].data_ptr() for k in ("thickness", "vp", "vs", "rho")]
+
+    def forward():
+        eng.run_device(*ptrs, B, per.data_ptr(), 0, TOL, 1., 0, vel.data_ptr(), i32[0].data_ptr(),
+                       i32[1].data_ptr(), i32[2].data_ptr(), grp.data_ptr(), gfl.data_ptr(), stream=stream)
+
+    def full():
+        eng.jacobian_device(*ptrs, B, per.data_ptr(), 0, vel.data_ptr(), jc.data_ptr(), group=grp.data_ptr(),
+                            jac_group=ju.data_ptr(), stream=stream)
+
+    def vjp():
+        eng.vjp_device(*ptrs, B, per.data_ptr(), 0, vel.data_ptr(), grad.data_ptr(), weight_phase=w.data_ptr(),
+                       weight_group=w.data_ptr(), group=grp.data_ptr(), stream=stream)
+
+    def timed(fn):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        total = 0.
+        for _ in range(steps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn()
+            b.record()
+            b.synchronize()
+            total += a.elapsed_time(b)
+        return total / steps
+
+    ms_f = timed(forward)
+    roots = int(torch.isfinite(vel).sum())
+    ms_j = timed(full)
+    ms_v = timed(vjp)
+    nan_rows = int(torch.isnan(jc[..., 0, 0][torch.isfinite(vel)]).sum())
+    eng.close()
+    return {"workload": "4096 models x 12 layers + half-space, 40 periods 1-40 s, 3 modes, Rayleigh, "
+                        "Jacobians of phase and group velocity w.r.t. h, Vp, Vs, rho of every row",
+            "roots": roots, "forward_ms": ms_f, "jacobian_ms": ms_j, "vjp_ms": ms_v,
+            "jacobian_roots_per_s": roots / ((ms_f + ms_j) * 1e-3),
+            "gradient_roots_per_s": roots / ((ms_f + ms_v) * 1e-3),
+            "jacobian_cost_ratio": ms_j / ms_f, "vjp_cost_ratio": ms_v / ms_f,
+            "failed_roots": nan_rows, "unit": "roots/s"}
 
 
 def device_run(torch, eng, tens, B, wave, stream):
@@ -310,6 +380,8 @@ def main():
         h2d, d2h = 2 * per_wave_in, 2 * per_wave_out
         solver.close()
 
+    jac = jacobian_bench(torch, local, max(2, args.steps // 2), 2, flush) if not args.no_jacobian else None
+
     peak32 = _native.measure_peak(local, fp64=False)
     peak64 = _native.measure_peak(local, fp64=True)
     achieved = scan_flops / (scan_ms * 1e-3)
@@ -337,6 +409,7 @@ def main():
             "gpu_launches": launches,
             "clocks": clocks.summary(),
             "engine_stats": {"rayleigh": e32_stats[0], "love": e32_stats[1]},
+            "jacobian": jac,
         }
         print(json.dumps(line))
     if world > 1:

@@ -110,6 +110,52 @@ int md200_run_device(md200_engine *engine, const double *thickness, const double
                      unsigned *group_flags, unsigned *prediction_flags, double *bounds_out,
                      unsigned long long *stats, void *stream);
 
+/* Phase- and group-velocity Jacobians of solved roots (no counterpart in the
+ * reference, which returns no derivatives; they serve the gradient of a misfit
+ * between predicted and observed dispersion).  For every finite root
+ * velocity[b][mode][period] of models [models][layers] (the engine's geometry)
+ * at `periods`, jac_phase[b][mode][period][4][layers] receives dc/dm and
+ * jac_group (optional) dU/dm, with m the row's thickness, vp, vs, rho in that
+ * order (km/s per km, per km/s, per g/cc).  The layer tables are prepared again
+ * from the inputs; dc/dm = (c/k) F_m / F_k and dU/dm from the second
+ * derivatives of the secular function, by a forward (k, omega) sweep and an
+ * adjoint sweep through the layer recurrence (adjoint.cuh).  Rows of zero
+ * thickness (padding) and the half-space thickness get 0; NaN rows mark a
+ * missing root (or, for jac_group, a missing group velocity where `group` is
+ * given) or a root with F_k = 0 or F_omega = 0.  Models of up to 145 rows.
+ * Device pointers, enqueued on `stream` (NULL = the engine's stream). */
+int md200_jacobian_device(md200_engine *engine, const double *thickness, const double *vp,
+                          const double *vs, const double *rho, int models, const double *periods,
+                          int wave, const double *velocity, const double *group, double *jac_phase,
+                          double *jac_group, void *stream);
+
+/* Host-pointer form of md200_jacobian_device (waits for the result);
+ * `failed` (optional) receives the number of finite roots whose rows are NaN. */
+int md200_jacobian(md200_engine *engine, const double *thickness, const double *vp, const double *vs,
+                   const double *rho, int models, const double *periods, int wave,
+                   const double *velocity, const double *group, double *jac_phase,
+                   double *jac_group, int *failed);
+
+/* Vector-Jacobian product without forming the Jacobians (no counterpart in the
+ * reference): grad[4][models][layers] = sum over cells of
+ * weight_phase[cell] dc/dm + weight_group[cell] dU/dm (either weight array may
+ * be NULL; cells without a finite root, or without a finite `group` where it is
+ * given, contribute nothing).  The backward pass of a misfit: weights are the
+ * misfit's derivatives with respect to each phase and group velocity.
+ * Accumulated with atomic adds: the summation order, and so the last bits, may
+ * differ between calls.  Device pointers, enqueued on `stream`. */
+int md200_vjp_device(md200_engine *engine, const double *thickness, const double *vp,
+                     const double *vs, const double *rho, int models, const double *periods,
+                     int wave, const double *velocity, const double *group,
+                     const double *weight_phase, const double *weight_group, double *grad,
+                     void *stream);
+
+/* Host-pointer form of md200_vjp_device (waits for the result). */
+int md200_vjp(md200_engine *engine, const double *thickness, const double *vp, const double *vs,
+              const double *rho, int models, const double *periods, int wave,
+              const double *velocity, const double *group, const double *weight_phase,
+              const double *weight_group, double *grad);
+
 /* Device time (ms) of each stage of the engine's last run, from cudaEvent pairs
  * recorded on the run's stream (the reference's profile timings,
  * cpp/cuda/qe.cu:853-864): [0] model preparation, [1] trace list, [2] scan,

@@ -71,6 +71,10 @@ EXPORTS = {
     "md200_stage_times": (_I, [_P, ctypes.POINTER(ctypes.c_double), _I]),
     "md200_kernel_launches": (_I, [_P]),
     "md200_measure_peak": (_I, [_I, _I, ctypes.POINTER(ctypes.c_double)]),
+    "md200_jacobian_device": (_I, [_P, _P, _P, _P, _P, _I, _P, _I, _P, _P, _P, _P, _P]),
+    "md200_jacobian": (_I, [_P, _P, _P, _P, _P, _I, _P, _I, _P, _P, _P, _P, ctypes.POINTER(_I)]),
+    "md200_vjp_device": (_I, [_P, _P, _P, _P, _P, _I, _P, _I, _P, _P, _P, _P, _P, _P]),
+    "md200_vjp": (_I, [_P, _P, _P, _P, _P, _I, _P, _I, _P, _P, _P, _P, _P]),
 }
 STAGES = ("prep", "trace_list", "scan", "refine", "repair_select", "repair_scan", "repair_refine",
           "assemble", "group_velocity")
@@ -174,6 +178,54 @@ class Engine:
             c(prediction) if prediction else None, c(bounds_out) if bounds_out else None,
             c(stats) if stats else None, c(stream) if stream is not None else None)
         check(status)
+
+    def jacobian(self, h, vp, vs, rho, periods, wave, velocity, group=None, want_group=True):
+        """Host-array Jacobians of the roots `velocity` [B, nmodes, T]: returns
+        (jac_phase, jac_group or None, failed) with jac_* [B, nmodes, T, 4, layers]
+        (thickness, vp, vs, rho)."""
+        arrays = [np.ascontiguousarray(x, dtype=np.float64) for x in (h, vp, vs, rho)]
+        B, L = arrays[0].shape
+        per = np.ascontiguousarray(periods, dtype=np.float64)
+        vel = np.ascontiguousarray(velocity, dtype=np.float64)
+        grp = None if group is None else np.ascontiguousarray(group, dtype=np.float64)
+        shape = (B, self.nmodes, self.periods, 4, L)
+        jc = np.empty(shape)
+        ju = np.empty(shape) if want_group else None
+        failed = ctypes.c_int()
+        check(lib().md200_jacobian(self.handle, *(ptr(a) for a in arrays), B, ptr(per), int(wave), ptr(vel),
+                                   ptr(grp), ptr(jc), ptr(ju), ctypes.byref(failed)))
+        return jc, ju, int(failed.value)
+
+    def vjp(self, h, vp, vs, rho, periods, wave, velocity, weight_phase=None, weight_group=None, group=None):
+        """Host-array vector-Jacobian product: [4, B, layers] gradient."""
+        arrays = [np.ascontiguousarray(x, dtype=np.float64) for x in (h, vp, vs, rho)]
+        B, L = arrays[0].shape
+        per = np.ascontiguousarray(periods, dtype=np.float64)
+        vel = np.ascontiguousarray(velocity, dtype=np.float64)
+        conv = lambda a: None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+        wc, wu, grp = conv(weight_phase), conv(weight_group), conv(group)
+        grad = np.empty((4, B, L))
+        check(lib().md200_vjp(self.handle, *(ptr(a) for a in arrays), B, ptr(per), int(wave), ptr(vel), ptr(grp),
+                              ptr(wc), ptr(wu), ptr(grad)))
+        return grad
+
+    def jacobian_device(self, h, vp, vs, rho, models, periods, wave, velocity, jac_phase, group=None,
+                        jac_group=None, stream=None):
+        """Device-pointer Jacobians (integer addresses), enqueued on `stream`."""
+        c = ctypes.c_void_p
+        opt = lambda x: c(x) if x else None
+        check(lib().md200_jacobian_device(self.handle, c(h), c(vp), c(vs), c(rho), int(models), c(periods),
+                                          int(wave), c(velocity), opt(group), c(jac_phase), opt(jac_group),
+                                          c(stream) if stream is not None else None))
+
+    def vjp_device(self, h, vp, vs, rho, models, periods, wave, velocity, grad, weight_phase=None,
+                   weight_group=None, group=None, stream=None):
+        """Device-pointer vector-Jacobian product into grad [4, models, layers]."""
+        c = ctypes.c_void_p
+        opt = lambda x: c(x) if x else None
+        check(lib().md200_vjp_device(self.handle, c(h), c(vp), c(vs), c(rho), int(models), c(periods), int(wave),
+                                     c(velocity), opt(group), opt(weight_phase), opt(weight_group), c(grad),
+                                     c(stream) if stream is not None else None))
 
     def stage_times(self) -> dict:
         """Device milliseconds per stage of the last run (waits for it)."""

@@ -16,6 +16,7 @@
 
 #include "modisp_b200.h"
 #include "kernels.cuh"
+#include "adjoint.cuh"
 
 using namespace md200;
 
@@ -62,6 +63,9 @@ struct md200_engine {
   unsigned long long *d_stats = nullptr;
   unsigned char *pinned = nullptr;
   size_t pinned_bytes = 0;
+  // host-path Jacobian buffers (allocated on first use)
+  double *jac_c = nullptr, *jac_u = nullptr, *jac_w = nullptr, *jac_grad = nullptr;
+  int jac_blocks = 0;
   std::vector<void *> owned;
   // per-stage timing (cudaEvent pairs on the run's stream)
   static constexpr int NSTAGE = 9;
@@ -183,6 +187,13 @@ int setup(md200_engine *e) {
   return 0;
 }
 
+// Lazily allocated engine-owned buffer.
+template <class T>
+int lazy_alloc(md200_engine *e, T **p, size_t count) {
+  if (*p) return 0;
+  return own_alloc(e, p, count);
+}
+
 int validate_geometry(md200_engine *e, int models) {
   if (!e) return fail("modisp_b200: null engine");
   if (models < 1 || models > e->cap)
@@ -278,6 +289,51 @@ int enqueue(md200_engine *e, const double *h, const double *vp, const double *vs
   }
   MD200_CK(mark(9));
   e->profiling = true;
+  return 0;
+}
+
+// Jacobians of given roots: the models are prepared again (the layer tables are
+// recomputed, not kept from the solve) and one thread per output cell runs the
+// forward + adjoint sweeps.  Full Jacobians when grad is null, otherwise the
+// weighted sum over cells into grad [4][B][Lmax].
+int jacobian_enqueue(md200_engine *e, const double *h, const double *vp, const double *vs, const double *rho,
+                     int B, const double *periods, int wave, const double *vel, const double *grp, double *jc,
+                     double *ju, const double *wc, const double *wu, double *grad, cudaStream_t s) {
+  if (wave != 0 && wave != 1) return fail("modisp_b200: wave must be 0 (Rayleigh) or 1 (Love)");
+  if (e->L - 1 > JAC_MAX_STEPS)
+    return fail("modisp_b200: Jacobians support models of at most " + std::to_string(JAC_MAX_STEPS + 1) +
+                " rows");
+  if (!vel) return fail("modisp_b200: Jacobians need the roots (velocity array)");
+  MD200_CK(cudaSetDevice(e->device));
+  Dev d = e->d;
+  d.B = B;
+  d.n_traces = B * e->T;
+  d.wave = wave;
+  d.h = h;
+  d.vp = vp;
+  d.vs = vs;
+  d.rho = rho;
+  d.periods = periods;
+  d.bounds_in = nullptr;
+  d.bounds_out = nullptr;
+  d.stats = nullptr;
+  d.pred = nullptr;
+  MD200_CK(cudaMemsetAsync(d.ctr, 0, sizeof(int) * C_COUNT, s));
+  const int pw = e->prep_warps;
+  prep_models<<<(B + pw - 1) / pw, 32 * pw, e->prep_smem, s>>>(d, e->sortcap, 0);
+  MD200_CK(cudaGetLastError());
+  if (grad) MD200_CK(cudaMemsetAsync(grad, 0, sizeof(double) * 4 * static_cast<size_t>(B) * e->L, s));
+  if (!e->jac_blocks) {
+    int sms = 148, occ = 0;
+    MD200_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device));
+    MD200_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, root_jacobians<0>, 128, 0));
+    e->jac_blocks = sms * std::max(1, occ);
+  }
+  const long long cells = static_cast<long long>(B) * e->nmodes * e->T;
+  const int blocks = static_cast<int>(std::min<long long>(e->jac_blocks, (cells + 127) / 128));
+  if (wave == 0) root_jacobians<0><<<blocks, 128, 0, s>>>(d, vel, grp, jc, ju, wc, wu, grad, d.ctr + C_JFAIL);
+  else root_jacobians<1><<<blocks, 128, 0, s>>>(d, vel, grp, jc, ju, wc, wu, grad, d.ctr + C_JFAIL);
+  MD200_CK(cudaGetLastError());
   return 0;
 }
 
@@ -465,6 +521,101 @@ int md200_run(md200_engine *e, const double *h, const double *vp, const double *
   if (bounds_out) std::memcpy(bounds_out, obd, sizeof(double) * 2 * B);
   if (stats && nstats > 0)
     std::memcpy(stats, ost, sizeof(unsigned long long) * std::min(nstats, int(MD200_STAT_COUNT)));
+  return 0;
+}
+
+int md200_jacobian_device(md200_engine *e, const double *h, const double *vp, const double *vs,
+                          const double *rho, int models, const double *periods, int wave,
+                          const double *velocity, const double *group, double *jac_phase,
+                          double *jac_group, void *stream) {
+  if (validate_geometry(e, models)) return 1;
+  if (!h || !vp || !vs || !rho || !periods || !jac_phase)
+    return fail("modisp_b200: missing input or output array");
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : e->stream;
+  return jacobian_enqueue(e, h, vp, vs, rho, models, periods, wave, velocity, group, jac_phase, jac_group,
+                          nullptr, nullptr, nullptr, s);
+}
+
+int md200_vjp_device(md200_engine *e, const double *h, const double *vp, const double *vs,
+                     const double *rho, int models, const double *periods, int wave,
+                     const double *velocity, const double *group, const double *weight_phase,
+                     const double *weight_group, double *grad, void *stream) {
+  if (validate_geometry(e, models)) return 1;
+  if (!h || !vp || !vs || !rho || !periods || !grad || (!weight_phase && !weight_group))
+    return fail("modisp_b200: missing input or output array");
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : e->stream;
+  return jacobian_enqueue(e, h, vp, vs, rho, models, periods, wave, velocity, group, nullptr, nullptr,
+                          weight_phase, weight_group, grad, s);
+}
+
+namespace {
+// Host-path staging shared by md200_jacobian and md200_vjp: inputs to the
+// engine's device buffers, roots and group velocities to jac_w.
+int stage_jacobian_inputs(md200_engine *e, const double *h, const double *vp, const double *vs,
+                          const double *rho, int models, const double *periods, const double *velocity,
+                          const double *group, const double *wc, const double *wu) {
+  const size_t B = models, L = e->L, T = e->T, nm = e->nmodes, cells = B * T * nm;
+  const size_t cap_cells = static_cast<size_t>(e->cap) * T * nm;
+  if (lazy_alloc(e, &e->jac_w, 4 * cap_cells)) return 1;
+  cudaStream_t s = e->stream;
+  MD200_CK(cudaMemcpyAsync(e->in_h, h, sizeof(double) * B * L, cudaMemcpyHostToDevice, s));
+  MD200_CK(cudaMemcpyAsync(e->in_vp, vp, sizeof(double) * B * L, cudaMemcpyHostToDevice, s));
+  MD200_CK(cudaMemcpyAsync(e->in_vs, vs, sizeof(double) * B * L, cudaMemcpyHostToDevice, s));
+  MD200_CK(cudaMemcpyAsync(e->in_rho, rho, sizeof(double) * B * L, cudaMemcpyHostToDevice, s));
+  MD200_CK(cudaMemcpyAsync(e->in_per, periods, sizeof(double) * T, cudaMemcpyHostToDevice, s));
+  MD200_CK(cudaMemcpyAsync(e->jac_w, velocity, sizeof(double) * cells, cudaMemcpyHostToDevice, s));
+  if (group)
+    MD200_CK(cudaMemcpyAsync(e->jac_w + cap_cells, group, sizeof(double) * cells, cudaMemcpyHostToDevice, s));
+  if (wc) MD200_CK(cudaMemcpyAsync(e->jac_w + 2 * cap_cells, wc, sizeof(double) * cells, cudaMemcpyHostToDevice, s));
+  if (wu) MD200_CK(cudaMemcpyAsync(e->jac_w + 3 * cap_cells, wu, sizeof(double) * cells, cudaMemcpyHostToDevice, s));
+  return 0;
+}
+}  // namespace
+
+int md200_jacobian(md200_engine *e, const double *h, const double *vp, const double *vs, const double *rho,
+                   int models, const double *periods, int wave, const double *velocity, const double *group,
+                   double *jac_phase, double *jac_group, int *failed) {
+  if (validate_geometry(e, models)) return 1;
+  if (!h || !vp || !vs || !rho || !periods || !velocity || !jac_phase)
+    return fail("modisp_b200: missing input or output array");
+  MD200_CK(cudaSetDevice(e->device));
+  const size_t cap_cells = static_cast<size_t>(e->cap) * e->T * e->nmodes;
+  const size_t n = static_cast<size_t>(models) * e->T * e->nmodes * 4 * e->L;
+  if (lazy_alloc(e, &e->jac_c, cap_cells * 4 * e->L)) return 1;
+  if (jac_group && lazy_alloc(e, &e->jac_u, cap_cells * 4 * e->L)) return 1;
+  if (stage_jacobian_inputs(e, h, vp, vs, rho, models, periods, velocity, group, nullptr, nullptr)) return 1;
+  if (jacobian_enqueue(e, e->in_h, e->in_vp, e->in_vs, e->in_rho, models, e->in_per, wave, e->jac_w,
+                       group ? e->jac_w + cap_cells : nullptr, e->jac_c, jac_group ? e->jac_u : nullptr, nullptr,
+                       nullptr, nullptr, e->stream))
+    return 1;
+  int nfail = 0;
+  MD200_CK(cudaMemcpyAsync(&nfail, e->d.ctr + C_JFAIL, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+  MD200_CK(cudaStreamSynchronize(e->stream));
+  MD200_CK(cudaMemcpy(jac_phase, e->jac_c, sizeof(double) * n, cudaMemcpyDeviceToHost));
+  if (jac_group) MD200_CK(cudaMemcpy(jac_group, e->jac_u, sizeof(double) * n, cudaMemcpyDeviceToHost));
+  if (failed) *failed = nfail;
+  return 0;
+}
+
+int md200_vjp(md200_engine *e, const double *h, const double *vp, const double *vs, const double *rho,
+              int models, const double *periods, int wave, const double *velocity, const double *group,
+              const double *weight_phase, const double *weight_group, double *grad) {
+  if (validate_geometry(e, models)) return 1;
+  if (!h || !vp || !vs || !rho || !periods || !velocity || !grad || (!weight_phase && !weight_group))
+    return fail("modisp_b200: missing input or output array");
+  MD200_CK(cudaSetDevice(e->device));
+  const size_t cap_cells = static_cast<size_t>(e->cap) * e->T * e->nmodes;
+  if (lazy_alloc(e, &e->jac_grad, 4 * static_cast<size_t>(e->cap) * e->L)) return 1;
+  if (stage_jacobian_inputs(e, h, vp, vs, rho, models, periods, velocity, group, weight_phase, weight_group))
+    return 1;
+  if (jacobian_enqueue(e, e->in_h, e->in_vp, e->in_vs, e->in_rho, models, e->in_per, wave, e->jac_w,
+                       group ? e->jac_w + cap_cells : nullptr, nullptr, nullptr,
+                       weight_phase ? e->jac_w + 2 * cap_cells : nullptr,
+                       weight_group ? e->jac_w + 3 * cap_cells : nullptr, e->jac_grad, e->stream))
+    return 1;
+  MD200_CK(cudaStreamSynchronize(e->stream));
+  MD200_CK(cudaMemcpy(grad, e->jac_grad, sizeof(double) * 4 * static_cast<size_t>(models) * e->L,
+                      cudaMemcpyDeviceToHost));
   return 0;
 }
 

@@ -21,6 +21,8 @@
 #include <stdint.h>
 #include <string.h>
 
+#include <type_traits>
+
 // Device code by default; MD200_HOST_SECULAR builds the same recurrences for the
 // host (with libm in place of the device intrinsics) for CPU-side studies.
 #ifdef MD200_HOST_SECULAR
@@ -34,21 +36,35 @@ namespace md200 {
 // ---------------------------------------------------------------------------
 // Number-type helpers
 // ---------------------------------------------------------------------------
+// Forward-mode number: value and ND directional derivatives.  T may itself be a
+// Dual (nested forward mode: second derivatives, or parameter derivatives of
+// the (k, omega) derivatives used by the adjoint Jacobians).
 template <class T, int ND>
 struct Dual {
   T v;
   T d[ND];
+  Dual() = default;
+  // a constant of this number type (all derivative parts zero)
+  template <class S, typename std::enable_if<std::is_arithmetic<S>::value, int>::type = 0>
+  MD200_FN explicit Dual(S x) : v(x) {
+#pragma unroll
+    for (int i = 0; i < ND; ++i) d[i] = T(0);
+  }
 };
 
+// Value part of a number (the innermost scalar for nested duals).
 MD200_FN double val(double x) { return x; }
 MD200_FN float val(float x) { return x; }
 template <class T, int ND>
-MD200_FN T val(const Dual<T, ND> &x) { return x.v; }
+MD200_FN auto val(const Dual<T, ND> &x) { return val(x.v); }
 
 template <class T>
 struct Base { using type = T; };
 template <class T, int ND>
-struct Base<Dual<T, ND>> { using type = T; };
+struct Base<Dual<T, ND>> { using type = typename Base<T>::type; };
+
+template <class T> struct IsDual : std::false_type {};
+template <class T, int ND> struct IsDual<Dual<T, ND>> : std::true_type {};
 
 // Constants of the number type.
 template <class N> struct Lift;
@@ -61,18 +77,17 @@ template <> struct Lift<float> {
   MD200_FN static float zero() { return 0.0f; }
 };
 template <class T, int ND> struct Lift<Dual<T, ND>> {
-  MD200_FN static Dual<T, ND> make(T x) {
-    Dual<T, ND> r;
-    r.v = x;
-#pragma unroll
-    for (int i = 0; i < ND; ++i) r.d[i] = T(0);
-    return r;
-  }
-  MD200_FN static Dual<T, ND> one() { return make(T(1)); }
-  MD200_FN static Dual<T, ND> zero() { return make(T(0)); }
+  MD200_FN static Dual<T, ND> one() { return Dual<T, ND>(1); }
+  MD200_FN static Dual<T, ND> zero() { return Dual<T, ND>(0); }
 };
 template <class N> MD200_FN N lift_one() { return Lift<N>::one(); }
 template <class N> MD200_FN N lift_zero() { return Lift<N>::zero(); }
+
+// a * b + c: one rounding for the scalar types, the dual product otherwise
+MD200_FN double mul_add(double a, double b, double c) { return ::fma(a, b, c); }
+MD200_FN float mul_add(float a, float b, float c) { return fmaf(a, b, c); }
+template <class T, int ND>
+MD200_FN Dual<T, ND> mul_add(const Dual<T, ND> &a, const Dual<T, ND> &b, const Dual<T, ND> &c);
 
 #define MD200_DUAL_BINOP(OP, VALUE, DERIV)                                              \
   template <class T, int ND>                                                            \
@@ -85,8 +100,13 @@ template <class N> MD200_FN N lift_zero() { return Lift<N>::zero(); }
   }
 MD200_DUAL_BINOP(+, a.v + b.v, a.d[i] + b.d[i])
 MD200_DUAL_BINOP(-, a.v - b.v, a.d[i] - b.d[i])
-MD200_DUAL_BINOP(*, a.v * b.v, fma(a.d[i], b.v, a.v * b.d[i]))
+MD200_DUAL_BINOP(*, a.v * b.v, mul_add(a.d[i], b.v, a.v * b.d[i]))
 #undef MD200_DUAL_BINOP
+
+template <class T, int ND>
+MD200_FN Dual<T, ND> mul_add(const Dual<T, ND> &a, const Dual<T, ND> &b, const Dual<T, ND> &c) {
+  return a * b + c;
+}
 
 template <class T, int ND>
 MD200_FN Dual<T, ND> operator/(const Dual<T, ND> &a, const Dual<T, ND> &b) {
@@ -119,7 +139,7 @@ MD200_FN Dual<T, ND> operator*(T s, const Dual<T, ND> &a) { return a * s; }
 template <class T, int ND>
 MD200_FN Dual<T, ND> operator+(const Dual<T, ND> &a, T s) {
   Dual<T, ND> r = a;
-  r.v += s;
+  r.v = r.v + s;
   return r;
 }
 template <class T, int ND>
@@ -127,13 +147,47 @@ MD200_FN Dual<T, ND> operator+(T s, const Dual<T, ND> &a) { return a + s; }
 template <class T, int ND>
 MD200_FN Dual<T, ND> operator-(const Dual<T, ND> &a, T s) {
   Dual<T, ND> r = a;
-  r.v -= s;
+  r.v = r.v - s;
   return r;
 }
 template <class T, int ND>
 MD200_FN Dual<T, ND> operator-(T s, const Dual<T, ND> &a) {
   Dual<T, ND> r = -a;
-  r.v += s;
+  r.v = r.v + s;
+  return r;
+}
+// Nested duals with a plain scalar (the innermost type)
+template <class T, int ND, class S,
+          typename std::enable_if<IsDual<T>::value && std::is_arithmetic<S>::value, int>::type = 0>
+MD200_FN Dual<T, ND> operator*(const Dual<T, ND> &a, S s) {
+  Dual<T, ND> r;
+  r.v = a.v * s;
+#pragma unroll
+  for (int i = 0; i < ND; ++i) r.d[i] = a.d[i] * s;
+  return r;
+}
+template <class T, int ND, class S,
+          typename std::enable_if<IsDual<T>::value && std::is_arithmetic<S>::value, int>::type = 0>
+MD200_FN Dual<T, ND> operator*(S s, const Dual<T, ND> &a) { return a * s; }
+template <class T, int ND, class S,
+          typename std::enable_if<IsDual<T>::value && std::is_arithmetic<S>::value, int>::type = 0>
+MD200_FN Dual<T, ND> operator+(const Dual<T, ND> &a, S s) {
+  Dual<T, ND> r = a;
+  r.v = r.v + s;
+  return r;
+}
+template <class T, int ND, class S,
+          typename std::enable_if<IsDual<T>::value && std::is_arithmetic<S>::value, int>::type = 0>
+MD200_FN Dual<T, ND> operator-(const Dual<T, ND> &a, S s) {
+  Dual<T, ND> r = a;
+  r.v = r.v - s;
+  return r;
+}
+template <class T, int ND, class S,
+          typename std::enable_if<IsDual<T>::value && std::is_arithmetic<S>::value, int>::type = 0>
+MD200_FN Dual<T, ND> operator-(S s, const Dual<T, ND> &a) {
+  Dual<T, ND> r = -a;
+  r.v = r.v + s;
   return r;
 }
 
@@ -218,7 +272,7 @@ MD200_FN Dual<T, ND> m_sqrt(const Dual<T, ND> &x) {
 }
 template <class T, int ND>
 MD200_FN Dual<T, ND> m_abs(const Dual<T, ND> &x) {
-  return x.v < T(0) ? -x : x;
+  return val(x) < 0 ? -x : x;
 }
 
 // Exact power-of-two reciprocal of the binade of x (x > 0, finite, normal):
@@ -310,14 +364,24 @@ struct LayerView {
   MD200_FN T imu(int j) const { return base[6 * Ls + j]; }
 };
 
-// One upward Dunkin step through layer m: e <- e * Ca(m).
-// Returns the exponent P + Q (value part) that the scaled hyperbolic functions
-// of the evanescent branches factor out: the unscaled step is the scaled one
-// times exp(P + Q).
+// The 15 distinct entries of one layer's Dunkin compound matrix; the 5x5
+// matrix acting on the column vector e is
+//   [A E tJ F O; D B tH N F; I G K H J; C M tG B E; L C tI D A],  t = -2 k^2
+// (the column of e[2] carries t outside the K entry).
+template <class N>
+struct RayleighEntries {
+  N A, B, C, D, E, F, G, H, I, J, K, Lm, M, Nn, O;
+};
+
+// Entries of layer (h, 1/vp, vs^2, 1/vs, rho, 1/rho) at wavenumber k (k2 = k^2),
+// frequency w (iw2 = 1/w^2).  Returns the exponent P + Q (value part) that the
+// scaled hyperbolic functions of the evanescent branches factor out: the
+// unscaled matrix is the returned one times exp(P + Q).  The layer constants may
+// be plain numbers or numbers of type N (parameter derivatives).
 template <class N, class T>
-MD200_FN typename Base<N>::type rayleigh_layer(N e[5], const N &k, const N &k2, const N &w,
-                                               const N &iw2, T h, T ivp, T vs2, T ivs, T rho,
-                                               T irho) {
+MD200_FN typename Base<N>::type rayleigh_entries(RayleighEntries<N> &X, const N &k, const N &k2,
+                                                 const N &w, const N &iw2, T h, T ivp, T vs2, T ivs,
+                                                 T rho, T irho) {
   using BT = typename Base<N>::type;
   BT expo = BT(0);
   const N ka = w * ivp, kb = w * ivs;
@@ -340,7 +404,7 @@ MD200_FN typename Base<N>::type rayleigh_layer(N e[5], const N &k, const N &k2, 
     xv = lift_zero<N>();
   } else {
     const N ep = m_exp(-(ra * h));
-    expo += val(ra) * h;
+    expo += val(ra) * val(h);
     const N fac = ep * ep;
     cosp = (fac + T(1)) * T(0.5);
     const N sp = (T(1) - fac) * T(0.5);
@@ -359,7 +423,7 @@ MD200_FN typename Base<N>::type rayleigh_layer(N e[5], const N &k, const N &k2, 
     zv = lift_zero<N>();
   } else {
     const N eq = m_exp(-(rb * h));
-    expo += val(rb) * h;
+    expo += val(rb) * val(h);
     const N fac = eq * eq;
     cosq = (fac + T(1)) * T(0.5);
     const N sq = (T(1) - fac) * T(0.5);
@@ -379,31 +443,46 @@ MD200_FN typename Base<N>::type rayleigh_layer(N e[5], const N &k, const N &k2, 
   const N a0pq = a0 - cpcq;
   const T rho2 = rho * rho, irho2 = irho * irho;
 
-  // Distinct entries; the matrix is
-  //   [A D I C L; E B G M C; tJ tH K tG tI; F N H B D; O F J E A], t = -2 k^2.
-  const N A = cpcq - (gmgm1 * a0pq) * T(2) - gmgmk * xz - k2 * gm1sq * wy;
-  const N D = (k2 * cpy - cqx) * irho;
-  const N I = -(twgm1 * a0pq + gammk * xz + k2 * gm1 * wy) * irho;
-  const N C = (cpz - k2 * cqw) * irho;
-  const N Lm = -((k2 * a0pq) * T(2) + xz + k2 * k2 * wy) * irho2;
-  const N E = (gmgmk * cpz - gm1sq * cqw) * rho;
-  const N G = gammk * cpz - gm1 * cqw;
-  const N M = -wz;
-  const N Nn = -xy;
-  const N F = (gm1sq * cpy - gmgmk * cqx) * rho;
-  const N H = gm1 * cpy - gammk * cqx;
-  const N O = -((gmgmk * gm1sq * a0pq) * T(2) + gmgmk * gmgmk * xz + gm1sq * gm1sq * wy) * rho2;
-  const N J = -(gammk * gm1 * twgm1 * a0pq + gam * gammk * gammk * xz + gm1 * gm1sq * wy) * rho;
-  const N K = a0 + (cpcq - A) * T(2);
-  const N B = cpcq;
+  X.A = cpcq - (gmgm1 * a0pq) * T(2) - gmgmk * xz - k2 * gm1sq * wy;
+  X.D = (k2 * cpy - cqx) * irho;
+  X.I = -(twgm1 * a0pq + gammk * xz + k2 * gm1 * wy) * irho;
+  X.C = (cpz - k2 * cqw) * irho;
+  X.Lm = -((k2 * a0pq) * T(2) + xz + k2 * k2 * wy) * irho2;
+  X.E = (gmgmk * cpz - gm1sq * cqw) * rho;
+  X.G = gammk * cpz - gm1 * cqw;
+  X.M = -wz;
+  X.Nn = -xy;
+  X.F = (gm1sq * cpy - gmgmk * cqx) * rho;
+  X.H = gm1 * cpy - gammk * cqx;
+  X.O = -((gmgmk * gm1sq * a0pq) * T(2) + gmgmk * gmgmk * xz + gm1sq * gm1sq * wy) * rho2;
+  X.J = -(gammk * gm1 * twgm1 * a0pq + gam * gammk * gammk * xz + gm1 * gm1sq * wy) * rho;
+  X.K = a0 + (cpcq - X.A) * T(2);
+  X.B = cpcq;
+  return expo;
+}
 
+// e <- M e for the matrix of RayleighEntries.
+template <class N>
+MD200_FN void rayleigh_apply(const RayleighEntries<N> &X, const N &k2, N e[5]) {
+  using BT = typename Base<N>::type;
   const N e0 = e[0], e1 = e[1], e4 = e[4], e3 = e[3];
-  const N e2t = e[2] * (k2 * T(-2));
-  e[0] = A * e0 + E * e1 + J * e2t + F * e3 + O * e4;
-  e[1] = D * e0 + B * e1 + H * e2t + Nn * e3 + F * e4;
-  e[2] = I * e0 + G * e1 + K * e[2] + H * e3 + J * e4;
-  e[3] = C * e0 + M * e1 + G * e2t + B * e3 + E * e4;
-  e[4] = Lm * e0 + C * e1 + I * e2t + D * e3 + A * e4;
+  const N e2t = e[2] * (k2 * BT(-2));
+  e[0] = X.A * e0 + X.E * e1 + X.J * e2t + X.F * e3 + X.O * e4;
+  e[1] = X.D * e0 + X.B * e1 + X.H * e2t + X.Nn * e3 + X.F * e4;
+  e[2] = X.I * e0 + X.G * e1 + X.K * e[2] + X.H * e3 + X.J * e4;
+  e[3] = X.C * e0 + X.M * e1 + X.G * e2t + X.B * e3 + X.E * e4;
+  e[4] = X.Lm * e0 + X.C * e1 + X.I * e2t + X.D * e3 + X.A * e4;
+}
+
+// One upward Dunkin step through a layer: e <- e * Ca(m); returns P + Q as
+// rayleigh_entries does.
+template <class N, class T>
+MD200_FN typename Base<N>::type rayleigh_layer(N e[5], const N &k, const N &k2, const N &w,
+                                               const N &iw2, T h, T ivp, T vs2, T ivs, T rho,
+                                               T irho) {
+  RayleighEntries<N> X;
+  const auto expo = rayleigh_entries<N, T>(X, k, k2, w, iw2, h, ivp, vs2, ivs, rho, irho);
+  rayleigh_apply<N>(X, k2, e);
   return expo;
 }
 
@@ -523,6 +602,49 @@ MD200_FN float rayleigh_layer_evanescent(float e[5], float k, float k2, float c,
 #define MD200_EVANESCENT_RATIO 16.f
 #endif
 
+// Fluid top layer (thickness h0, 1/vp ivp0): cos and sin/r of its P phase, the
+// factors that turn the solid-stack vector into the fluid-top secular value
+// cp e[0] - wv rho0 e[1].
+template <class N, class T>
+MD200_FN void water_top(const N &k, const N &w, T h0, T ivp0, N *cp, N *wv) {
+  using B = typename Base<N>::type;
+  const N ka = w * ivp0;
+  N rf, irf;
+  radical(k, ka, &rf, &irf);
+  if (val(k) < val(ka)) {
+    N sn;
+    m_sincos(rf * h0, &sn, cp);
+    *wv = sn * irf;
+  } else if (val(k) == val(ka)) {
+    *cp = lift_one<N>();
+    *wv = lift_one<N>() * h0;
+  } else {
+    const N ez = m_exp(-(rf * h0));
+    const N z = ez * ez;
+    *cp = (z + B(1)) * B(0.5);
+    *wv = ((B(1) - z) * B(0.5)) * irf;
+  }
+}
+
+// Half-space start vector of the upward sweep (half-space 1/vp, 1/vs, vs^2, rho).
+template <class N, class T>
+MD200_FN void rayleigh_start(N e[5], const N &k, const N &k2, const N &w, const N &iw2, T ivp, T ivs,
+                             T vs2, T rh) {
+  const N ka = w * ivp, kb = w * ivs;
+  N ra, ira, rb, irb;
+  radical(k, ka, &ra, &ira);
+  radical(k, kb, &rb, &irb);
+  const N gammk = (iw2 * vs2) * T(2);
+  const N gam = gammk * k2;
+  const N gm1 = gam - T(1);
+  const N rarb = ra * rb;
+  e[0] = (gm1 * gm1 - gam * gammk * rarb) * (rh * rh);
+  e[1] = -(ra * rh);
+  e[2] = (gm1 - gammk * rarb) * rh;
+  e[3] = rb * rh;
+  e[4] = k2 - rarb;
+}
+
 // Rayleigh secular values F(k_s, w) of S samples at one frequency, with shape
 // features g = F / |e| (water top: the fluid form).  Units: k = w / c in rad/km,
 // w in rad/s.  The S recurrences are independent and interleaved layer by layer
@@ -545,20 +667,8 @@ MD200_FN void rayleigh_multi(const LayerView<T> &m, const N *k, const N &w, N *F
 #pragma unroll
   for (int s = 0; s < S; ++s) {
     k2[s] = k[s] * k[s];
-    const N ka = w * m.ivp(last), kb = w * m.ivs(last);
-    N ra, ira, rb, irb;
-    radical(k[s], ka, &ra, &ira);
-    radical(k[s], kb, &rb, &irb);
-    const N gammk = (iw2 * m.vs2(last)) * T(2);
-    const N gam = gammk * k2[s];
-    const N gm1 = gam - T(1);
     const T rh = m.rho(last);
-    const N rarb = ra * rb;
-    e[s][0] = (gm1 * gm1 - gam * gammk * rarb) * (rh * rh);
-    e[s][1] = -(ra * rh);
-    e[s][2] = (gm1 - gammk * rarb) * rh;
-    e[s][3] = rb * rh;
-    e[s][4] = k2[s] - rarb;
+    rayleigh_start<N, T>(e[s], k[s], k2[s], w, iw2, m.ivp(last), m.ivs(last), m.vs2(last), rh);
     if constexpr (sizeof(N) == sizeof(float)) {
       // single precision: the factored start vector well below the shear velocity
       const float c = w / k[s];
@@ -598,24 +708,8 @@ MD200_FN void rayleigh_multi(const LayerView<T> &m, const N *k, const N &w, N *F
   for (int s = 0; s < S; ++s) {
     if (lmag) lmag[s] = static_cast<B>(ex[s]) + ev[s] * B(1.4426950408889634);
     if (m.water) {
-      const N ka = w * m.ivp(0);
-      N rf, irf;
-      radical(k[s], ka, &rf, &irf);
-      const T h0 = m.h(0);
       N cp, wv;
-      if (val(k[s]) < val(ka)) {
-        N sn;
-        m_sincos(rf * h0, &sn, &cp);
-        wv = sn * irf;
-      } else if (val(k[s]) == val(ka)) {
-        cp = lift_one<N>();
-        wv = lift_one<N>() * h0;
-      } else {
-        const N ez = m_exp(-(rf * h0));
-        const N z = ez * ez;
-        cp = (z + B(1)) * B(0.5);
-        wv = ((B(1) - z) * B(0.5)) * irf;
-      }
+      water_top<N, T>(k[s], w, m.h(0), m.ivp(0), &cp, &wv);
       const N t0 = cp * e[s][0], t1 = wv * e[s][1] * m.rho(0);
       N pair[2] = {t0, t1};
       const int pex = scale_vector(pair, 2, tiny);
@@ -639,6 +733,36 @@ MD200_FN N rayleigh_secular(const LayerView<T> &m, const N &k, const N &w, N *sh
   N F;
   rayleigh_multi<N, T, 1>(m, &k, w, &F, shape, lmag);
   return F;
+}
+
+// Entries of one SH layer step, [[cq, z mu], [y / mu, cq]], from the radical
+// r = sqrt((k + kj)|k - kj|) (ir its reciprocal) of wavenumber k against the
+// layer's shear wavenumber kj; returns the exponent the scaled hyperbolic
+// functions factor out (value part).
+template <class N, class T>
+MD200_FN typename Base<N>::type love_entries(const N &k, const N &kj, const N &r, const N &ir, T h, N *cq,
+                                             N *y, N *z) {
+  using B = typename Base<N>::type;
+  if (val(k) < val(kj)) {
+    N sn;
+    m_sincos(r * h, &sn, cq);
+    *y = sn * ir;
+    *z = -(r * sn);
+    return B(0);
+  }
+  if (val(k) == val(kj)) {
+    *cq = lift_one<N>();
+    *y = lift_one<N>() * h;
+    *z = lift_zero<N>();
+    return B(0);
+  }
+  const N eq = m_exp(-(r * h));
+  const N f = eq * eq;
+  *cq = (f + B(1)) * B(0.5);
+  const N half = (B(1) - f) * B(0.5);
+  *y = half * ir;
+  *z = half * r;
+  return val(r) * val(h);
 }
 
 // Love secular values (SH propagator) and shape features of S samples.
@@ -681,23 +805,8 @@ MD200_FN void love_multi(const LayerView<T> &m, const N *k, const N &w, N *F, N 
         y = ir > 0.f ? half * ir : h;
         z = prop ? -(r * half) : r * half;
         ev[s] += prop ? 0.f : q;
-      } else if (val(k[s]) < val(kj)) {
-        N sn;
-        m_sincos(r * h, &sn, &cq);
-        y = sn * ir;
-        z = -(r * sn);
-      } else if (val(k[s]) == val(kj)) {
-        cq = lift_one<N>();
-        y = lift_one<N>() * h;
-        z = lift_zero<N>();
       } else {
-        const N eq = m_exp(-(r * h));
-        ev[s] += val(r) * h;
-        const N f = eq * eq;
-        cq = (f + B(1)) * B(0.5);
-        const N half = (B(1) - f) * B(0.5);
-        y = half * ir;
-        z = half * r;
+        ev[s] += love_entries<N, T>(k[s], kj, r, ir, h, &cq, &y, &z);
       }
       const N u = e[s][0] * cq + e[s][1] * z * mu;
       const N v = e[s][0] * y * imu + e[s][1] * cq;

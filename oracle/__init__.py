@@ -162,6 +162,65 @@ def parameter_derivatives(h, vp, vs, rho, period, c, wave=0):
     return out.reshape(4, L), fc.value
 
 
+def phase_jacobian(h, vp, vs, rho, period, c, wave=0):
+    """dc/dtheta [4, L] (thickness, vp, vs, rho) at a root c: -F_theta / F_c from the
+    long-double complex-step derivatives.  Rows of zero thickness are padding by the
+    engine's convention and get 0 (as does the half-space thickness)."""
+    dF, Fc = parameter_derivatives(h, vp, vs, rho, period, c, wave)
+    jac = -dF / Fc
+    padding = np.asarray(h, dtype=np.float64) == 0.
+    padding[0] = padding[-1] = False  # the first row and the half-space are always kept
+    jac[:, padding] = 0.
+    jac[0, -1] = 0.
+    return jac
+
+
+def group_jacobian_fd(h, vp, vs, rho, period, c, wave=0, rel=1e-6, window=1e-4):
+    """dU/dtheta [4, L] by central differences (relative step `rel`) of the oracle's
+    polished group velocity; each perturbed root is re-polished inside
+    c (1 -+ window).  Zero-valued parameters (padding thickness, fluid shear
+    velocity, the half-space thickness) get 0."""
+    base = [np.array(x, dtype=np.float64) for x in (h, vp, vs, rho)]
+    L = base[0].size
+    out = np.zeros((4, L))
+    for p in range(4):
+        for j in range(L):
+            if base[p][j] == 0. or (p == 0 and j == L - 1):
+                continue
+            vals = []
+            for sgn in (1., -1.):
+                a = [x.copy() for x in base]
+                a[p][j] *= 1. + sgn * rel
+                vals.append(group(*a, period, c, c * (1. - window), c * (1. + window), wave))
+            out[p, j] = (vals[0] - vals[1]) / (2. * rel * base[p][j])
+    return out
+
+
+def reference_fd_phase_jacobian(h, vp, vs, rho, periods, nmodes, wave=0, rel=1e-6, tol=1e-13):
+    """Central differences (step `rel` relative) of the reference CPU solver's roots
+    for one model: (roots [nmodes, T], dc/dtheta [nmodes, T, 4, L]).  Every
+    perturbed model is solved in one batched reference call; zero-valued
+    parameters get 0."""
+    base = [np.array(x, dtype=np.float64) for x in (h, vp, vs, rho)]
+    L = base[0].size
+    rows, index = [tuple(base)], []
+    for p in range(4):
+        for j in range(L):
+            if base[p][j] == 0. or (p == 0 and j == L - 1):
+                continue
+            for sgn in (1., -1.):
+                m = [x.copy() for x in base]
+                m[p][j] *= 1. + sgn * rel
+                rows.append(tuple(m))
+            index.append((p, j))
+    batch = [np.stack([r[i] for r in rows]) for i in range(4)]
+    out = reference_solve(*batch, np.asarray(periods, dtype=np.float64), nmodes, wave=wave, tol=tol)["phase_velocity"]
+    fd = np.zeros((nmodes, len(periods), 4, L))
+    for n, (p, j) in enumerate(index):
+        fd[:, :, p, j] = (out[1 + 2 * n] - out[2 + 2 * n]) / (2. * rel * base[p][j])
+    return out[0], fd
+
+
 def group_windows(roots, lower, upper, close_rtol=0.005):
     """Neighbour-midpoint windows and close-root flags (cpp/cpu/solver.cpp:96-103)."""
     n = len(roots)

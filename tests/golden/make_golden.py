@@ -13,6 +13,9 @@ Outputs (all small .npz files, committed):
   default group_rtol 1e-3).  Cases: the quickstart model (Rayleigh, Love),
   48-model subsets of the crustal batch (Rayleigh, Love), 48 low-velocity-layer
   models (Rayleigh, Love), six surface-water models (Rayleigh).
+* ``jac_<case>.npz``: phase-velocity Jacobians by central differences (step 1e-6
+  relative) of the reference CPU solver's roots (c_tol_rel 1e-13): four
+  config-4 models (Rayleigh), two (Love), two surface-water models (Rayleigh).
 * ``fixture_<name>.npz``: the reference test suite's own frozen fixtures
   (tests/data/accuracy_high_cpu_linux/*.npz, tests/data/witness_*.npz,
   tests/data/B10000_*.npz) repacked with their inputs and expected roots.
@@ -68,6 +71,21 @@ def water_models():
     return workloads._pad(rows, max(r[0].size for r in rows))
 
 
+def save_jacobian_case(name, batch, periods, nmodes, wave):
+    """Central differences of the reference solver's roots (the phase-velocity
+    Jacobian the engine's adjoint must reproduce)."""
+    B, L = batch["thickness"].shape
+    roots = np.full((B, nmodes, len(periods)), np.nan)
+    jac = np.zeros((B, nmodes, len(periods), 4, L))
+    for b in range(B):
+        roots[b], jac[b] = oracle.reference_fd_phase_jacobian(
+            batch["thickness"][b], batch["vp"][b], batch["vs"][b], batch["rho"][b], periods, nmodes, wave)
+    np.savez_compressed(HERE / f"jac_{name}.npz", thickness=batch["thickness"], vp=batch["vp"], vs=batch["vs"],
+                        rho=batch["rho"], periods=periods, nmodes=nmodes, wave=wave, rel_step=1e-6, tol=1e-13,
+                        phase_velocity=roots, jac_phase_fd=jac)
+    print(f"jac_{name}: {int(np.isfinite(roots).sum())} roots")
+
+
 def repack_reference_fixtures(reference: Path):
     data = reference / "tests" / "data"
     for path in sorted((data / "accuracy_high_cpu_linux").glob("*.npz")):
@@ -102,6 +120,10 @@ def main():
     save_reference_case("lvz48_rayleigh", subset(lvz, np.arange(48)), periods, nmodes, 0)
     save_reference_case("lvz48_love", subset(lvz, np.arange(48)), periods, nmodes, 1)
     save_reference_case("water6_rayleigh", water_models(), np.geomspace(0.2, 20., 24), 4, 0)
+    c4, periods4, nmodes4 = workloads.config4(16)
+    save_jacobian_case("config4_rayleigh", subset(c4, np.arange(4)), periods4, nmodes4, 0)
+    save_jacobian_case("config4_love", subset(c4, np.arange(4, 6)), periods4, nmodes4, 1)
+    save_jacobian_case("water_rayleigh", subset(water_models(), np.arange(2)), np.geomspace(0.5, 20., 12), 3, 0)
     repack_reference_fixtures(Path(args.reference))
 
 

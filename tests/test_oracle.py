@@ -212,3 +212,65 @@ def test_complex_step_matches_finite_differences(oracle_lib):
     ratio_fd = ((fp - fm) / (2 * eps)) / ((cp - cm) / (2e-7 * c))
     assert abs(ratio_fd) > 1e-3
     assert abs(ratio_fd - dth[2, j] / dfdc) < 1e-4 * abs(ratio_fd)
+
+
+@pytest.mark.parametrize("wave", [0, 1])
+def test_phase_jacobian_matches_reference_finite_differences(wave, oracle_lib, reference_engine):
+    """The oracle's implicit-function Jacobian dc/dm = -F_m / F_c equals central
+    differences (step 1e-6 relative) of the reference solver's roots."""
+    rng = np.random.default_rng(41 + wave)
+    n = 6
+    vs = np.linspace(rng.uniform(.3, 1.), rng.uniform(3.5, 4.7), n + 1) * rng.uniform(.9, 1.1, n + 1)
+    vs[-1] = max(vs[-1], vs[:-1].max() * 1.02)
+    vp = vs * rng.uniform(1.7, 2., n + 1)
+    rho = 1.74 * vp ** .25
+    h = rng.uniform(.2, 3., n + 1)
+    h[-1] = 0.
+    periods = np.geomspace(1., 40., 6)
+    roots, fd = oracle_lib.reference_fd_phase_jacobian(h, vp, vs, rho, periods, 3, wave)
+    checked = 0
+    for m in range(3):
+        for f, period in enumerate(periods):
+            c = roots[m, f]
+            if not np.isfinite(c):
+                continue
+            jac = oracle_lib.phase_jacobian(h, vp, vs, rho, period, c, wave)
+            scale = np.abs(jac).max()
+            assert np.abs(jac - fd[m, f]).max() < 1e-6 * scale, (m, f)
+            checked += 1
+    assert checked >= 10
+
+
+def test_group_jacobian_differences_are_converged(oracle_lib):
+    """Central differences of the polished group velocity agree at two step sizes
+    (1e-6 and 1e-5 relative) to well inside the tolerance the engine is held to."""
+    h = np.array([0.3, 1.2, 0.]); vp = np.array([2., 3.5, 6.]); vs = np.array([.8, 2., 3.4])
+    rho = 1.74 * vp ** .25
+    for wave in (0, 1):
+        lo, hi = oracle_lib.bounds(h, vp, vs, rho, wave)[0]
+        n, roots = oracle_lib.dense_roots(h, vp, vs, rho, 3.0, lo, hi, 3, 1e-14, wave)
+        for c in roots[:n]:
+            a = oracle_lib.group_jacobian_fd(h, vp, vs, rho, 3.0, c, wave, rel=1e-6)
+            b = oracle_lib.group_jacobian_fd(h, vp, vs, rho, 3.0, c, wave, rel=1e-5)
+            assert np.abs(a - b).max() < 1e-7 * np.abs(a).max()
+
+
+@pytest.mark.parametrize("name", ["jac_config4_rayleigh", "jac_config4_love", "jac_water_rayleigh"])
+def test_jacobian_fixtures_agree_with_the_oracle(name, oracle_lib):
+    """The committed finite-difference Jacobians of the reference solver agree with
+    the oracle's implicit-function Jacobians at every recorded root."""
+    g = load_golden(name)
+    wave = int(g["wave"])
+    v = g["phase_velocity"]
+    worst, checked = 0., 0
+    for b in range(v.shape[0]):
+        model = [g[k][b] for k in ("thickness", "vp", "vs", "rho")]
+        for m in range(v.shape[1]):
+            for f, period in enumerate(g["periods"]):
+                c = v[b, m, f]
+                if not np.isfinite(c):
+                    continue
+                jac = oracle_lib.phase_jacobian(*model, period, c, wave)
+                worst = max(worst, np.abs(jac - g["jac_phase_fd"][b, m, f]).max() / np.abs(jac).max())
+                checked += 1
+    assert checked > 50 and worst < 1e-6
