@@ -100,7 +100,8 @@ int md200_run(md200_engine *engine, const double *thickness, const double *vp, c
               int nstats);
 
 /* As md200_run, but every array is a device pointer and the work is enqueued on
- * `stream` (a cudaStream_t; NULL selects the engine's own stream) without a host
+ * `stream` (a cudaStream_t; NULL selects the engine's own stream, cudaStreamLegacy the
+ * legacy default stream) without a host
  * synchronisation.  stats, if given, is a device array of MD200_STAT_COUNT
  * counters. */
 int md200_run_device(md200_engine *engine, const double *thickness, const double *vp,

@@ -117,6 +117,18 @@ def default_options() -> Options:
     return o
 
 
+# cudaStreamLegacy: the legacy default stream.  The C ABI reads a NULL stream as
+# "the engine's own stream", so handle 0 (torch's default stream) is passed as
+# the legacy-stream handle instead.
+CUDA_STREAM_LEGACY = 1
+
+
+def _stream_arg(stream):
+    if stream is None:
+        return None
+    return ctypes.c_void_p(int(stream) if int(stream) != 0 else CUDA_STREAM_LEGACY)
+
+
 def ptr(a: np.ndarray | None):
     return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
 
@@ -176,7 +188,7 @@ class Engine:
             float(tol), float(accept), int(wave), c(velocity), c(flags), c(levels), c(counts),
             c(group) if group else None, c(group_flags) if group_flags else None,
             c(prediction) if prediction else None, c(bounds_out) if bounds_out else None,
-            c(stats) if stats else None, c(stream) if stream is not None else None)
+            c(stats) if stats else None, _stream_arg(stream))
         check(status)
 
     def jacobian(self, h, vp, vs, rho, periods, wave, velocity, group=None, want_group=True):
@@ -216,7 +228,7 @@ class Engine:
         opt = lambda x: c(x) if x else None
         check(lib().md200_jacobian_device(self.handle, c(h), c(vp), c(vs), c(rho), int(models), c(periods),
                                           int(wave), c(velocity), opt(group), c(jac_phase), opt(jac_group),
-                                          c(stream) if stream is not None else None))
+                                          _stream_arg(stream)))
 
     def vjp_device(self, h, vp, vs, rho, models, periods, wave, velocity, grad, weight_phase=None,
                    weight_group=None, group=None, stream=None):
@@ -225,7 +237,7 @@ class Engine:
         opt = lambda x: c(x) if x else None
         check(lib().md200_vjp_device(self.handle, c(h), c(vp), c(vs), c(rho), int(models), c(periods), int(wave),
                                      c(velocity), opt(group), opt(weight_phase), opt(weight_group), c(grad),
-                                     c(stream) if stream is not None else None))
+                                     _stream_arg(stream)))
 
     def stage_times(self) -> dict:
         """Device milliseconds per stage of the last run (waits for it)."""

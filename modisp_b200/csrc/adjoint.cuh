@@ -12,31 +12,37 @@
 // leaves unchanged on the root curve, so the Jacobians are those of the
 // reference function.
 //
-// Per root (one thread):
-//  1. forward sweep with second-order duals in (k, omega): F, F_k, F_w, F_kk,
-//     F_kw; the per-layer scale exponents are recorded and the (k, omega)-dual
-//     state vector is checkpointed every JAC_SEG layers;
-//  2. reverse sweep, top to bottom: the layer's states are recomputed from the
-//     checkpoint (the layer matrices are recomputed, never stored), the adjoint
-//     vector runs through the transposed layer matrix, and the layer's four
-//     parameter derivatives of (F, F_k, F_w) come from the layer matrix in
-//     nested duals (outer: h, vp, vs, rho of this row; inner: k, omega)
-//     contracted with the adjoint and the state -- forward-over-reverse.
+// Per root (one thread), all arithmetic on D2 = (value, d/dk, d/domega) numbers:
+//  1. forward sweep with an extra k-direction on top of D2: F, F_k, F_w, F_kk,
+//     F_kw; the per-layer scale exponents are recorded and the D2 state vector
+//     is checkpointed every JAC_SEG layers;
+//  2. reverse sweep, top to bottom: each segment's states are recomputed from
+//     its checkpoint (the layer matrices are recomputed, never stored), and the
+//     hand-written adjoint of the layer step -- the transposed compound matrix
+//     for the adjoint vector, then reverse accumulation through the 15 entry
+//     polynomials into the wave blocks and the material constants -- yields the
+//     row's derivatives of (F, F_k, F_w): the D2 parts of the adjoint carry the
+//     (k, omega) derivatives of the parameter gradient (forward-over-reverse).
 #pragma once
 #include "engine.cuh"
 #include "secular.cuh"
 
 #ifdef MD200_HOST_SECULAR
 #define MD200_HD __host__ __device__
+#define MD200_OUTLINE __host__ __device__
 #else
 #define MD200_HD __device__
+// the layer steps of the Jacobian sweeps are called, not inlined: each gets the
+// whole register file instead of competing with the sweep's bookkeeping
+#define MD200_OUTLINE __device__ __noinline__
 #endif
 
 namespace md200 {
 
 using D2 = Dual<double, 2>;  // value, d/dk, d/domega
-using DD = Dual<D2, 2>;      // second order in (k, omega)
-using P4 = Dual<D2, 4>;      // d/d(h, vp, vs, rho) of one row, of (k, omega) duals
+using K1 = Dual<D2, 1>;      // ... and d/dk of all three (second order in k)
+using Q2 = Dual<D2, 2>;      // d/d(h, 1/v) of one wave block
+using P4 = Dual<D2, 4>;      // d/d(h, vp, vs, rho) of one row (start vector, fluid top)
 
 constexpr int JAC_SEG = 12;     // layer steps per recomputed segment
 constexpr int JAC_MAXSEG = 12;  // checkpoints: up to 144 layer steps (145 rows)
@@ -59,11 +65,11 @@ MD200_FN double pow2(int e) { return scalbn(1.0, e); }
 
 // A row's constants as nested duals in its own (h, vp, vs, rho).
 struct RowP4 {
-  P4 h, ivp, ivs, vs2, rho, irho, mu, imu;
+  P4 h, ivp, ivs, vs2, rho, irho;
 };
 MD200_FN RowP4 row_p4(const double *tab, int Ls, int j) {
   const double h = tab[j], ivp = tab[Ls + j], ivs = tab[2 * Ls + j], vs2 = tab[3 * Ls + j];
-  const double rho = tab[4 * Ls + j], irho = tab[5 * Ls + j], imu = tab[6 * Ls + j], vs = tab[8 * Ls + j];
+  const double rho = tab[4 * Ls + j], irho = tab[5 * Ls + j], vs = tab[8 * Ls + j];
   RowP4 r;
   r.h = seed4(h, 0, 1.);
   r.ivp = seed4(ivp, 1, -ivp * ivp);
@@ -71,31 +77,219 @@ MD200_FN RowP4 row_p4(const double *tab, int Ls, int j) {
   r.vs2 = seed4(vs2, 2, 2. * vs);
   r.rho = seed4(rho, 3, 1.);
   r.irho = seed4(irho, 3, -irho * irho);
-  r.mu = r.rho * r.vs2;
-  r.imu = P4(imu);
-  if (vs > 0.) {
-    r.imu.d[2] = D2(-2. * imu / vs);
-    r.imu.d[3] = D2(-imu / rho);
-  }
   return r;
 }
 
-// e <- M^T lam for the matrix of RayleighEntries (value parts of P4 entries).
-MD200_FN void rayleigh_apply_transpose(const RayleighEntries<P4> &X, const D2 &k2, D2 lam[5]) {
-  const D2 t = k2 * -2.;
-  const D2 l0 = lam[0], l1 = lam[1], l2 = lam[2], l3 = lam[3], l4 = lam[4];
-  lam[0] = X.A.v * l0 + X.D.v * l1 + X.I.v * l2 + X.C.v * l3 + X.Lm.v * l4;
-  lam[1] = X.E.v * l0 + X.B.v * l1 + X.G.v * l2 + X.M.v * l3 + X.C.v * l4;
-  lam[2] = t * (X.J.v * l0 + X.H.v * l1 + X.G.v * l3 + X.I.v * l4) + X.K.v * l2;
-  lam[3] = X.F.v * l0 + X.Nn.v * l1 + X.H.v * l2 + X.B.v * l3 + X.D.v * l4;
-  lam[4] = X.O.v * l0 + X.F.v * l1 + X.J.v * l2 + X.E.v * l3 + X.A.v * l4;
+// One wave block with its derivatives along (h, 1/v): cs, sr, rs, scale.
+struct BlockQ {
+  Q2 cs, sr, rs, sc;
+};
+MD200_FN void block_q(const D2 &k, const D2 &w, double h, double iv, BlockQ &b) {
+  Q2 kq, wq, hq(h), ivq(iv);
+  kq.v = k;
+  kq.d[0] = kq.d[1] = D2(0);
+  wq.v = w;
+  wq.d[0] = wq.d[1] = D2(0);
+  hq.d[0] = D2(1);
+  ivq.d[1] = D2(1);
+  const Q2 kv = wq * ivq;
+  wave_block<Q2, Q2>(kq, kv, hq, &b.cs, &b.sr, &b.rs, &b.sc);
 }
 
 // Derivatives of (F, F_k, F_w) along one row's parameters, as D2 numbers
-// (value: F_m; d[0]: F_km; d[1]: F_wm).
+// (value: F_m; d[0]: F_km; d[1]: F_wm), for m = h, vp, vs, rho.
 struct RowGrad {
   D2 g[4];
 };
+
+// Reverse step through one Rayleigh layer.  s: the state before the step; lam:
+// the adjoint of the (scaled) state after it, replaced by the adjoint of s;
+// r: the step's power-of-two scale.  Returns the row's derivatives.
+MD200_OUTLINE RowGrad rayleigh_layer_adjoint(const D2 &k, const D2 &k2, const D2 &w, const D2 &iw2, double h,
+                                             double ivp, double ivs, double vs2, double vs, double rho,
+                                             double irho, const D2 s[5], D2 lam[5], double r) {
+  BlockQ P, S;
+  block_q(k, w, h, ivp, P);
+  block_q(k, w, h, ivs, S);
+  const D2 cosp = P.cs.v, wv = P.sr.v, xv = P.rs.v, a0p = P.sc.v;
+  const D2 cosq = S.cs.v, yv = S.sr.v, zv = S.rs.v, a0s = S.sc.v;
+  const D2 a0 = a0p * a0s;
+  const D2 gammk = (iw2 * vs2) * 2.;
+  const D2 gam = gammk * k2;
+  RayleighEntries<D2> X;
+  rayleigh_poly<D2, double>(X, cosp, wv, xv, cosq, yv, zv, a0, gam, gammk, k2, rho, irho);
+
+  // adjoint of M s, scaled: W_X = sum over the positions of entry X of lam_row s_col
+  D2 lr[5];
+  for (int i = 0; i < 5; ++i) lr[i] = lam[i] * r;
+  const D2 t = k2 * -2.;
+  const D2 s2t = s[2] * t;
+  const D2 WA = lr[0] * s[0] + lr[4] * s[4], WE = lr[0] * s[1] + lr[3] * s[4];
+  const D2 WJ = lr[0] * s2t + lr[2] * s[4], WF = lr[0] * s[3] + lr[1] * s[4];
+  const D2 WO = lr[0] * s[4], WD = lr[1] * s[0] + lr[4] * s[3], WB = lr[1] * s[1] + lr[3] * s[3];
+  const D2 WH = lr[1] * s2t + lr[2] * s[3], WN = lr[1] * s[3], WI = lr[2] * s[0] + lr[4] * s2t;
+  const D2 WG = lr[2] * s[1] + lr[3] * s2t, WK = lr[2] * s[2], WC = lr[3] * s[0] + lr[4] * s[1];
+  const D2 WM = lr[3] * s[1], WL = lr[4] * s[0];
+
+  // adjoint vector through the transposed matrix
+  const D2 tcol = X.J * lr[0] + X.H * lr[1] + X.G * lr[3] + X.I * lr[4];
+  lam[0] = X.A * lr[0] + X.D * lr[1] + X.I * lr[2] + X.C * lr[3] + X.Lm * lr[4];
+  lam[1] = X.E * lr[0] + X.B * lr[1] + X.G * lr[2] + X.M * lr[3] + X.C * lr[4];
+  lam[2] = t * tcol + X.K * lr[2];
+  lam[3] = X.F * lr[0] + X.Nn * lr[1] + X.H * lr[2] + X.B * lr[3] + X.D * lr[4];
+  lam[4] = X.O * lr[0] + X.F * lr[1] + X.J * lr[2] + X.E * lr[3] + X.A * lr[4];
+
+  // density: each entry is rho^n times a density-free polynomial
+  const D2 brho = ((X.E * WE + X.F * WF + X.J * WJ) + X.O * WO * 2. - (X.D * WD + X.I * WI + X.C * WC) -
+                   X.Lm * WL * 2.) * irho;
+
+  // reverse through the entry polynomials
+  const D2 cpcq = cosp * cosq, cpy = cosp * yv, cpz = cosp * zv, cqw = cosq * wv, cqx = cosq * xv;
+  const D2 xy = xv * yv, xz = xv * zv, wy = wv * yv, wz = wv * zv;
+  const D2 gm1 = gam - 1., twgm1 = gam + gm1, gmgmk = gam * gammk, gmgm1 = gam * gm1, gm1sq = gm1 * gm1;
+  const D2 a0pq = a0 - cpcq;
+  const double rho2 = rho * rho, irho2 = irho * irho;
+  const D2 z0(0);
+  const D2 bA = WA - WK * 2.;  // K = a0 + 2 cpcq - 2 A
+  D2 b_a0 = WK, b_cpcq = WK * 2. + WB + bA;
+  D2 b_gmgm1 = -(a0pq * bA) * 2., b_a0pq = -(gmgm1 * bA) * 2., b_gmgmk = -(xz * bA), b_xz = -(gmgmk * bA);
+  D2 b_gm1sq = -(k2 * wy * bA), b_wy = -(k2 * gm1sq * bA);
+  D2 b_cpy = z0, b_cqx = z0, b_twgm1 = z0, b_gammk = z0, b_gm1 = z0, b_cpz = z0, b_cqw = z0, b_gam = z0;
+  {  // D = (k2 cpy - cqx) / rho
+    const D2 d = WD * irho;
+    b_cpy = b_cpy + k2 * d;
+    b_cqx = b_cqx - d;
+  }
+  {  // I = -(twgm1 a0pq + gammk xz + k2 gm1 wy) / rho
+    const D2 d = -(WI * irho);
+    b_twgm1 = b_twgm1 + a0pq * d;
+    b_a0pq = b_a0pq + twgm1 * d;
+    b_gammk = b_gammk + xz * d;
+    b_xz = b_xz + gammk * d;
+    b_gm1 = b_gm1 + k2 * wy * d;
+    b_wy = b_wy + k2 * gm1 * d;
+  }
+  {  // C = (cpz - k2 cqw) / rho
+    const D2 d = WC * irho;
+    b_cpz = b_cpz + d;
+    b_cqw = b_cqw - k2 * d;
+  }
+  {  // Lm = -(2 k2 a0pq + xz + k2^2 wy) / rho^2
+    const D2 d = -(WL * irho2);
+    b_a0pq = b_a0pq + k2 * d * 2.;
+    b_xz = b_xz + d;
+    b_wy = b_wy + k2 * k2 * d;
+  }
+  {  // E = (gmgmk cpz - gm1sq cqw) rho
+    const D2 d = WE * rho;
+    b_gmgmk = b_gmgmk + cpz * d;
+    b_cpz = b_cpz + gmgmk * d;
+    b_gm1sq = b_gm1sq - cqw * d;
+    b_cqw = b_cqw - gm1sq * d;
+  }
+  {  // G = gammk cpz - gm1 cqw
+    b_gammk = b_gammk + cpz * WG;
+    b_cpz = b_cpz + gammk * WG;
+    b_gm1 = b_gm1 - cqw * WG;
+    b_cqw = b_cqw - gm1 * WG;
+  }
+  const D2 b_wz = -WM, b_xy = -WN;  // M = -wz, Nn = -xy
+  {  // F = (gm1sq cpy - gmgmk cqx) rho
+    const D2 d = WF * rho;
+    b_gm1sq = b_gm1sq + cpy * d;
+    b_cpy = b_cpy + gm1sq * d;
+    b_gmgmk = b_gmgmk - cqx * d;
+    b_cqx = b_cqx - gmgmk * d;
+  }
+  {  // H = gm1 cpy - gammk cqx
+    b_gm1 = b_gm1 + cpy * WH;
+    b_cpy = b_cpy + gm1 * WH;
+    b_gammk = b_gammk - cqx * WH;
+    b_cqx = b_cqx - gammk * WH;
+  }
+  {  // O = -(2 gmgmk gm1sq a0pq + gmgmk^2 xz + gm1sq^2 wy) rho^2
+    const D2 d = -(WO * rho2);
+    b_gmgmk = b_gmgmk + (gm1sq * a0pq + gmgmk * xz) * d * 2.;
+    b_gm1sq = b_gm1sq + (gmgmk * a0pq + gm1sq * wy) * d * 2.;
+    b_a0pq = b_a0pq + gmgmk * gm1sq * d * 2.;
+    b_xz = b_xz + gmgmk * gmgmk * d;
+    b_wy = b_wy + gm1sq * gm1sq * d;
+  }
+  {  // J = -(gammk gm1 twgm1 a0pq + gam gammk^2 xz + gm1 gm1sq wy) rho
+    const D2 d = -(WJ * rho);
+    b_gammk = b_gammk + (gm1 * twgm1 * a0pq + gam * gammk * xz * 2.) * d;
+    b_gm1 = b_gm1 + (gammk * twgm1 * a0pq + gm1sq * wy) * d;
+    b_twgm1 = b_twgm1 + gammk * gm1 * a0pq * d;
+    b_a0pq = b_a0pq + gammk * gm1 * twgm1 * d;
+    b_gam = b_gam + gammk * gammk * xz * d;
+    b_xz = b_xz + gam * gammk * gammk * d;
+    b_gm1sq = b_gm1sq + gm1 * wy * d;
+    b_wy = b_wy + gm1 * gm1sq * d;
+  }
+  // intermediates, in reverse order of their definitions
+  b_a0 = b_a0 + b_a0pq;
+  b_cpcq = b_cpcq - b_a0pq;
+  b_gm1 = b_gm1 + gm1 * b_gm1sq * 2.;
+  b_gam = b_gam + gm1 * b_gmgm1 + gammk * b_gmgmk + b_twgm1;
+  b_gm1 = b_gm1 + gam * b_gmgm1 + b_twgm1;
+  b_gammk = b_gammk + gam * b_gmgmk;
+  b_gam = b_gam + b_gm1;
+  b_gammk = b_gammk + k2 * b_gam;
+  const D2 b_vs2 = iw2 * b_gammk * 2.;
+  // products of the wave blocks
+  const D2 b_cosp = b_cpcq * cosq + b_cpy * yv + b_cpz * zv;
+  const D2 b_cosq = b_cpcq * cosp + b_cqw * wv + b_cqx * xv;
+  const D2 b_wv = b_cqw * cosq + b_wy * yv + b_wz * zv;
+  const D2 b_xv = b_cqx * cosq + b_xy * yv + b_xz * zv;
+  const D2 b_yv = b_cpy * cosp + b_xy * xv + b_wy * wv;
+  const D2 b_zv = b_cpz * cosp + b_xz * xv + b_wz * wv;
+  const D2 b_a0p = b_a0 * a0s, b_a0s = b_a0 * a0p;
+  RowGrad g;
+  D2 cp[2], cs[2];
+  for (int q = 0; q < 2; ++q) {
+    cp[q] = b_cosp * P.cs.d[q] + b_wv * P.sr.d[q] + b_xv * P.rs.d[q] + b_a0p * P.sc.d[q];
+    cs[q] = b_cosq * S.cs.d[q] + b_yv * S.sr.d[q] + b_zv * S.rs.d[q] + b_a0s * S.sc.d[q];
+  }
+  g.g[0] = cp[0] + cs[0];
+  g.g[1] = cp[1] * (-ivp * ivp);
+  g.g[2] = cs[1] * (-ivs * ivs) + b_vs2 * (2. * vs);
+  g.g[3] = brho;
+  return g;
+}
+
+// Reverse step through one SH layer (u = e0 cq + e1 z mu, v = e0 y / mu + e1 cq).
+MD200_OUTLINE RowGrad love_layer_adjoint(const D2 &k, const D2 &w, double h, double ivs, double vs, double rho,
+                                         double vs2, double imu, const D2 s[2], D2 lam[2], double r) {
+  BlockQ S;
+  block_q(k, w, h, ivs, S);
+  const D2 cq = S.cs.v, y = S.sr.v, z = S.rs.v;
+  const double mu = rho * vs2;
+  const D2 l0 = lam[0] * r, l1 = lam[1] * r;
+  lam[0] = l0 * cq + l1 * (y * imu);
+  lam[1] = l0 * (z * mu) + l1 * cq;
+  const D2 b_cq = l0 * s[0] + l1 * s[1], b_z = l0 * s[1] * mu, b_y = l1 * s[0] * imu;
+  const D2 b_mu = l0 * s[1] * z, b_imu = l1 * s[0] * y;
+  D2 c[2];
+  for (int q = 0; q < 2; ++q) c[q] = b_cq * S.cs.d[q] + b_y * S.sr.d[q] + b_z * S.rs.d[q];
+  RowGrad g;
+  g.g[0] = c[0];
+  g.g[1] = D2(0);
+  g.g[2] = c[1] * (-ivs * ivs) + b_mu * (2. * rho * vs) + b_imu * (-2. * imu / vs);
+  g.g[3] = b_mu * vs2 + b_imu * (-imu / rho);
+  return g;
+}
+
+// Forward layer steps of the Jacobian sweeps (out of line).
+MD200_OUTLINE int rayleigh_step_k1(K1 e[5], const K1 &k, const K1 &k2, const K1 &w, const K1 &iw2, double h,
+                                   double ivp, double vs2, double ivs, double rho, double irho) {
+  rayleigh_layer<K1, double>(e, k, k2, w, iw2, h, ivp, vs2, ivs, rho, irho);
+  return scale_vector(e, 5, 1e-40);
+}
+MD200_OUTLINE void rayleigh_step_d2(D2 e[5], const D2 &k, const D2 &k2, const D2 &w, const D2 &iw2, double h,
+                                    double ivp, double vs2, double ivs, double rho, double irho, double r) {
+  rayleigh_layer<D2, double>(e, k, k2, w, iw2, h, ivp, vs2, ivs, rho, irho);
+  for (int i = 0; i < 5; ++i) e[i] = e[i] * r;
+}
 
 // Per-root quantities of the forward sweep.
 struct RootForward {
@@ -106,64 +300,61 @@ struct RootForward {
 // compact row's parameter derivatives (top row first, half-space last).
 template <int WAVE, class Sink>
 MD200_HD bool root_adjoint(const LayerView<double> &m, const double *tab, double w, double c,
-                             RootForward &fw, Sink &&sink) {
+                           RootForward &fw, Sink &&sink) {
   const int L = m.L, Ls = m.Ls, last = L - 1, top = m.water;
   const int nsteps = last - top;  // layer steps (rows last-1 .. top)
   if (nsteps > JAC_MAX_STEPS) return false;
   const double tiny = 1e-40;
-  const double k0 = w / c;
-  // (k, omega) duals and their second-order lifts
+  constexpr int NV = WAVE ? 2 : 5;
+  // (k, omega) duals and their k-lifts
   D2 k, wd;
-  k.v = k0; k.d[0] = 1.; k.d[1] = 0.;
+  k.v = w / c; k.d[0] = 1.; k.d[1] = 0.;
   wd.v = w; wd.d[0] = 0.; wd.d[1] = 1.;
   const D2 iw = D2(1) / wd, iw2 = iw * iw, k2 = k * k;
-  DD kk, ww;
-  kk.v = k; kk.d[0] = D2(1); kk.d[1] = D2(0);
-  ww.v = wd; ww.d[0] = D2(0); ww.d[1] = D2(1);
-  const DD iwx = DD(1) / ww, iw2x = iwx * iwx, k2x = kk * kk;
+  K1 kk, ww;
+  kk.v = k; kk.d[0] = D2(1);
+  ww.v = wd; ww.d[0] = D2(0);
+  const K1 iwx = K1(1) / ww, iw2x = iwx * iwx, k2x = kk * kk;
 
-  D2 ck[JAC_MAXSEG][5];
+  D2 ck[JAC_MAXSEG][NV];
   int ex[JAC_MAX_STEPS];
   int ex0 = 0, pex = 0;
-  constexpr int NV = WAVE ? 2 : 5;
 
-  // ---- 1. forward sweep (second order), exponents and checkpoints ----
-  DD e[NV];
+  // ---- 1. forward sweep, exponents and checkpoints ----
+  K1 e[NV];
   if constexpr (WAVE == 0) {
-    rayleigh_start<DD, double>(e, kk, k2x, ww, iw2x, m.ivp(last), m.ivs(last), m.vs2(last), m.rho(last));
+    rayleigh_start<K1, double>(e, kk, k2x, ww, iw2x, m.ivp(last), m.ivs(last), m.vs2(last), m.rho(last));
+    ex0 = scale_vector(e, 5, tiny);
   } else {
-    const DD kb = ww * m.ivs(last);
-    DD r, ir;
+    const K1 kb = ww * m.ivs(last);
+    K1 r, ir;
     radical(kk, kb, &r, &ir);
     e[0] = r * m.rho(last);
-    e[1] = DD(1) * (m.ivs(last) * m.ivs(last));
+    e[1] = K1(1) * (m.ivs(last) * m.ivs(last));
   }
-  if constexpr (WAVE == 0) ex0 = scale_vector(e, 5, tiny);
   for (int s = 0; s < nsteps; ++s) {
     const int l = last - 1 - s;
     if (s % JAC_SEG == 0)
       for (int i = 0; i < NV; ++i) ck[s / JAC_SEG][i] = e[i].v;
     if constexpr (WAVE == 0) {
-      rayleigh_layer<DD, double>(e, kk, k2x, ww, iw2x, m.h(l), m.ivp(l), m.vs2(l), m.ivs(l), m.rho(l), m.irho(l));
+      ex[s] = rayleigh_step_k1(e, kk, k2x, ww, iw2x, m.h(l), m.ivp(l), m.vs2(l), m.ivs(l), m.rho(l), m.irho(l));
     } else {
-      const DD kj = ww * m.ivs(l);
-      DD r, ir, cq, y, z;
-      radical(kk, kj, &r, &ir);
-      love_entries<DD, double>(kk, kj, r, ir, m.h(l), &cq, &y, &z);
+      const K1 kj = ww * m.ivs(l);
+      K1 cq, y, z;
+      love_entries<K1, double>(kk, kj, m.h(l), &cq, &y, &z);
       const double mu = m.rho(l) * m.vs2(l);
-      const DD u = e[0] * cq + e[1] * z * mu;
-      const DD v = e[0] * y * m.imu(l) + e[1] * cq;
+      const K1 u = e[0] * cq + e[1] * z * mu;
+      const K1 v = e[0] * y * m.imu(l) + e[1] * cq;
       e[0] = u;
       e[1] = v;
+      ex[s] = scale_vector(e, NV, tiny);
     }
-    ex[s] = scale_vector(e, NV, tiny);
   }
-  // top: the secular value as a function of the final state
-  DD F;
-  DD cpx, wvx;
+  K1 F;
   if (WAVE == 0 && top) {
-    water_top<DD, double>(kk, ww, m.h(0), m.ivp(0), &cpx, &wvx);
-    DD pair[2] = {cpx * e[0], wvx * e[1] * m.rho(0)};
+    K1 cpx, wvx;
+    water_top<K1, double>(kk, ww, m.h(0), m.ivp(0), &cpx, &wvx);
+    K1 pair[2] = {cpx * e[0], wvx * e[1] * m.rho(0)};
     pex = scale_vector(pair, 2, tiny);
     F = pair[0] - pair[1];
   } else {
@@ -176,13 +367,12 @@ MD200_HD bool root_adjoint(const LayerView<double> &m, const double *tab, double
   if (!isfinite(fw.Fk) || !isfinite(fw.Fw) || fw.Fk == 0. || fw.Fw == 0.) return false;
 
   // ---- 2. reverse sweep ----
-  const P4 kP = lift4(k), k2P = lift4(k2), wP = lift4(wd), iw2P = lift4(iw2);
   D2 lam[NV];
   for (int i = 0; i < NV; ++i) lam[i] = D2(0);
+  const P4 kP = lift4(k), k2P = lift4(k2), wP = lift4(wd), iw2P = lift4(iw2);
   if (WAVE == 0 && top) {
-    // F = (cp e0 - wv e1 rho0) 2^-pex, with the fluid row's own parameters
+    // F = (cp e0 - wv e1 rho0) 2^-pex with the fluid row's own parameters
     const double rp = pow2(-pex);
-    // final state (value parts of the forward sweep)
     const RowP4 r0 = row_p4(tab, Ls, 0);
     P4 cp, wv;
     water_top<P4, P4>(kP, wP, r0.h, r0.ivp, &cp, &wv);
@@ -207,54 +397,31 @@ MD200_HD bool root_adjoint(const LayerView<double> &m, const double *tab, double
       const int l = last - 1 - s;
       for (int i = 0; i < NV; ++i) st[s - s0][i] = x[i];
       if (s + 1 == s1) break;
+      const double r = pow2(-ex[s]);
       if constexpr (WAVE == 0) {
-        rayleigh_layer<D2, double>(x, k, k2, wd, iw2, m.h(l), m.ivp(l), m.vs2(l), m.ivs(l), m.rho(l), m.irho(l));
+        rayleigh_step_d2(x, k, k2, wd, iw2, m.h(l), m.ivp(l), m.vs2(l), m.ivs(l), m.rho(l), m.irho(l), r);
       } else {
         const D2 kj = wd * m.ivs(l);
-        D2 r, ir, cq, y, z;
-        radical(k, kj, &r, &ir);
-        love_entries<D2, double>(k, kj, r, ir, m.h(l), &cq, &y, &z);
+        D2 cq, y, z;
+        love_entries<D2, double>(k, kj, m.h(l), &cq, &y, &z);
         const double mu = m.rho(l) * m.vs2(l);
         const D2 u = x[0] * cq + x[1] * z * mu;
         const D2 v = x[0] * y * m.imu(l) + x[1] * cq;
-        x[0] = u;
-        x[1] = v;
+        x[0] = u * r;
+        x[1] = v * r;
       }
-      const double r = pow2(-ex[s]);
-      for (int i = 0; i < NV; ++i) x[i] = x[i] * r;
     }
     // reverse through the segment, top layer first
     for (int s = s1 - 1; s >= s0; --s) {
       const int l = last - 1 - s;
       const double r = pow2(-ex[s]);
-      const RowP4 row = row_p4(tab, Ls, l);
+      const double vs = tab[8 * Ls + l];
       RowGrad g;
-      if constexpr (WAVE == 0) {
-        RayleighEntries<P4> X;
-        rayleigh_entries<P4, P4>(X, kP, k2P, wP, iw2P, row.h, row.ivp, row.vs2, row.ivs, row.rho, row.irho);
-        P4 y[5];
-        for (int i = 0; i < 5; ++i) y[i] = lift4(st[s - s0][i]);
-        rayleigh_apply<P4>(X, k2P, y);
-        for (int p = 0; p < 4; ++p) {
-          D2 acc = lam[0] * y[0].d[p];
-          for (int i = 1; i < 5; ++i) acc = acc + lam[i] * y[i].d[p];
-          g.g[p] = acc * r;
-        }
-        rayleigh_apply_transpose(X, k2, lam);
-        for (int i = 0; i < 5; ++i) lam[i] = lam[i] * r;
-      } else {
-        const P4 kj = wP * row.ivs;
-        P4 rr, ir, cq, y, z;
-        radical(kP, kj, &rr, &ir);
-        love_entries<P4, P4>(kP, kj, rr, ir, row.h, &cq, &y, &z);
-        const P4 e0 = lift4(st[s - s0][0]), e1 = lift4(st[s - s0][1]);
-        const P4 u = e0 * cq + e1 * z * row.mu;
-        const P4 v = e0 * y * row.imu + e1 * cq;
-        for (int p = 0; p < 4; ++p) g.g[p] = (lam[0] * u.d[p] + lam[1] * v.d[p]) * r;
-        const D2 l0 = lam[0], l1 = lam[1];
-        lam[0] = (l0 * cq.v + l1 * (y.v * row.imu.v)) * r;
-        lam[1] = (l0 * (z.v * row.mu.v) + l1 * cq.v) * r;
-      }
+      if constexpr (WAVE == 0)
+        g = rayleigh_layer_adjoint(k, k2, wd, iw2, m.h(l), m.ivp(l), m.ivs(l), m.vs2(l), vs, m.rho(l), m.irho(l),
+                                   st[s - s0], lam, r);
+      else
+        g = love_layer_adjoint(k, wd, m.h(l), m.ivs(l), vs, m.rho(l), m.vs2(l), m.imu(l), st[s - s0], lam, r);
       sink(l, g);
     }
   }
@@ -367,7 +534,6 @@ __global__ void __launch_bounds__(128) root_jacobians(Dev d, const double *vel, 
     }
   }
 }
-
 #endif  // MD200_HOST_SECULAR
 
 }  // namespace md200

@@ -373,6 +373,79 @@ struct RayleighEntries {
   N A, B, C, D, E, F, G, H, I, J, K, Lm, M, Nn, O;
 };
 
+// One wave (P or S) of a layer at wavenumber k against the layer's wavenumber kv:
+// cs = cos(r h), sr = sin(r h) / r, rs = -r sin(r h) for a propagating wave
+// (k < kv); for an evanescent one the hyperbolic forms scaled by
+// scale = exp(-r h): cs = (1 + e^2) / 2, sr = (1 - e^2) / (2 r), rs = r (1 - e^2) / 2,
+// and the return value is r h (value part), the exponent factored out; at
+// k = kv the limits 1, h, 0.  r = sqrt((k + kv)|k - kv|).  scale is 1 unless
+// evanescent.
+template <class N, class T>
+MD200_FN typename Base<N>::type wave_block(const N &k, const N &kv, T h, N *cs, N *sr, N *rs, N *scale) {
+  using BT = typename Base<N>::type;
+  N r, ir;
+  radical(k, kv, &r, &ir);
+  *scale = lift_one<N>();
+  if (val(k) < val(kv)) {
+    N sn;
+    m_sincos(r * h, &sn, cs);
+    *sr = sn * ir;
+    *rs = -(r * sn);
+    return BT(0);
+  }
+  if (val(k) == val(kv)) {
+    *cs = lift_one<N>();
+    *sr = lift_one<N>() * h;
+    *rs = lift_zero<N>();
+    return BT(0);
+  }
+  const N e = m_exp(-(r * h));
+  const N fac = e * e;
+  *cs = (fac + BT(1)) * BT(0.5);
+  const N sh = (BT(1) - fac) * BT(0.5);
+  *sr = sh * ir;
+  *rs = r * sh;
+  *scale = e;
+  return val(r) * val(h);
+}
+
+// The 15 entries from the wave blocks (cosp, wv = sin_p/r_p, xv = -r_p sin_p;
+// cosq, yv, zv likewise for S; a0 the product of the evanescent scales),
+// gam = 2 k^2 vs^2 / w^2, gammk = gam / k^2, and the density.
+template <class N, class T>
+MD200_FN void rayleigh_poly(RayleighEntries<N> &X, const N &cosp, const N &wv, const N &xv, const N &cosq,
+                            const N &yv, const N &zv, const N &a0, const N &gam, const N &gammk, const N &k2,
+                            T rho, T irho) {
+  using BT = typename Base<N>::type;
+  const N cpcq = cosp * cosq, cpy = cosp * yv, cpz = cosp * zv;
+  const N cqw = cosq * wv, cqx = cosq * xv;
+  const N xy = xv * yv, xz = xv * zv, wy = wv * yv, wz = wv * zv;
+
+  const N gm1 = gam - BT(1);
+  const N twgm1 = gam + gm1;
+  const N gmgmk = gam * gammk;
+  const N gmgm1 = gam * gm1;
+  const N gm1sq = gm1 * gm1;
+  const N a0pq = a0 - cpcq;
+  const T rho2 = rho * rho, irho2 = irho * irho;
+
+  X.A = cpcq - (gmgm1 * a0pq) * BT(2) - gmgmk * xz - k2 * gm1sq * wy;
+  X.D = (k2 * cpy - cqx) * irho;
+  X.I = -(twgm1 * a0pq + gammk * xz + k2 * gm1 * wy) * irho;
+  X.C = (cpz - k2 * cqw) * irho;
+  X.Lm = -((k2 * a0pq) * BT(2) + xz + k2 * k2 * wy) * irho2;
+  X.E = (gmgmk * cpz - gm1sq * cqw) * rho;
+  X.G = gammk * cpz - gm1 * cqw;
+  X.M = -wz;
+  X.Nn = -xy;
+  X.F = (gm1sq * cpy - gmgmk * cqx) * rho;
+  X.H = gm1 * cpy - gammk * cqx;
+  X.O = -((gmgmk * gm1sq * a0pq) * BT(2) + gmgmk * gmgmk * xz + gm1sq * gm1sq * wy) * rho2;
+  X.J = -(gammk * gm1 * twgm1 * a0pq + gam * gammk * gammk * xz + gm1 * gm1sq * wy) * rho;
+  X.K = a0 + (cpcq - X.A) * BT(2);
+  X.B = cpcq;
+}
+
 // Entries of layer (h, 1/vp, vs^2, 1/vs, rho, 1/rho) at wavenumber k (k2 = k^2),
 // frequency w (iw2 = 1/w^2).  Returns the exponent P + Q (value part) that the
 // scaled hyperbolic functions of the evanescent branches factor out: the
@@ -383,81 +456,12 @@ MD200_FN typename Base<N>::type rayleigh_entries(RayleighEntries<N> &X, const N 
                                                  const N &w, const N &iw2, T h, T ivp, T vs2, T ivs,
                                                  T rho, T irho) {
   using BT = typename Base<N>::type;
-  BT expo = BT(0);
   const N ka = w * ivp, kb = w * ivs;
-  const N gammk = (iw2 * vs2) * T(2);
+  const N gammk = (iw2 * vs2) * BT(2);
   const N gam = gammk * k2;
-  N ra, ira, rb, irb;
-  radical(k, ka, &ra, &ira);
-  radical(k, kb, &rb, &irb);
-
-  N cosp, wv, xv, cosq, yv, zv;
-  N a0 = lift_one<N>();
-  if (val(k) < val(ka)) {
-    N sp;
-    m_sincos(ra * h, &sp, &cosp);
-    wv = sp * ira;
-    xv = -(ra * sp);
-  } else if (val(k) == val(ka)) {
-    cosp = lift_one<N>();
-    wv = lift_one<N>() * h;
-    xv = lift_zero<N>();
-  } else {
-    const N ep = m_exp(-(ra * h));
-    expo += val(ra) * val(h);
-    const N fac = ep * ep;
-    cosp = (fac + T(1)) * T(0.5);
-    const N sp = (T(1) - fac) * T(0.5);
-    wv = sp * ira;
-    xv = ra * sp;
-    a0 = ep;
-  }
-  if (val(k) < val(kb)) {
-    N sq;
-    m_sincos(rb * h, &sq, &cosq);
-    yv = sq * irb;
-    zv = -(rb * sq);
-  } else if (val(k) == val(kb)) {
-    cosq = lift_one<N>();
-    yv = lift_one<N>() * h;
-    zv = lift_zero<N>();
-  } else {
-    const N eq = m_exp(-(rb * h));
-    expo += val(rb) * val(h);
-    const N fac = eq * eq;
-    cosq = (fac + T(1)) * T(0.5);
-    const N sq = (T(1) - fac) * T(0.5);
-    yv = sq * irb;
-    zv = rb * sq;
-    a0 = a0 * eq;
-  }
-  const N cpcq = cosp * cosq, cpy = cosp * yv, cpz = cosp * zv;
-  const N cqw = cosq * wv, cqx = cosq * xv;
-  const N xy = xv * yv, xz = xv * zv, wy = wv * yv, wz = wv * zv;
-
-  const N gm1 = gam - T(1);
-  const N twgm1 = gam + gm1;
-  const N gmgmk = gam * gammk;
-  const N gmgm1 = gam * gm1;
-  const N gm1sq = gm1 * gm1;
-  const N a0pq = a0 - cpcq;
-  const T rho2 = rho * rho, irho2 = irho * irho;
-
-  X.A = cpcq - (gmgm1 * a0pq) * T(2) - gmgmk * xz - k2 * gm1sq * wy;
-  X.D = (k2 * cpy - cqx) * irho;
-  X.I = -(twgm1 * a0pq + gammk * xz + k2 * gm1 * wy) * irho;
-  X.C = (cpz - k2 * cqw) * irho;
-  X.Lm = -((k2 * a0pq) * T(2) + xz + k2 * k2 * wy) * irho2;
-  X.E = (gmgmk * cpz - gm1sq * cqw) * rho;
-  X.G = gammk * cpz - gm1 * cqw;
-  X.M = -wz;
-  X.Nn = -xy;
-  X.F = (gm1sq * cpy - gmgmk * cqx) * rho;
-  X.H = gm1 * cpy - gammk * cqx;
-  X.O = -((gmgmk * gm1sq * a0pq) * T(2) + gmgmk * gmgmk * xz + gm1sq * gm1sq * wy) * rho2;
-  X.J = -(gammk * gm1 * twgm1 * a0pq + gam * gammk * gammk * xz + gm1 * gm1sq * wy) * rho;
-  X.K = a0 + (cpcq - X.A) * T(2);
-  X.B = cpcq;
+  N cosp, wv, xv, ep, cosq, yv, zv, eq;
+  const BT expo = wave_block<N, T>(k, ka, h, &cosp, &wv, &xv, &ep) + wave_block<N, T>(k, kb, h, &cosq, &yv, &zv, &eq);
+  rayleigh_poly<N, T>(X, cosp, wv, xv, cosq, yv, zv, ep * eq, gam, gammk, k2, rho, irho);
   return expo;
 }
 
@@ -735,34 +739,13 @@ MD200_FN N rayleigh_secular(const LayerView<T> &m, const N &k, const N &w, N *sh
   return F;
 }
 
-// Entries of one SH layer step, [[cq, z mu], [y / mu, cq]], from the radical
-// r = sqrt((k + kj)|k - kj|) (ir its reciprocal) of wavenumber k against the
-// layer's shear wavenumber kj; returns the exponent the scaled hyperbolic
-// functions factor out (value part).
+// Entries of one SH layer step, [[cq, z mu], [y / mu, cq]]: the S-wave block of
+// wavenumber k against the layer's shear wavenumber kj; returns the exponent the
+// scaled hyperbolic functions factor out (value part).
 template <class N, class T>
-MD200_FN typename Base<N>::type love_entries(const N &k, const N &kj, const N &r, const N &ir, T h, N *cq,
-                                             N *y, N *z) {
-  using B = typename Base<N>::type;
-  if (val(k) < val(kj)) {
-    N sn;
-    m_sincos(r * h, &sn, cq);
-    *y = sn * ir;
-    *z = -(r * sn);
-    return B(0);
-  }
-  if (val(k) == val(kj)) {
-    *cq = lift_one<N>();
-    *y = lift_one<N>() * h;
-    *z = lift_zero<N>();
-    return B(0);
-  }
-  const N eq = m_exp(-(r * h));
-  const N f = eq * eq;
-  *cq = (f + B(1)) * B(0.5);
-  const N half = (B(1) - f) * B(0.5);
-  *y = half * ir;
-  *z = half * r;
-  return val(r) * val(h);
+MD200_FN typename Base<N>::type love_entries(const N &k, const N &kj, T h, N *cq, N *y, N *z) {
+  N scale;
+  return wave_block<N, T>(k, kj, h, cq, y, z, &scale);
 }
 
 // Love secular values (SH propagator) and shape features of S samples.
@@ -790,11 +773,11 @@ MD200_FN void love_multi(const LayerView<T> &m, const N *k, const N &w, N *F, N 
 #pragma unroll
     for (int s = 0; s < S; ++s) {
       const N kj = w * ivs;
-      N r, ir;
-      radical(k[s], kj, &r, &ir);
       N cq, y, z;
       if constexpr (sizeof(N) == sizeof(float)) {
         // branch-free single precision: both forms, selected
+        N r, ir;
+        radical(k[s], kj, &r, &ir);
         const float q = r * h;
         float sn, cs;
         m_sincos(q, &sn, &cs);
@@ -806,7 +789,7 @@ MD200_FN void love_multi(const LayerView<T> &m, const N *k, const N &w, N *F, N 
         z = prop ? -(r * half) : r * half;
         ev[s] += prop ? 0.f : q;
       } else {
-        ev[s] += love_entries<N, T>(k[s], kj, r, ir, h, &cq, &y, &z);
+        ev[s] += love_entries<N, T>(k[s], kj, h, &cq, &y, &z);
       }
       const N u = e[s][0] * cq + e[s][1] * z * mu;
       const N v = e[s][0] * y * imu + e[s][1] * cq;
