@@ -524,10 +524,12 @@ __device__ __forceinline__ void put_bracket(double *slot, int r, double lo, doub
 // is kept when a V with its vertex on zero fits the samples -- the linear
 // extension of either flank reaches zero before the far neighbour -- or when a
 // parabola through the three samples dips to zero.
+// `noise_l` and `noise_r` are the rounding noise of the left (u, v) and right
+// (v, z) sample pairs.
 __device__ __forceinline__ bool trough_may_hide_roots(double x0, double x1, double x2, float u, float v, float z,
-                                                      float noise = 1e-7f) {
-  // both flanks must rise by more than the evaluation's rounding noise
-  if (!(v + noise < u && v + noise < z) || !(x0 < x1 && x1 < x2)) return false;
+                                                      float noise_l = 1e-7f, float noise_r = 1e-7f) {
+  // both flanks must rise by more than the evaluations' rounding noise
+  if (!(v + noise_l < u && v + noise_r < z) || !(x0 < x1 && x1 < x2)) return false;
   // single precision suffices for the slope test: spacings are differences of
   // exact positions, well above float resolution
   const float h0 = static_cast<float>(x1 - x0), h1 = static_cast<float>(x2 - x1);
@@ -655,7 +657,7 @@ __device__ __noinline__ bool screen_trough32(const LayerView<float> &m, float w,
     const double xlo = arg ? __shfl_sync(FULL, x, il) : a, xhi = arg < 31 ? __shfl_sync(FULL, x, ir) : b;
     const double xm = __shfl_sync(FULL, x, arg);
     const bool go = mode ? magnitude_dip(xlo, xm, xhi, ml, __shfl_sync(FULL, static_cast<double>(lm), arg), mr) > MDIP
-                         : trough_may_hide_roots(xlo, xm, xhi, vl, __shfl_sync(FULL, v, arg), vr, 1e-5f);
+                         : trough_may_hide_roots(xlo, xm, xhi, vl, __shfl_sync(FULL, v, arg), vr, 1e-5f, 1e-5f);
     if (!go) return true;
     a = xlo; b = xhi; sa = vl; sb = vr; ma = ml; mb = mr;
   }
@@ -679,7 +681,7 @@ __device__ __noinline__ bool screen_trough32(const LayerView<float> &m, float w,
 struct Sample {
   double c;
   float g, M;
-  int seg;  // running sign-change count, with the sign of F in bit 30
+  int seg;  // running sign-change count; bit 29: value evaluated in FP64; bit 30: sign of F
 };
 
 __device__ __forceinline__ Sample shfl_sample(const Sample &s, int src) {
@@ -691,7 +693,52 @@ __device__ __forceinline__ Sample shfl_sample(const Sample &s, int src) {
   return r;
 }
 __device__ __forceinline__ double sample_sign(const Sample &s) { return (s.seg >> 30) & 1 ? -1. : 1.; }
-__device__ __forceinline__ int sample_segment(const Sample &s) { return s.seg & 0x3fffffff; }
+__device__ __forceinline__ int sample_segment(const Sample &s) { return s.seg & 0x1fffffff; }
+__device__ __forceinline__ bool sample_exact(const Sample &s) { return (s.seg >> 29) & 1; }
+// Rounding noise of the shape-feature difference of two samples: single
+// precision unless both were evaluated in FP64 (the sign-uncertain samples of the
+// FP32 scan are, so troughs whose floor lies in that band keep the FP64 test).
+__device__ __forceinline__ float pair_noise(bool single, const Sample &a, const Sample &b) {
+  return single && !(sample_exact(a) && sample_exact(b)) ? 1e-5f : 1e-7f;
+}
+
+// The last cell of a window: its right end is the window end, which no V test
+// sees as a middle sample.  When the shape feature falls into the end steeply
+// enough that its linear extension would reach zero within one more cell (the
+// left-flank test of trough_may_hide_roots, mirrored), a pair may hide in the
+// cell: it is screened and zoomed like an interior trough.  R2, R1: the last two
+// regular samples, in one sign segment.  Out of line: it runs once per trace,
+// after the scan loop, and keeps its registers out of the loop's allocation.
+template <class T, int WAVE>
+__device__ __noinline__ int last_cell(const LayerView<T> view, const LayerView<double> view64, double w, Sample R2,
+                                      Sample R1, double tol, double *slot, int nbr, int K, int lane, int nsteps,
+                                      unsigned long long &evals, unsigned long long &evals32,
+                                      unsigned long long &steps, unsigned long long &steps32,
+                                      unsigned long long &zooms) {
+  constexpr bool single = sizeof(T) == 4;
+  const double sgn = sample_sign(R1);
+  const float u = static_cast<float>(sgn) * R2.g, v = static_cast<float>(sgn) * R1.g;
+  const float h0 = static_cast<float>(R1.c - R2.c);
+  const float noise = pair_noise(single, R2, R1);
+  if (!(u > v + noise && v / ((u - v) / h0) < 1.25f * h0)) return nbr;
+  bool dismissed = false;
+  if constexpr (single) {
+    unsigned long long se = 0;
+    dismissed = screen_trough32<WAVE>(view, static_cast<float>(w), R2.c, R1.c, u, v, R2.M, R1.M, sgn, 0, lane, se);
+    evals += se;
+    evals32 += se;
+    steps += se * nsteps;
+    steps32 += se * nsteps;
+  }
+  if (!dismissed) {
+    unsigned long long ze = 0;
+    nbr = zoom_trough<WAVE>(view64, w, R2.c, R1.c, u, v, R2.M, R1.M, sgn, 0, tol, slot, nbr, K, lane, ze);
+    evals += ze;
+    steps += ze * nsteps;
+    ++zooms;
+  }
+  return nbr;
+}
 
 #ifndef MD200_SCAN_MIN_BLOCKS
 #define MD200_SCAN_MIN_BLOCKS 4
@@ -790,7 +837,10 @@ __global__ void __launch_bounds__(128, MD200_SCAN_MIN_BLOCKS) scan(Dev d, const 
         si += __popc(__ballot_sync(FULL, ps < 32 && sv < INFINITY));
         vm[h] = __ballot_sync(FULL, cs[h] < INFINITY);
       }
-      if (!vm[0]) break;
+      if (!vm[0]) {
+        finished = true;  // the window is exhausted
+        break;
+      }
 
       // ---- secular values, shape features and log-magnitudes ----
       double Fs[S], gs[S], Ms[S];
@@ -886,7 +936,8 @@ __global__ void __launch_bounds__(128, MD200_SCAN_MIN_BLOCKS) scan(Dev d, const 
         const bool sc = valid && vl && (signbit(Fl) != signbit(F));  // +0 counts as positive
         const unsigned scm = __ballot_sync(FULL, sc);
         const int myseg = nseg + __popc(scm & le);
-        Sample me{c, static_cast<float>(g), static_cast<float>(M), myseg | (signbit(F) ? (1 << 30) : 0)};
+        Sample me{c, static_cast<float>(g), static_cast<float>(M),
+                  myseg | (exact ? (1 << 29) : 0) | (signbit(F) ? (1 << 30) : 0)};
         // ---- regular samples and their two regular predecessors ----
         const bool reg = valid && !(vl && c - cl < 1e-6 * c);
         const unsigned rmask = __ballot_sync(FULL, reg);
@@ -907,7 +958,7 @@ __global__ void __launch_bounds__(128, MD200_SCAN_MIN_BLOCKS) scan(Dev d, const 
         if (reg && hp1 && hp2 && sample_segment(P2) == myseg && sample_segment(P1) == myseg) {
           const double sgn = sample_sign(P1);
           tr = trough_may_hide_roots(P2.c, P1.c, c, sgn * P2.g, sgn * P1.g, sgn * static_cast<float>(g),
-                                     single ? 1e-5f : 1e-7f);
+                                     pair_noise(single, P2, P1), pair_noise(single, P1, me));
           if (!tr) trm_ = magnitude_dip(P2.c, P1.c, c, P2.M, P1.M, static_cast<float>(M)) > MDIP;
           tr = tr || trm_;
         }
@@ -975,6 +1026,10 @@ __global__ void __launch_bounds__(128, MD200_SCAN_MIN_BLOCKS) scan(Dev d, const 
         }
       }
     }
+    if (finished && nbr < K && !(tfl & TRACE_SEARCH_UNCONVERGED) && hr1 && hr2 && R2.c < R1.c &&
+        zoom_right <= R2.c && sample_segment(R1) == sample_segment(R2))
+      nbr = last_cell<T, WAVE>(view, view64, w, R2, R1, d.tol, slot, nbr, K, lane, nsteps, evals, evals32, steps,
+                               steps32, zooms);
     // ---- publish brackets ----
     if (lane == 0) {
       d.nbr[t] = nbr;

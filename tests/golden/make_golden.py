@@ -12,7 +12,9 @@ Outputs (all small .npz files, committed):
   refinement, Love phase strategy, c_tol_rel 1e-12, group velocity at the
   default group_rtol 1e-3).  Cases: the quickstart model (Rayleigh, Love),
   48-model subsets of the crustal batch (Rayleigh, Love), 48 low-velocity-layer
-  models (Rayleigh, Love), six surface-water models (Rayleigh).
+  models (Rayleigh, Love), six surface-water models (Rayleigh), one crustal model
+  with a close pair whose shape-feature trough lies in the FP32 scan's FP64 band, and
+  one low-velocity-layer model with a pair in the last cell before the cutoff.
 * ``jac_<case>.npz``: phase-velocity Jacobians by central differences (step 1e-6
   relative) of the reference CPU solver's roots (c_tol_rel 1e-13): four
   config-4 models (Rayleigh), two (Love), two surface-water models (Rayleigh).
@@ -120,6 +122,14 @@ def main():
     save_reference_case("lvz48_rayleigh", subset(lvz, np.arange(48)), periods, nmodes, 0)
     save_reference_case("lvz48_love", subset(lvz, np.arange(48)), periods, nmodes, 1)
     save_reference_case("water6_rayleigh", water_models(), np.geomspace(0.2, 20., 24), 4, 0)
+    # a close pair (2.6293 / 2.6359 km/s at T = 9.7 s) whose trough floor lies in the
+    # band the FP32 scan re-evaluates in FP64
+    pair = workloads.crustal_batch(2000, workloads.SEED + 2)
+    save_reference_case("pair1678_rayleigh", subset(pair, np.arange(1678, 1679)), periods, nmodes, 0)
+    # a low-velocity-layer model with a pair (4.1023 / 4.1185 km/s at T = 13.3 s) in the
+    # last grid cell before the half-space cutoff
+    lvz5k = workloads.crustal_batch(5000, workloads.SEED + 3, lvz_fraction=0.3)
+    save_reference_case("pair3501_rayleigh", subset(lvz5k, np.arange(3501, 3502)), periods, nmodes, 0)
     c4, periods4, nmodes4 = workloads.config4(16)
     save_jacobian_case("config4_rayleigh", subset(c4, np.arange(4)), periods4, nmodes4, 0)
     save_jacobian_case("config4_love", subset(c4, np.arange(4, 6)), periods4, nmodes4, 1)

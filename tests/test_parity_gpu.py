@@ -158,6 +158,26 @@ def test_live_reference_on_fresh_lvz_batch(wave):
         assert_root_parity(ref, engine_solve64(case, sp), f"live wave={wave} fp32={sp}")
 
 
+@pytest.mark.parametrize("wave", [0, 1])
+def test_live_reference_on_crustal_sample(wave):
+    """384 models of the benchmark's crustal batch and 128 low-velocity-layer models,
+    60 periods, against the reference engine run live on the host's cores."""
+    import os
+    import oracle
+    from modisp_b200 import workloads
+    if oracle.reference() is None:
+        pytest.skip("reference CPU engine not built")
+    periods = np.geomspace(0.5, 50., 60)
+    threads = len(os.sched_getaffinity(0))
+    for name, batch in (("crustal", workloads.crustal_batch(384, workloads.SEED + 2)),
+                        ("lvz", workloads.crustal_batch(128, workloads.SEED + 3, lvz_fraction=0.3))):
+        ref = oracle.reference_solve(batch["thickness"], batch["vp"], batch["vs"], batch["rho"], periods, 5,
+                                     wave=wave, tol=1e-10, threads=threads)
+        case = dict(batch, periods=periods, nmodes=5, wave=wave, search_bounds=ref["search_bounds"])
+        for sp in (False, True):
+            assert_root_parity(ref, engine_solve64(case, sp), f"{name} wave={wave} fp32={sp}")
+
+
 def test_automatic_window_matches_reference_bounds():
     """The engine's on-device window (no bounds passed) equals the reference's."""
     from modisp_b200 import _native
