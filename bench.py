@@ -47,6 +47,10 @@ WORKLOAD = "crustal batch: 10000 models x 8-20 layers, 60 periods 0.5-50 s, 5 mo
 # each 1, an FMA 2; the elementary functions counted separately: 2 rsqrt and
 # 2 sin/cos-or-exp per Rayleigh step, 1 rsqrt and 1 sin/cos-or-exp per Love step).
 FLOPS_PER_STEP = {0: 170, 1: 24}
+# DRAM traffic of the FP32 Rayleigh scan, dram__bytes_read.sum + dram__bytes_write.sum
+# from one ncu capture of a 2,000-model launch (120,000 traces: 30.1 MB + 93.0 MB),
+# per trace; scaled to this workload's launch by its trace count.
+SCAN32_DRAM_BYTES_PER_TRACE = (30.053632e6 + 92.991232e6) / 120_000
 
 
 def parse():
@@ -401,7 +405,11 @@ def main():
                      "fp32_scan_speedup": value / value64},
             "e2e": {"value": e2e_value, "unit": "roots/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "fp32-cuda-core", "kernel": "scan<float>", "achieved": achieved / 1e12,
-                         "peak": peak32 / 1e12, "unit": "TFLOP/s", "frac": achieved / peak32, "traffic": None,
+                         "peak": peak32 / 1e12, "unit": "TFLOP/s", "frac": achieved / peak32,
+                         "traffic": SCAN32_DRAM_BYTES_PER_TRACE * B * T,
+                         "traffic_note": "bytes per Rayleigh FP32 scan launch, from an ncu capture of 2,000 models "
+                                         "scaled by traces; the algorithmic input is the model tables (~1.5 KB per "
+                                         "model): the kernel is compute-bound, DRAM at 0.2 % of peak",
                          "peak_kind": "measured FMA throughput (md200_measure_peak), not MEASURED_PEAKS.json",
                          "fp64_peak": peak64 / 1e12, "scan_ms_per_step": scan_ms,
                          "stage_ms": {("rayleigh" if w == 0 else "love"): stage[w] for w in (0, 1)}},
