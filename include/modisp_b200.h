@@ -111,6 +111,39 @@ int md200_run_device(md200_engine *engine, const double *thickness, const double
                      unsigned *group_flags, unsigned *prediction_flags, double *bounds_out,
                      unsigned long long *stats, void *stream);
 
+/* Ragged batch (no counterpart in the reference, whose periods are one array
+ * shared by every model, python/modisp/__init__.py:285-286; its per-row form
+ * allows one period per model only, cpp/cuda/qe.cu:1069-1070): every model has
+ * its own period list and its own mode count, and all of them share one set of
+ * launches.  Host arrays, waits for the result.
+ *   period_offsets [models + 1] : model b's periods are periods[period_offsets[b] ..
+ *                                 period_offsets[b+1]) (CSR; offsets[0] = 0,
+ *                                 non-decreasing; the total is at most capacity x
+ *                                 the engine's periods)
+ *   modes [models]              : mode count of model b, 1 .. the engine's nmodes
+ * Outputs: per trace (CSR order) flags, levels, counts [traces]; velocity (and
+ * group, group_flags) hold, for model b, a [modes[b]][T_b] block (mode, period),
+ * the blocks concatenated in model order (sum of modes[b] T_b values).
+ * Trace semantics are those of md200_run; windows are computed on the device. */
+int md200_run_ragged(md200_engine *engine, const double *thickness, const double *vp, const double *vs,
+                     const double *rho, int models, const int *period_offsets, const double *periods,
+                     const int *modes, double c_tol_rel, double f_accept, int wave, double *velocity,
+                     unsigned *flags, int *levels, int *counts, double *group, unsigned *group_flags,
+                     unsigned long long *stats, int nstats);
+
+/* Device-pointer form of md200_run_ragged, enqueued on `stream` (NULL = the
+ * engine's stream) without a host synchronisation.  `traces` is
+ * period_offsets[models]; out_offsets [models] gives the index of model b's
+ * output block (the running sum of modes[b'] T_b' over b' < b).  The CSR
+ * description is not checked on the device: offsets must be non-decreasing and
+ * the output arrays large enough; mode counts are clamped to 1 .. nmodes. */
+int md200_run_ragged_device(md200_engine *engine, const double *thickness, const double *vp,
+                            const double *vs, const double *rho, int models, int traces,
+                            const int *period_offsets, const double *periods, const int *modes,
+                            const long long *out_offsets, double c_tol_rel, double f_accept, int wave,
+                            double *velocity, unsigned *flags, int *levels, int *counts, double *group,
+                            unsigned *group_flags, unsigned long long *stats, void *stream);
+
 /* Phase- and group-velocity Jacobians of solved roots (no counterpart in the
  * reference, which returns no derivatives; they serve the gradient of a misfit
  * between predicted and observed dispersion).  For every finite root

@@ -71,6 +71,9 @@ EXPORTS = {
     "md200_stage_times": (_I, [_P, ctypes.POINTER(ctypes.c_double), _I]),
     "md200_kernel_launches": (_I, [_P]),
     "md200_measure_peak": (_I, [_I, _I, ctypes.POINTER(ctypes.c_double)]),
+    "md200_run_ragged": (_I, [_P, _P, _P, _P, _P, _I, _P, _P, _P, _D, _D, _I, _P, _P, _P, _P, _P, _P, _P, _I]),
+    "md200_run_ragged_device": (_I, [_P, _P, _P, _P, _P, _I, _I, _P, _P, _P, _P, _D, _D, _I, _P, _P, _P, _P, _P,
+                                     _P, _P, _P]),
     "md200_jacobian_device": (_I, [_P, _P, _P, _P, _P, _I, _P, _I, _P, _P, _P, _P, _P]),
     "md200_jacobian": (_I, [_P, _P, _P, _P, _P, _I, _P, _I, _P, _P, _P, _P, ctypes.POINTER(_I)]),
     "md200_vjp_device": (_I, [_P, _P, _P, _P, _P, _I, _P, _I, _P, _P, _P, _P, _P, _P]),
@@ -190,6 +193,42 @@ class Engine:
             c(prediction) if prediction else None, c(bounds_out) if bounds_out else None,
             c(stats) if stats else None, _stream_arg(stream))
         check(status)
+
+    def run_ragged(self, h, vp, vs, rho, period_offsets, periods, modes, tol, accept, wave, group=False):
+        """Ragged host-array run: model b has periods[period_offsets[b]:period_offsets[b+1]]
+        and modes[b] modes.  Returns flat outputs: velocity (and group) as the
+        concatenated [modes[b], T_b] blocks, trace arrays in CSR order."""
+        arrays = [np.ascontiguousarray(x, dtype=np.float64) for x in (h, vp, vs, rho)]
+        B = arrays[0].shape[0]
+        off = np.ascontiguousarray(period_offsets, dtype=np.int32)
+        per = np.ascontiguousarray(periods, dtype=np.float64)
+        md = np.ascontiguousarray(modes, dtype=np.int32)
+        if off.size != B + 1 or md.size != B:
+            raise ValueError("period_offsets needs models + 1 entries and modes one per model")
+        traces = int(off[-1])
+        cells = int(np.sum(md.astype(np.int64) * np.diff(off)))
+        out = dict(velocity=np.empty(cells), flags=np.empty(traces, np.uint32), levels=np.empty(traces, np.int32),
+                   counts=np.empty(traces, np.int32), stats=np.zeros(STAT_COUNT, np.uint64))
+        if group:
+            out["group_velocity"] = np.empty(cells)
+            out["group_velocity_flags"] = np.empty(cells, np.uint32)
+        check(lib().md200_run_ragged(self.handle, *(ptr(a) for a in arrays), B, ptr(off), ptr(per), ptr(md),
+                                     float(tol), float(accept), int(wave), ptr(out["velocity"]), ptr(out["flags"]),
+                                     ptr(out["levels"]), ptr(out["counts"]), ptr(out.get("group_velocity")),
+                                     ptr(out.get("group_velocity_flags")), ptr(out["stats"]), STAT_COUNT))
+        out["stats"] = dict(zip(STAT_NAMES, (int(x) for x in out["stats"])))
+        return out
+
+    def run_ragged_device(self, h, vp, vs, rho, models, traces, period_offsets, periods, modes, out_offsets, tol,
+                          accept, wave, velocity, flags, levels, counts, group=None, group_flags=None, stats=None,
+                          stream=None):
+        """Device-pointer ragged run (integer addresses), enqueued on `stream`."""
+        c = ctypes.c_void_p
+        opt = lambda x: c(x) if x else None
+        check(lib().md200_run_ragged_device(self.handle, c(h), c(vp), c(vs), c(rho), int(models), int(traces),
+                                            c(period_offsets), c(periods), c(modes), c(out_offsets), float(tol),
+                                            float(accept), int(wave), c(velocity), c(flags), c(levels), c(counts),
+                                            opt(group), opt(group_flags), opt(stats), _stream_arg(stream)))
 
     def jacobian(self, h, vp, vs, rho, periods, wave, velocity, group=None, want_group=True):
         """Host-array Jacobians of the roots `velocity` [B, nmodes, T]: returns

@@ -65,6 +65,10 @@ struct md200_engine {
   size_t pinned_bytes = 0;
   // host-path Jacobian buffers (allocated on first use)
   double *jac_c = nullptr, *jac_u = nullptr, *jac_w = nullptr, *jac_grad = nullptr;
+  // host-path ragged buffers (allocated on first use)
+  int *rg_offsets = nullptr, *rg_modes = nullptr;
+  long long *rg_outbase = nullptr;
+  double *rg_periods = nullptr;
   int jac_blocks = 0;
   std::vector<void *> owned;
   // per-stage timing (cudaEvent pairs on the run's stream)
@@ -129,6 +133,8 @@ int setup(md200_engine *e) {
       own_alloc(e, &d.knot, static_cast<size_t>(B) * d.nkmax) || own_alloc(e, &d.nknot, B) ||
       own_alloc(e, &d.seed, static_cast<size_t>(B) * d.nsmax) || own_alloc(e, &d.nseed, B) ||
       own_alloc(e, &d.nbr, nt) || own_alloc(e, &d.tflags, nt) ||
+      own_alloc(e, &d.tr_model, nt) || own_alloc(e, &d.tr_stride, nt) || own_alloc(e, &d.tr_modes, nt) ||
+      own_alloc(e, &d.tr_period, nt) || own_alloc(e, &d.tr_out, nt) ||
       own_alloc(e, &d.slot, nt * d.KB * SLOT) ||
       own_alloc(e, &d.trace_list, nt) || own_alloc(e, &d.repair_list, nt) ||
       own_alloc(e, &d.refine_list, 2 * nt * d.KB) ||
@@ -202,10 +208,19 @@ int validate_geometry(md200_engine *e, int models) {
   return 0;
 }
 
+// Ragged batches: traces in CSR order of the models (see Dev); uniform batches
+// pass ntraces = 0 and no descriptor.
+struct Ragged {
+  int ntraces = 0;
+  const int *offsets = nullptr, *modes = nullptr;
+  const long long *outbase = nullptr;
+};
+
 int enqueue(md200_engine *e, const double *h, const double *vp, const double *vs, const double *rho,
             int B, const double *periods, const double *bounds, double tol, double accept, int wave,
             double *vel, unsigned *flags, int *levels, int *counts, double *grp, unsigned *gflags,
-            unsigned *pred, double *bounds_out, unsigned long long *stats, cudaStream_t s) {
+            unsigned *pred, double *bounds_out, unsigned long long *stats, cudaStream_t s,
+            const Ragged &rg = Ragged()) {
   if (!(tol > 0.) || !(tol < 1.)) return fail("modisp_b200: c_tol_rel must lie in (0, 1)");
   if (wave != 0 && wave != 1) return fail("modisp_b200: wave must be 0 (Rayleigh) or 1 (Love)");
   if (e->d.group && (!grp || !gflags))
@@ -213,7 +228,11 @@ int enqueue(md200_engine *e, const double *h, const double *vp, const double *vs
   MD200_CK(cudaSetDevice(e->device));
   Dev d = e->d;
   d.B = B;
-  d.n_traces = B * e->T;
+  d.n_traces = rg.offsets ? rg.ntraces : B * e->T;
+  d.ragged = rg.offsets ? 1 : 0;
+  d.r_offsets = rg.offsets;
+  d.r_modes = rg.modes;
+  d.r_outbase = rg.outbase;
   d.wave = wave;
   d.tol = tol;
   d.accept = accept;
@@ -616,6 +635,97 @@ int md200_vjp(md200_engine *e, const double *h, const double *vp, const double *
   MD200_CK(cudaStreamSynchronize(e->stream));
   MD200_CK(cudaMemcpy(grad, e->jac_grad, sizeof(double) * 4 * static_cast<size_t>(models) * e->L,
                       cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+int md200_run_ragged_device(md200_engine *e, const double *h, const double *vp, const double *vs,
+                            const double *rho, int models, int traces, const int *period_offsets,
+                            const double *periods, const int *modes, const long long *out_offsets, double tol,
+                            double accept, int wave, double *velocity, unsigned *flags, int *levels, int *counts,
+                            double *group, unsigned *group_flags, unsigned long long *stats, void *stream) {
+  if (validate_geometry(e, models)) return 1;
+  if (traces < 1 || static_cast<long long>(traces) > static_cast<long long>(e->cap) * e->T)
+    return fail("modisp_b200: ragged trace count " + std::to_string(traces) + " outside 1.." +
+                std::to_string(static_cast<long long>(e->cap) * e->T) + " (capacity x periods)");
+  if (!h || !vp || !vs || !rho || !period_offsets || !periods || !modes || !out_offsets || !velocity || !flags ||
+      !levels || !counts)
+    return fail("modisp_b200: missing input or output array");
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : e->stream;
+  Ragged rg;
+  rg.ntraces = traces;
+  rg.offsets = period_offsets;
+  rg.modes = modes;
+  rg.outbase = out_offsets;
+  return enqueue(e, h, vp, vs, rho, models, periods, nullptr, tol, accept, wave, velocity, flags, levels, counts,
+                 group, group_flags, nullptr, nullptr, stats, s, rg);
+}
+
+int md200_run_ragged(md200_engine *e, const double *h, const double *vp, const double *vs, const double *rho,
+                     int models, const int *period_offsets, const double *periods, const int *modes, double tol,
+                     double accept, int wave, double *velocity, unsigned *flags, int *levels, int *counts,
+                     double *group, unsigned *group_flags, unsigned long long *stats, int nstats) {
+  if (validate_geometry(e, models)) return 1;
+  if (!h || !vp || !vs || !rho || !period_offsets || !periods || !modes || !velocity || !flags || !levels ||
+      !counts)
+    return fail("modisp_b200: missing input or output array");
+  if (e->d.group && (!group || !group_flags))
+    return fail("modisp_b200: group-velocity engine needs group output arrays");
+  // the CSR description, checked here (the device path trusts it)
+  if (period_offsets[0] != 0) return fail("modisp_b200: period_offsets[0] must be 0");
+  std::vector<long long> outbase(models);
+  long long cells = 0;
+  for (int b = 0; b < models; ++b) {
+    const int nb = period_offsets[b + 1] - period_offsets[b];
+    if (nb < 0) return fail("modisp_b200: period_offsets must be non-decreasing");
+    if (modes[b] < 1 || modes[b] > e->nmodes)
+      return fail("modisp_b200: modes[" + std::to_string(b) + "] = " + std::to_string(modes[b]) +
+                  " outside 1.." + std::to_string(e->nmodes));
+    outbase[b] = cells;
+    cells += static_cast<long long>(modes[b]) * nb;
+  }
+  const int traces = period_offsets[models];
+  if (traces < 1 || static_cast<long long>(traces) > static_cast<long long>(e->cap) * e->T)
+    return fail("modisp_b200: ragged trace count " + std::to_string(traces) + " outside 1.." +
+                std::to_string(static_cast<long long>(e->cap) * e->T) + " (capacity x periods)");
+  for (int t = 0; t < traces; ++t)
+    if (!(periods[t] > 0.)) return fail("modisp_b200: periods must be positive");
+  MD200_CK(cudaSetDevice(e->device));
+  const size_t B = models, L = e->L, capt = static_cast<size_t>(e->cap) * e->T;
+  if (lazy_alloc(e, &e->rg_offsets, static_cast<size_t>(e->cap) + 1) || lazy_alloc(e, &e->rg_modes, e->cap) ||
+      lazy_alloc(e, &e->rg_outbase, e->cap) || lazy_alloc(e, &e->rg_periods, capt))
+    return 1;
+  cudaStream_t s = e->stream;
+  MD200_CK(cudaStreamSynchronize(s));  // the staging buffers below are reused
+  MD200_CK(cudaMemcpy(e->in_h, h, sizeof(double) * B * L, cudaMemcpyHostToDevice));
+  MD200_CK(cudaMemcpy(e->in_vp, vp, sizeof(double) * B * L, cudaMemcpyHostToDevice));
+  MD200_CK(cudaMemcpy(e->in_vs, vs, sizeof(double) * B * L, cudaMemcpyHostToDevice));
+  MD200_CK(cudaMemcpy(e->in_rho, rho, sizeof(double) * B * L, cudaMemcpyHostToDevice));
+  MD200_CK(cudaMemcpy(e->rg_offsets, period_offsets, sizeof(int) * (B + 1), cudaMemcpyHostToDevice));
+  MD200_CK(cudaMemcpy(e->rg_modes, modes, sizeof(int) * B, cudaMemcpyHostToDevice));
+  MD200_CK(cudaMemcpy(e->rg_outbase, outbase.data(), sizeof(long long) * B, cudaMemcpyHostToDevice));
+  MD200_CK(cudaMemcpy(e->rg_periods, periods, sizeof(double) * traces, cudaMemcpyHostToDevice));
+  const bool grp = e->d.group != 0;
+  Ragged rg;
+  rg.ntraces = traces;
+  rg.offsets = e->rg_offsets;
+  rg.modes = e->rg_modes;
+  rg.outbase = e->rg_outbase;
+  if (enqueue(e, e->in_h, e->in_vp, e->in_vs, e->in_rho, models, e->rg_periods, nullptr, tol, accept, wave,
+              e->out_vel, e->out_flags, e->out_levels, e->out_counts, grp ? e->out_grp : nullptr,
+              grp ? e->out_gflags : nullptr, nullptr, nullptr, e->d_stats, s, rg))
+    return 1;
+  MD200_CK(cudaStreamSynchronize(s));
+  MD200_CK(cudaMemcpy(velocity, e->out_vel, sizeof(double) * cells, cudaMemcpyDeviceToHost));
+  MD200_CK(cudaMemcpy(flags, e->out_flags, sizeof(unsigned) * traces, cudaMemcpyDeviceToHost));
+  MD200_CK(cudaMemcpy(levels, e->out_levels, sizeof(int) * traces, cudaMemcpyDeviceToHost));
+  MD200_CK(cudaMemcpy(counts, e->out_counts, sizeof(int) * traces, cudaMemcpyDeviceToHost));
+  if (grp) {
+    MD200_CK(cudaMemcpy(group, e->out_grp, sizeof(double) * cells, cudaMemcpyDeviceToHost));
+    MD200_CK(cudaMemcpy(group_flags, e->out_gflags, sizeof(unsigned) * cells, cudaMemcpyDeviceToHost));
+  }
+  if (stats && nstats > 0)
+    MD200_CK(cudaMemcpy(stats, e->d_stats, sizeof(unsigned long long) * std::min(nstats, int(MD200_STAT_COUNT)),
+                        cudaMemcpyDeviceToHost));
   return 0;
 }
 

@@ -63,6 +63,17 @@ struct Dev {
   int *nknot;
   double *seed;     // [B][nsmax]
   int *nseed;
+  // trace geometry (filled by init_traces): model, period, output
+  // index of mode 0, stride between modes, mode count.  Uniform batches: trace
+  // t = b T + f, outputs [B][nmodes][T].  Ragged batches: traces in CSR order
+  // (model b owns traces r_offsets[b] .. r_offsets[b+1]), outputs of model b a
+  // [r_modes[b]][T_b] block at r_outbase[b].
+  int ragged;
+  const int *r_offsets, *r_modes;
+  const long long *r_outbase;
+  int *tr_model, *tr_stride, *tr_modes;
+  double *tr_period;
+  long long *tr_out;
   // traces
   int *nbr;
   unsigned *tflags;

@@ -428,8 +428,34 @@ __global__ void prep_models(Dev d, int sortcap, int automatic) {
 __global__ void init_traces(Dev d) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= d.n_traces) return;
-  const int b = q % d.B, f = q / d.B;
-  const int t = b * d.T + f;
+  int b, t;
+  if (d.ragged) {
+    // CSR order; the owning model by binary search of the offsets
+    t = q;
+    int lo = 0, hi = d.B;  // r_offsets[lo] <= t < r_offsets[hi]
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (d.r_offsets[mid] <= t) lo = mid;
+      else hi = mid;
+    }
+    b = lo;
+    const int f = t - d.r_offsets[b];
+    d.tr_model[t] = b;
+    d.tr_period[t] = d.periods[t];
+    d.tr_out[t] = d.r_outbase[b] + f;
+    d.tr_stride[t] = d.r_offsets[b + 1] - d.r_offsets[b];
+    const int mb = d.r_modes[b];
+    d.tr_modes[t] = mb < 1 ? 1 : (mb > d.nmodes ? d.nmodes : mb);  // the bracket slots hold nmodes + 2
+  } else {
+    b = q % d.B;
+    const int f = q / d.B;
+    t = b * d.T + f;
+    d.tr_model[t] = b;
+    d.tr_period[t] = d.periods[f];
+    d.tr_out[t] = static_cast<long long>(b) * d.nmodes * d.T + f;
+    d.tr_stride[t] = d.T;
+    d.tr_modes[t] = d.nmodes;
+  }
   d.nbr[t] = 0;
   d.tflags[t] = 0;
   if (d.pred) d.pred[t] = 8u;  // searched independently (PredictionFlag.BYPASSED)
@@ -447,8 +473,8 @@ __global__ void tail_values(Dev d) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= *(volatile int *)&d.ctr[C_NTRACE]) return;
   const int t = d.trace_list[q];
-  const int b = t / d.T, f = t - b * d.T;
-  const double w = TWO_PI / d.periods[f];
+  const int b = d.tr_model[t];
+  const double w = TWO_PI / d.tr_period[t];
   const LayerView<double> m = make_view<double>(d.layer64 + static_cast<size_t>(b) * ROWS * d.Ls, d.Ls,
                                                 d.mL[b], d.mwater[b]);
   for (int i = 0; i < 2; ++i) {
@@ -752,7 +778,6 @@ __global__ void __launch_bounds__(128, MD200_SCAN_MIN_BLOCKS) scan(Dev d, const 
   T *tab = reinterpret_cast<T *>(mine);
   double *mbuf = reinterpret_cast<double *>(mine + tab_bytes);
   unsigned long long evals = 0, evals32 = 0, steps = 0, steps32 = 0, zooms = 0;
-  const int K = d.K;
   const double density = d.density, step = 1. / density;
   constexpr bool single = sizeof(T) == 4;
   const unsigned lt = lanemask_lt(), le = lt | (1u << lane);
@@ -763,8 +788,9 @@ __global__ void __launch_bounds__(128, MD200_SCAN_MIN_BLOCKS) scan(Dev d, const 
     q = __shfl_sync(FULL, q, 0);
     if (q >= *(volatile int *)&d.ctr[count_id]) break;
     const int t = list[q];
-    const int b = t / d.T, f = t - b * d.T;
-    const double period = d.periods[f];
+    const int b = d.tr_model[t];
+    const int K = d.tr_modes[t] + 2;  // nmodes + 2 guard roots
+    const double period = d.tr_period[t];
     const double w = TWO_PI / period, fr = 1. / period;
     const int L = d.mL[b], water = d.mwater[b];
     // stage the model's recurrence rows (16-byte cp.async, coalesced)
@@ -1118,9 +1144,9 @@ __global__ void refine(Dev d) {
        i += gridDim.x * blockDim.x) {
     const int id = d.refine_list[i];
     const int t = id / d.KB;
-    const int b = t / d.T, f = t - b * d.T;
+    const int b = d.tr_model[t];
     const LayerView<double> m = global_view(d, b);
-    const double w = TWO_PI / d.periods[f];
+    const double w = TWO_PI / d.tr_period[t];
     double *sl = d.slot + static_cast<size_t>(id) * SLOT;
     const double lo = sl[0], hi = sl[1];
     double flo = sl[2], fhi = sl[3];
@@ -1175,9 +1201,9 @@ __global__ void collect_repairs(Dev d) {
 __global__ void assemble(Dev d) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= d.n_traces) return;
-  const int b = t / d.T, f = t - b * d.T;
-  const int nm = d.nmodes, T = d.T;
-  const size_t out0 = static_cast<size_t>(b) * nm * T + f;
+  const int b = d.tr_model[t];
+  const int nm = d.tr_modes[t], T = d.tr_stride[t];  // modes of this trace, stride between them
+  const size_t out0 = static_cast<size_t>(d.tr_out[t]);
   const int state = d.mstate[b];
   if (state != 0) {
     for (int m = 0; m < nm; ++m) d.vel[out0 + static_cast<size_t>(m) * T] = NAN;
@@ -1197,7 +1223,7 @@ __global__ void assemble(Dev d) {
   // gather, order and cap at K (the K = nmodes + 2 smallest roots)
   double r[64] = {};
   int n = 0;
-  const int K = d.K;
+  const int K = nm + 2;
   const int cap = K < 64 ? K : 64;
   bool failed = (fl & (TRACE_SEARCH_UNCONVERGED | INTERNAL_REPAIR)) != 0;
   auto push = [&](double x) {
@@ -1223,7 +1249,7 @@ __global__ void assemble(Dev d) {
   const double lo = d.mlo[b], hi = d.mhi[b];
   const LayerView<double> m = global_view(d, b);
   const double vs_hs = layer_table<double>(d, b)[8 * d.Ls + m.L - 1];
-  const double w = TWO_PI / d.periods[f];
+  const double w = TWO_PI / d.tr_period[t];
   int level = d.fp32 ? ((fl & TRACE_FP64_REPAIR) ? LEVEL_REPAIRED : LEVEL_FP32) : LEVEL_FP64;
   int count = n;
   if (failed) {
@@ -1265,7 +1291,7 @@ __global__ void assemble(Dev d) {
         } else {
           d.gflags[cell] = 0;
           const int pos = atomicAdd(&d.ctr[C_NGROUP], 1);
-          d.group_list[pos] = static_cast<int>(cell);
+          d.group_list[pos] = t * d.KB + mo;
         }
       }
     }
@@ -1290,13 +1316,13 @@ __global__ void group_velocity(Dev d) {
   const int n = d.ctr[C_NGROUP];
   unsigned long long steps = 0, count = 0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const int cell = d.group_list[i];
-    const int T = d.T, nm = d.nmodes;
-    const int b = cell / (nm * T);
-    const int f = cell % T;
+    const int id = d.group_list[i];  // trace * KB + mode
+    const int t = id / d.KB, mo = id - t * d.KB;
+    const size_t cell = static_cast<size_t>(d.tr_out[t]) + static_cast<size_t>(mo) * d.tr_stride[t];
+    const int b = d.tr_model[t];
     const LayerView<double> m = global_view(d, b);
     const double c = d.vel[cell];
-    const double w = TWO_PI / d.periods[f];
+    const double w = TWO_PI / d.tr_period[t];
     using D2 = Dual<double, 2>;
     D2 k, wd;
     k.v = w / c; k.d[0] = 1.; k.d[1] = 0.;

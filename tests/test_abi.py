@@ -104,3 +104,26 @@ def test_workloads_have_the_stated_shapes():
     assert 0.15 < drops.mean() < 0.45
     b4, p4, k4 = workloads.config4(16)
     assert b4["thickness"].shape == (16, 13) and p4.size == 40 and k4 == 3
+
+
+def test_ragged_layout_and_validation():
+    """CSR bookkeeping of the ragged API (no GPU needed)."""
+    from modisp_b200.ragged import RaggedDispersion, _csr
+    off, flat = _csr([np.array([1., 2.]), np.array([3.]), np.array([])], 3)
+    assert off.tolist() == [0, 2, 3, 3] and flat.tolist() == [1., 2., 3.]
+    with pytest.raises(ValueError):
+        _csr([np.array([1.])], 2)
+    with pytest.raises(ValueError):
+        _csr([np.array([-1.]), np.array([2.])], 2)
+    with pytest.raises(ValueError):
+        _csr((np.array([0, 2, 1]), np.array([1., 2.])), 2)
+    modes = np.array([2, 1, 3])
+    cells = modes * np.diff(off)
+    outb = np.concatenate([[0], np.cumsum(cells)[:-1]])
+    vel = np.arange(cells.sum(), dtype=float)
+    r = RaggedDispersion(off, flat, modes, outb, vel, np.zeros(3, np.uint32), np.zeros(3, np.int32),
+                         np.array([2, 2, 1]), None, None, "rayleigh", {})
+    assert r.phase_velocity_of(0).tolist() == [[0., 1.], [2., 3.]]
+    assert r.phase_velocity_of(1).tolist() == [[4.]]
+    assert r.phase_velocity_of(2).shape == (3, 0)
+    assert r.root_count_of(0).tolist() == [2, 2]
