@@ -63,6 +63,7 @@ def parse():
     p.add_argument("--cpu-sample", type=int, default=128, help="models in the CPU-baseline sample")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-jacobian", action="store_true")
+    p.add_argument("--no-ragged", action="store_true")
     return p.parse_args()
 
 
@@ -248,6 +249,73 @@ def jacobian_bench(torch, local, steps, warmup, flush):
             "failed_roots": nan_rows, "unit": "roots/s"}
 
 
+RAGGED_MODELS = 10_000
+
+
+def ragged_bench(torch, local, steps, warmup, flush, models=RAGGED_MODELS):
+    """Large uneven batch: smooth-gradient models of 30-100 thin layers, each with its
+    own 50-120 periods inside 0.2-100 s and 1-10 modes, Rayleigh + Love, FP32 scan /
+    FP64 refinement, group velocity; one ragged (CSR) run per wave, both captured in
+    one CUDA graph that each step replays.  A seeded sample of the 1,000,000-model
+    workload (throughput does not depend on the batch size beyond filling the GPU)."""
+    from modisp_b200 import _native, workloads
+    batch, periods, modes = workloads.gradient_batch(models, seed=workloads.SEED + 50)
+    B, L = batch["thickness"].shape
+    off = np.zeros(B + 1, np.int32)
+    off[1:] = np.cumsum([p.size for p in periods])
+    flat = np.concatenate(periods)
+    md = np.asarray(modes, np.int32)
+    cells = md.astype(np.int64) * np.diff(off)
+    outb = np.zeros(B, np.int64)
+    outb[1:] = np.cumsum(cells)[:-1]
+    ntr, ncell = int(off[-1]), int(cells.sum())
+    dev = torch.device("cuda", local)
+    x = {k: torch.tensor(batch[k], device=dev) for k in ("thickness", "vp", "vs", "rho")}
+    meta = {k: torch.tensor(v, device=dev) for k, v in (("off", off), ("per", flat), ("md", md), ("outb", outb))}
+    vel = [torch.empty(ncell, dtype=torch.float64, device=dev) for _ in range(2)]
+    grp = [torch.empty_like(v) for v in vel]
+    gfl = [torch.empty(ncell, dtype=torch.int32, device=dev) for _ in range(2)]
+    tr = [[torch.empty(ntr, dtype=torch.int32, device=dev) for _ in range(3)] for _ in range(2)]
+    o = _native.default_options()
+    o.single_precision = 1
+    o.group_velocity = 1
+    eng = _native.Engine(local, B, L, int(np.diff(off).max()), int(md.max()), o)
+    eng.graph_begin()
+    for wave in (0, 1):
+        eng.run_ragged_device(x["thickness"].data_ptr(), x["vp"].data_ptr(), x["vs"].data_ptr(), x["rho"].data_ptr(),
+                              B, ntr, meta["off"].data_ptr(), meta["per"].data_ptr(), meta["md"].data_ptr(),
+                              meta["outb"].data_ptr(), TOL, 1., wave, vel[wave].data_ptr(), tr[wave][0].data_ptr(),
+                              tr[wave][1].data_ptr(), tr[wave][2].data_ptr(), grp[wave].data_ptr(),
+                              gfl[wave].data_ptr())
+    eng.graph_end()
+    stream = torch.cuda.current_stream().cuda_stream
+    for _ in range(warmup):
+        eng.graph_launch(stream)
+    torch.cuda.synchronize()
+    total = 0.
+    for _ in range(steps):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        eng.graph_launch(stream)
+        b.record()
+        b.synchronize()
+        total += a.elapsed_time(b)
+    roots = sum(int(torch.isfinite(v).sum()) for v in vel)
+    unconverged = sum(int((t[2] < 0).sum()) for t in tr)
+    eng.close()
+    return {"workload": f"{B} of the 1,000,000 smooth-gradient models (30-100 layers over 0-80 km), own 50-120 "
+                        "periods in 0.2-100 s, 1-10 modes each; Rayleigh + Love; ragged CSR batch, one CUDA graph",
+            "models": B, "traces_per_wave": ntr, "output_cells_per_wave": ncell, "roots_per_step": roots,
+            "ms_per_step": total / steps, "value": roots * steps / (total * 1e-3), "unit": "roots/s",
+            "unconverged_traces": unconverged, "launches_per_step": eng_launches_ragged()}
+
+
+def eng_launches_ragged():
+    # prep, init, tail values, scan, refine, repair select, repair scan, repair refine, assemble, group: per wave
+    return 2 * 10
+
+
 def device_run(torch, eng, tens, B, wave, stream):
     """Enqueue one engine run on device-resident tensors."""
     eng.run_device(tens["h"].data_ptr(), tens["vp"].data_ptr(), tens["vs"].data_ptr(), tens["rho"].data_ptr(), B,
@@ -385,6 +453,7 @@ def main():
         solver.close()
 
     jac = jacobian_bench(torch, local, max(2, args.steps // 2), 2, flush) if not args.no_jacobian else None
+    ragged = ragged_bench(torch, local, max(2, args.steps // 2), 2, flush) if not args.no_ragged else None
 
     peak32 = _native.measure_peak(local, fp64=False)
     peak64 = _native.measure_peak(local, fp64=True)
@@ -418,6 +487,7 @@ def main():
             "clocks": clocks.summary(),
             "engine_stats": {"rayleigh": e32_stats[0], "love": e32_stats[1]},
             "jacobian": jac,
+            "ragged": ragged,
         }
         print(json.dumps(line))
     if world > 1:

@@ -144,6 +144,19 @@ int md200_run_ragged_device(md200_engine *engine, const double *thickness, const
                             double *velocity, unsigned *flags, int *levels, int *counts, double *group,
                             unsigned *group_flags, unsigned long long *stats, void *stream);
 
+/* CUDA-graph capture of device-pointer runs (no counterpart in the reference,
+ * which launches its stages one by one, cpp/cuda/qe.cu:927-957).  Between
+ * md200_graph_begin and md200_graph_end, md200_run_device and
+ * md200_run_ragged_device calls made with stream NULL are recorded on the
+ * engine's stream instead of executed (one or more calls, e.g. both waves); the
+ * recorded launches read the device pointers given at capture, so a replay
+ * solves whatever those buffers hold at launch time.  md200_graph_launch
+ * replays the graph on `stream` (NULL = the engine's stream).  Stage times are
+ * not recorded inside a graph.  A new capture replaces the previous graph. */
+int md200_graph_begin(md200_engine *engine);
+int md200_graph_end(md200_engine *engine);
+int md200_graph_launch(md200_engine *engine, void *stream);
+
 /* Phase- and group-velocity Jacobians of solved roots (no counterpart in the
  * reference, which returns no derivatives; they serve the gradient of a misfit
  * between predicted and observed dispersion).  For every finite root

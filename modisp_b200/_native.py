@@ -74,6 +74,9 @@ EXPORTS = {
     "md200_run_ragged": (_I, [_P, _P, _P, _P, _P, _I, _P, _P, _P, _D, _D, _I, _P, _P, _P, _P, _P, _P, _P, _I]),
     "md200_run_ragged_device": (_I, [_P, _P, _P, _P, _P, _I, _I, _P, _P, _P, _P, _D, _D, _I, _P, _P, _P, _P, _P,
                                      _P, _P, _P]),
+    "md200_graph_begin": (_I, [_P]),
+    "md200_graph_end": (_I, [_P]),
+    "md200_graph_launch": (_I, [_P, _P]),
     "md200_jacobian_device": (_I, [_P, _P, _P, _P, _P, _I, _P, _I, _P, _P, _P, _P, _P]),
     "md200_jacobian": (_I, [_P, _P, _P, _P, _P, _I, _P, _I, _P, _P, _P, _P, ctypes.POINTER(_I)]),
     "md200_vjp_device": (_I, [_P, _P, _P, _P, _P, _I, _P, _I, _P, _P, _P, _P, _P, _P]),
@@ -277,6 +280,18 @@ class Engine:
         check(lib().md200_vjp_device(self.handle, c(h), c(vp), c(vs), c(rho), int(models), c(periods), int(wave),
                                      c(velocity), opt(group), opt(weight_phase), opt(weight_group), c(grad),
                                      _stream_arg(stream)))
+
+    def graph_begin(self):
+        """Start recording device-pointer runs (stream None) into a CUDA graph."""
+        check(lib().md200_graph_begin(self.handle))
+
+    def graph_end(self):
+        """Finish the recording and instantiate the graph."""
+        check(lib().md200_graph_end(self.handle))
+
+    def graph_launch(self, stream=None):
+        """Replay the recorded runs on `stream` (None = the engine's stream)."""
+        check(lib().md200_graph_launch(self.handle, _stream_arg(stream)))
 
     def stage_times(self) -> dict:
         """Device milliseconds per stage of the last run (waits for it)."""

@@ -75,6 +75,10 @@ struct md200_engine {
   static constexpr int NSTAGE = 9;
   cudaEvent_t ev[NSTAGE + 1] = {};
   bool profiling = false;
+  // CUDA graph of the calls captured between md200_graph_begin and md200_graph_end
+  bool capturing = false;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
 };
 
 namespace {
@@ -97,6 +101,8 @@ void release(md200_engine *e) {
   if (e->pinned) cudaFreeHost(e->pinned);
   for (auto &x : e->ev)
     if (x) cudaEventDestroy(x);
+  if (e->graph_exec) cudaGraphExecDestroy(e->graph_exec);
+  if (e->graph) cudaGraphDestroy(e->graph);
   if (e->stream) cudaStreamDestroy(e->stream);
   cudaSetDevice(prev);
 }
@@ -256,7 +262,9 @@ int enqueue(md200_engine *e, const double *h, const double *vp, const double *vs
   if (stats) MD200_CK(cudaMemsetAsync(stats, 0, sizeof(unsigned long long) * MD200_STAT_COUNT, s));
   // stage marks: 0 prep, 1 init, 2 scan, 3 refine, 4 repair collect, 5 repair scan,
   // 6 repair refine, 7 assemble, 8 group (empty stages record back-to-back events)
-  auto mark = [&](int i) { return cudaEventRecord(e->ev[i], s); };
+  // stage marks (not while a graph is being captured: the stage times are of
+  // direct runs)
+  auto mark = [&](int i) { return e->capturing ? cudaSuccess : cudaEventRecord(e->ev[i], s); };
   MD200_CK(mark(0));
   const int pw = e->prep_warps;
   prep_models<<<(B + pw - 1) / pw, 32 * pw, e->prep_smem, s>>>(d, e->sortcap, 0);
@@ -307,7 +315,7 @@ int enqueue(md200_engine *e, const double *h, const double *vp, const double *vs
     MD200_CK(cudaGetLastError());
   }
   MD200_CK(mark(9));
-  e->profiling = true;
+  if (!e->capturing) e->profiling = true;
   return 0;
 }
 
@@ -726,6 +734,44 @@ int md200_run_ragged(md200_engine *e, const double *h, const double *vp, const d
   if (stats && nstats > 0)
     MD200_CK(cudaMemcpy(stats, e->d_stats, sizeof(unsigned long long) * std::min(nstats, int(MD200_STAT_COUNT)),
                         cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+int md200_graph_begin(md200_engine *e) {
+  if (!e) return fail("modisp_b200: null engine");
+  if (e->capturing) return fail("modisp_b200: a graph capture is already open on this engine");
+  MD200_CK(cudaSetDevice(e->device));
+  MD200_CK(cudaStreamSynchronize(e->stream));
+  MD200_CK(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+  e->capturing = true;
+  return 0;
+}
+
+int md200_graph_end(md200_engine *e) {
+  if (!e) return fail("modisp_b200: null engine");
+  if (!e->capturing) return fail("modisp_b200: no graph capture is open on this engine");
+  MD200_CK(cudaSetDevice(e->device));
+  e->capturing = false;
+  cudaGraph_t g = nullptr;
+  MD200_CK(cudaStreamEndCapture(e->stream, &g));
+  cudaGraphExec_t x = nullptr;
+  const cudaError_t err = cudaGraphInstantiate(&x, g, 0);
+  if (err != cudaSuccess) {
+    cudaGraphDestroy(g);
+    return fail(std::string("modisp_b200 CUDA: ") + cudaGetErrorString(err) + " (cudaGraphInstantiate)");
+  }
+  if (e->graph_exec) cudaGraphExecDestroy(e->graph_exec);
+  if (e->graph) cudaGraphDestroy(e->graph);
+  e->graph = g;
+  e->graph_exec = x;
+  return 0;
+}
+
+int md200_graph_launch(md200_engine *e, void *stream) {
+  if (!e) return fail("modisp_b200: null engine");
+  if (!e->graph_exec) return fail("modisp_b200: no captured graph on this engine");
+  MD200_CK(cudaSetDevice(e->device));
+  MD200_CK(cudaGraphLaunch(e->graph_exec, stream ? static_cast<cudaStream_t>(stream) : e->stream));
   return 0;
 }
 

@@ -1,0 +1,81 @@
+"""CUDA-graph capture of device-pointer runs: a replay solves the current contents
+of the captured buffers exactly as a direct run does (bit for bit)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_graph_replay_matches_direct_runs():
+    import torch
+    from modisp_b200 import _native, workloads
+    dev = torch.device("cuda", 0)
+    periods = np.geomspace(0.5, 50., 30)
+    first = workloads.crustal_batch(64, workloads.SEED + 21)
+    second = workloads.crustal_batch(64, workloads.SEED + 22)
+    L = max(first["thickness"].shape[1], second["thickness"].shape[1])
+
+    def pad(batch):
+        out = {}
+        for k, v in batch.items():
+            extra = L - v.shape[1]
+            if k == "thickness":
+                out[k] = np.concatenate([v[:, :-1], np.zeros((v.shape[0], extra)), v[:, -1:]], axis=1)
+            else:
+                out[k] = np.concatenate([v[:, :-1], np.repeat(v[:, -1:], extra, 1), v[:, -1:]], axis=1)
+        return out
+
+    first, second = pad(first), pad(second)
+    B, T = 64, periods.size
+    o = _native.default_options()
+    o.single_precision = 1
+    o.group_velocity = 1
+    eng = _native.Engine(0, B, L, T, 5, o)
+    try:
+        x = {k: torch.tensor(first[k], device=dev) for k in ("thickness", "vp", "vs", "rho")}
+        per = torch.tensor(periods, device=dev)
+        vel = [torch.empty((B, 5, T), dtype=torch.float64, device=dev) for _ in range(2)]
+        grp = [torch.empty_like(v) for v in vel]
+        i32 = [[torch.empty(s, dtype=torch.int32, device=dev) for s in ((B, T), (B, T), (B, T), (B, 5, T))]
+               for _ in range(2)]
+
+        def runs(stream):
+            for wave in (0, 1):
+                fl, lv, ct, gf = i32[wave]
+                eng.run_device(x["thickness"].data_ptr(), x["vp"].data_ptr(), x["vs"].data_ptr(), x["rho"].data_ptr(),
+                               B, per.data_ptr(), 0, 1e-10, 1., wave, vel[wave].data_ptr(), fl.data_ptr(),
+                               lv.data_ptr(), ct.data_ptr(), grp[wave].data_ptr(), gf.data_ptr(), stream=stream)
+
+        torch.cuda.synchronize()
+        eng.graph_begin()
+        runs(None)  # recorded, not executed
+        eng.graph_end()
+        for batch in (first, second, first):
+            for k in x:
+                x[k].copy_(torch.tensor(batch[k], device=dev))
+            torch.cuda.synchronize()
+            eng.graph_launch()
+            torch.cuda.synchronize()
+            replay = [(v.cpu().numpy().copy(), g.cpu().numpy().copy(), i32[w][2].cpu().numpy().copy())
+                      for w, (v, g) in enumerate(zip(vel, grp))]
+            for wave in (0, 1):
+                direct = eng.run(batch["thickness"], batch["vp"], batch["vs"], batch["rho"], periods, None, 1e-10, 1.,
+                                 wave, group=True)
+                np.testing.assert_array_equal(replay[wave][0].view(np.uint64), direct["velocity"].view(np.uint64))
+                np.testing.assert_array_equal(replay[wave][1].view(np.uint64), direct["group_velocity"].view(np.uint64))
+                np.testing.assert_array_equal(replay[wave][2], direct["counts"])
+    finally:
+        eng.close()
+
+
+def test_graph_calls_are_checked():
+    from modisp_b200 import _native
+    o = _native.default_options()
+    eng = _native.Engine(0, 4, 3, 2, 2, o)
+    try:
+        with pytest.raises(RuntimeError, match="no captured graph"):
+            eng.graph_launch()
+        with pytest.raises(RuntimeError, match="no graph capture is open"):
+            eng.graph_end()
+    finally:
+        eng.close()
