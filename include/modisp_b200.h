@@ -39,6 +39,7 @@ enum md200_stat {
   MD200_STAT_DUAL_LAYER_STEPS = 12,/* layer steps of forward-mode derivative evaluations */
   MD200_STAT_CONT_ACCEPTED = 13,   /* continuation targets accepted */
   MD200_STAT_CONT_FALLBACK = 14,   /* continuation targets searched globally */
+  MD200_STAT_CONTINUITY = 15,      /* FP32-scan traces re-scanned by the continuity recheck */
   MD200_STAT_COUNT = 16
 };
 
@@ -65,6 +66,8 @@ typedef struct md200_options {
   int log_points;          /* background log-spaced points per window; <= 0 default */
   int warps_per_block;     /* scan CTA shape; <= 0 default */
   int blocks_per_sm;       /* persistent CTAs per SM; <= 0 default */
+  int continuity_check;    /* FP32 scan: re-scan in FP64 the traces whose roots leave the
+                              +-5 % envelope of both neighbouring periods (default 1) */
 } md200_options;
 
 /* Fill *options with the defaults of a high-accuracy FP64 engine. */
@@ -207,7 +210,9 @@ int md200_vjp(md200_engine *engine, const double *thickness, const double *vp, c
  * recorded on the run's stream (the reference's profile timings,
  * cpp/cuda/qe.cu:853-864): [0] model preparation, [1] trace list, [2] scan,
  * [3] refinement, [4] repair selection, [5] FP64 re-scan, [6] re-scan
- * refinement, [7] assembly, [8] group velocity.  Waits for the run to finish. */
+ * refinement, [7] assembly, [8] group velocity, [9] FP64 continuity recheck
+ * (screen, re-scan, refinement, assembly and group velocity of the suspects).
+ * Waits for the run to finish. */
 int md200_stage_times(md200_engine *engine, double *ms, int n);
 
 /* Number of kernel launches one md200_run of this engine enqueues. */

@@ -17,7 +17,7 @@ ABI_VERSION = 1
 STAT_NAMES = ("evaluations", "evaluations_fp32", "layer_steps", "layer_steps_fp32", "brackets",
               "trough_probes", "probe_pairs", "fp64_repair_traces", "unconverged", "group_roots",
               "roots", "traces", "dual_layer_steps", "continuation_accepted",
-              "continuation_fallbacks", "reserved")
+              "continuation_fallbacks", "continuity_rescans")
 STAT_COUNT = 16
 
 
@@ -44,6 +44,7 @@ class Options(ctypes.Structure):
         ("log_points", ctypes.c_int),
         ("warps_per_block", ctypes.c_int),
         ("blocks_per_sm", ctypes.c_int),
+        ("continuity_check", ctypes.c_int),
     ]
 
 
@@ -83,7 +84,7 @@ EXPORTS = {
     "md200_vjp": (_I, [_P, _P, _P, _P, _P, _I, _P, _I, _P, _P, _P, _P, _P]),
 }
 STAGES = ("prep", "trace_list", "scan", "refine", "repair_select", "repair_scan", "repair_refine",
-          "assemble", "group_velocity")
+          "assemble", "group_velocity", "continuity")
 
 
 def lib():

@@ -72,7 +72,7 @@ struct md200_engine {
   int jac_blocks = 0;
   std::vector<void *> owned;
   // per-stage timing (cudaEvent pairs on the run's stream)
-  static constexpr int NSTAGE = 9;
+  static constexpr int NSTAGE = 10;
   cudaEvent_t ev[NSTAGE + 1] = {};
   bool profiling = false;
   // CUDA graph of the calls captured between md200_graph_begin and md200_graph_end
@@ -315,6 +315,28 @@ int enqueue(md200_engine *e, const double *h, const double *vp, const double *vs
     MD200_CK(cudaGetLastError());
   }
   MD200_CK(mark(9));
+  if (d.fp32 && e->o.continuity_check) {
+    // FP64 continuity recheck: suspects of the bilateral envelope screen are
+    // re-scanned in FP64, refined, assembled and given group velocities again
+    MD200_CK(cudaMemsetAsync(d.ctr + C_REPAIR_CURSOR, 0, 2 * sizeof(int), s));
+    continuity_screen<<<(nt + 255) / 256, 256, 0, s>>>(d);
+    MD200_CK(cudaGetLastError());
+    if (wave == 0)
+      scan<double, 0><<<e->scan_blocks64, 32 * e->scan_warps, e->scan_smem64, s>>>(d, d.repair_list,
+                                                                                 C_REPAIR_CURSOR, C_NREPAIR);
+    else
+      scan<double, 1><<<e->scan_blocks64, 32 * e->scan_warps, e->scan_smem64, s>>>(d, d.repair_list,
+                                                                                 C_REPAIR_CURSOR, C_NREPAIR);
+    MD200_CK(cudaGetLastError());
+    refine<<<e->list_blocks, 128, 0, s>>>(d);
+    assemble<<<(nt + 255) / 256, 256, 0, s>>>(d, d.repair_list, C_NREPAIR);
+    MD200_CK(cudaGetLastError());
+    if (d.group) {
+      group_velocity<<<e->list_blocks, 128, 0, s>>>(d);
+      MD200_CK(cudaGetLastError());
+    }
+  }
+  MD200_CK(mark(10));
   if (!e->capturing) e->profiling = true;
   return 0;
 }
@@ -428,6 +450,7 @@ void md200_default_options(md200_options *o) {
   o->love_phase = 1;
   o->group_rtol = 1e-3;
   o->anchor_stride = 4;
+  o->continuity_check = 1;
 }
 
 md200_engine *md200_create(int device, int capacity, int layers, int periods, int nmodes,
@@ -788,7 +811,8 @@ int md200_stage_times(md200_engine *e, double *ms, int n) {
 
 int md200_kernel_launches(md200_engine *e) {
   if (!e) return -1;
-  return 6 + (e->d.fp32 ? 4 : 0) - (e->d.group ? 0 : 1);
+  const int check = e->d.fp32 && e->o.continuity_check ? 4 + (e->d.group ? 1 : 0) : 0;
+  return 6 + (e->d.fp32 ? 4 : 0) - (e->d.group ? 0 : 1) + check;
 }
 
 void md200_destroy(md200_engine *e) {

@@ -1198,9 +1198,16 @@ __global__ void collect_repairs(Dev d) {
 // ---------------------------------------------------------------------------
 // assemble: one thread per trace.
 // ---------------------------------------------------------------------------
-__global__ void assemble(Dev d) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= d.n_traces) return;
+// With `list`, only the traces list[0 .. ctr[count_id]) (re-solved traces)
+// are assembled again; their previous roots are taken out of the root count.
+__global__ void assemble(Dev d, const int *list = nullptr, int count_id = 0) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (list) {
+    if (t >= *(volatile int *)&d.ctr[count_id]) return;
+    t = list[t];
+  } else if (t >= d.n_traces) {
+    return;
+  }
   const int b = d.tr_model[t];
   const int nm = d.tr_modes[t], T = d.tr_stride[t];  // modes of this trace, stride between them
   const size_t out0 = static_cast<size_t>(d.tr_out[t]);
@@ -1300,11 +1307,75 @@ __global__ void assemble(Dev d) {
   d.olevels[t] = level;
   d.ocounts[t] = count;
   if (d.stats) {
-    atomicAdd(&d.stats[11], 1ULL);
+    if (!list) atomicAdd(&d.stats[11], 1ULL);
     if (failed) atomicAdd(&d.stats[8], 1ULL);
     int finite = 0;
     for (int mo = 0; mo < nm && mo < n; ++mo) finite += isfinite(d.vel[out0 + static_cast<size_t>(mo) * T]);
     if (finite) atomicAdd(&d.stats[10], static_cast<unsigned long long>(finite));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// continuity_screen: one thread per trace of an FP32-scan run, after assembly.
+// A trace is suspect when, with both neighbouring periods of its model within
+// a log step of 0.25 (the nearest shorter and longer period, in value order),
+// some mode has roots at both neighbours but is missing here or lies outside
+// [0.95 min, 1.05 max] of them -- the bilateral envelope of the reference's
+// continuity screen (cpp/cpu/continuity_screen.hpp:8-67).  Suspects are queued
+// for an FP64 re-scan (the repair list); their old roots are taken out of the
+// root count, their group-velocity entries re-queued.
+// ---------------------------------------------------------------------------
+__global__ void continuity_screen(Dev d) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t == 0) {
+    d.ctr[C_REFINE_BEGIN] = d.ctr[C_NREFINE];
+    d.ctr[C_GROUP_BEGIN] = d.ctr[C_NGROUP];
+  }
+  if (t >= d.n_traces) return;
+  const int b = d.tr_model[t];
+  if (d.mstate[b] != 0) return;
+  const unsigned fl = d.tflags[t];
+  if (fl & (TRACE_FP64_REPAIR | TRACE_SEARCH_UNCONVERGED)) return;
+  // the model's traces
+  int first, count;
+  if (d.ragged) {
+    first = d.r_offsets[b];
+    count = d.r_offsets[b + 1] - first;
+  } else {
+    first = b * d.T;
+    count = d.T;
+  }
+  const double p = d.tr_period[t];
+  int l = -1, r = -1;
+  double pl = 0., pr = INFINITY;
+  for (int j = 0; j < count; ++j) {
+    const double q = d.tr_period[first + j];
+    if (q < p && q > pl) { pl = q; l = first + j; }
+    if (q > p && q < pr) { pr = q; r = first + j; }
+  }
+  if (l < 0 || r < 0 || !(log(pr / pl) <= .25)) return;
+  const int nm = d.tr_modes[t];
+  const size_t o = static_cast<size_t>(d.tr_out[t]), ol = static_cast<size_t>(d.tr_out[l]),
+               orr = static_cast<size_t>(d.tr_out[r]);
+  const int s = d.tr_stride[t], sl = d.tr_stride[l], sr = d.tr_stride[r];
+  bool suspect = false;
+  for (int k = 0; k < nm && !suspect; ++k) {
+    const double cl = d.vel[ol + static_cast<size_t>(k) * sl], cr = d.vel[orr + static_cast<size_t>(k) * sr];
+    if (!(isfinite(cl) && isfinite(cr))) continue;
+    const double c = d.vel[o + static_cast<size_t>(k) * s];
+    suspect = !isfinite(c) || c < .95 * fmin(cl, cr) || c > 1.05 * fmax(cl, cr);
+  }
+  if (!suspect) return;
+  const int pos = atomicAdd(&d.ctr[C_NREPAIR], 1);
+  d.repair_list[pos] = t;
+  d.tflags[t] = fl | TRACE_FP64_REPAIR;
+  d.nbr[t] = 0;
+  atomicAdd(&d.ctr[C_NSUSPECT], 1);
+  if (d.stats) {
+    int finite = 0;
+    for (int k = 0; k < nm; ++k) finite += isfinite(d.vel[o + static_cast<size_t>(k) * s]);
+    if (finite) atomicAdd(&d.stats[10], static_cast<unsigned long long>(-finite));
+    atomicAdd(&d.stats[15], 1ULL);
   }
 }
 
@@ -1315,7 +1386,7 @@ __global__ void assemble(Dev d) {
 __global__ void group_velocity(Dev d) {
   const int n = d.ctr[C_NGROUP];
   unsigned long long steps = 0, count = 0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  for (int i = d.ctr[C_GROUP_BEGIN] + blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const int id = d.group_list[i];  // trace * KB + mode
     const int t = id / d.KB, mo = id - t * d.KB;
     const size_t cell = static_cast<size_t>(d.tr_out[t]) + static_cast<size_t>(mo) * d.tr_stride[t];
