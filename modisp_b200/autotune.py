@@ -1,0 +1,111 @@
+"""Launch-shape autotuner for the engine.
+
+The scan is a persistent kernel whose best CTA shape depends on the model depth,
+the period range and the wave: warps per CTA (1, 2 or 4 traces in flight per
+CTA) and the number of resident CTAs per SM trade latency hiding against
+instruction-cache and register pressure.  ``autotune`` times each candidate
+shape on a sample of the caller's workload (device time of a full run, best of
+``repeats``), checks that every shape returns bit-identical results (the launch
+shape must never change a root), and caches the fastest per device and
+workload geometry.
+
+The scan-grid density is not searched: 16 points per phase unit is the
+smallest density whose root sets matched the reference on the validation
+batches; coarser grids were faster but changed root sets, and denser ones only
+cost time.
+"""
+from __future__ import annotations
+
+import json
+import os
+from pathlib import Path
+
+import numpy as np
+
+from . import _native
+
+# (warps per CTA, CTAs per SM; 0 = as many as registers allow)
+CANDIDATES = ((4, 0), (4, 3), (4, 2), (2, 0), (2, 4), (1, 0))
+
+
+def cache_path() -> Path:
+    base = os.environ.get("MODISP_B200_CACHE") or os.path.join(os.path.expanduser("~"), ".cache", "modisp_b200")
+    return Path(base) / "autotune.json"
+
+
+def workload_key(device_name: str, layers: int, periods: int, nmodes: int, wave: int, single: bool) -> str:
+    """Cache key: device and the geometry buckets that move the optimum."""
+    lb = 1 << max(0, int(np.ceil(np.log2(max(layers, 1)))))  # layers rounded up to a power of two
+    return f"{device_name}|L{lb}|T{periods}|K{nmodes}|wave{wave}|{'fp32' if single else 'fp64'}"
+
+
+def _load(path: Path) -> dict:
+    try:
+        return json.loads(path.read_text())
+    except (OSError, ValueError):
+        return {}
+
+
+def _store(path: Path, table: dict) -> None:
+    try:
+        path.parent.mkdir(parents=True, exist_ok=True)
+        tmp = path.with_suffix(".tmp")
+        tmp.write_text(json.dumps(table, indent=1, sort_keys=True))
+        os.replace(tmp, path)
+    except OSError:
+        pass  # a read-only home only loses the cache
+
+
+def apply(options, shape) -> None:
+    options.warps_per_block, options.blocks_per_sm = int(shape[0]), int(shape[1])
+
+
+def measure(shape, sample, periods, nmodes, wave, single, device=0, repeats=2, tol=1e-10):
+    """Device milliseconds of one full run (best of ``repeats``) and its outputs."""
+    B, L = sample["thickness"].shape
+    o = _native.default_options()
+    o.single_precision = int(single)
+    o.group_velocity = 1
+    apply(o, shape)
+    eng = _native.Engine(device, B, L, len(periods), nmodes, o)
+    try:
+        args = (sample["thickness"], sample["vp"], sample["vs"], sample["rho"], np.asarray(periods, float), None, tol,
+                1., wave)
+        eng.run(*args, group=True)  # warm-up
+        best, out = np.inf, None
+        for _ in range(repeats):
+            out = eng.run(*args, group=True)
+            best = min(best, sum(eng.stage_times().values()))
+        return best, out
+    finally:
+        eng.close()
+
+
+def autotune(sample, periods, nmodes=5, wave=0, single=True, device=0, candidates=CANDIDATES, use_cache=True,
+             timer=measure):
+    """Fastest launch shape for this workload: (warps_per_block, blocks_per_sm).
+
+    ``sample``: a representative [B, L] batch (a few hundred to a few thousand
+    models).  ``timer`` is the measuring function (replaceable in tests).
+    """
+    name = _native.device_name(device) if timer is measure else "test-device"
+    key = workload_key(name, sample["thickness"].shape[1], len(periods), nmodes, wave, single)
+    path = cache_path()
+    table = _load(path) if use_cache else {}
+    if key in table:
+        return tuple(table[key]["shape"])
+    results, reference = [], None
+    for shape in candidates:
+        ms, out = timer(shape, sample, periods, nmodes, wave, single, device)
+        if reference is None:
+            reference = out
+        elif out is not None and reference is not None:
+            for field in ("velocity", "counts", "flags"):
+                if not np.array_equal(np.asarray(out[field]).view(np.uint8), np.asarray(reference[field]).view(np.uint8)):
+                    raise RuntimeError(f"launch shape {shape} changed the {field} output")
+        results.append((ms, shape))
+    ms, shape = min(results)
+    if use_cache:
+        table[key] = {"shape": list(shape), "ms": ms, "timings": {f"{s[0]}x{s[1]}": t for t, s in results}}
+        _store(path, table)
+    return tuple(shape)

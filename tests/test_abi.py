@@ -1,5 +1,6 @@
 """The C-ABI library and the Python binding, without a GPU."""
 import ctypes
+import json
 import re
 
 import numpy as np
@@ -127,3 +128,30 @@ def test_ragged_layout_and_validation():
     assert r.phase_velocity_of(1).tolist() == [[4.]]
     assert r.phase_velocity_of(2).shape == (3, 0)
     assert r.root_count_of(0).tolist() == [2, 2]
+
+
+def test_autotuner_picks_the_fastest_shape_and_caches_it(tmp_path, monkeypatch):
+    """Search, identity check and cache of the launch-shape autotuner (fake timer, no GPU)."""
+    from modisp_b200 import autotune
+    monkeypatch.setenv("MODISP_B200_CACHE", str(tmp_path))
+    sample = {k: np.ones((4, 6)) for k in ("thickness", "vp", "vs", "rho")}
+    same = {"velocity": np.arange(6.), "counts": np.arange(3), "flags": np.zeros(3, np.uint32)}
+    calls = []
+
+    def timer(shape, *args):
+        calls.append(shape)
+        return {(2, 0): 1.0}.get(tuple(shape), 2.0), same
+
+    best = autotune.autotune(sample, [1., 2.], 3, 0, True, timer=timer)
+    assert best == (2, 0) and len(calls) == len(autotune.CANDIDATES)
+    table = json.loads(autotune.cache_path().read_text())
+    assert list(table.values())[0]["shape"] == [2, 0]
+    calls.clear()
+    assert autotune.autotune(sample, [1., 2.], 3, 0, True, timer=timer) == (2, 0) and not calls  # cached
+
+    def bad_timer(shape, *args):
+        out = dict(same, velocity=same["velocity"] + (shape[0] == 1))
+        return 1.0, out
+
+    with pytest.raises(RuntimeError, match="changed"):
+        autotune.autotune(sample, [1., 2., 3.], 3, 0, True, timer=bad_timer, use_cache=False)

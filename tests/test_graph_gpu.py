@@ -79,3 +79,13 @@ def test_graph_calls_are_checked():
             eng.graph_end()
     finally:
         eng.close()
+
+
+def test_autotuner_on_a_sample(tmp_path, monkeypatch):
+    """Every launch shape returns the same roots; the tuner returns one of them."""
+    from modisp_b200 import autotune, workloads
+    monkeypatch.setenv("MODISP_B200_CACHE", str(tmp_path))
+    sample = workloads.crustal_batch(300, workloads.SEED + 41)
+    shape = autotune.autotune(sample, np.geomspace(0.5, 50., 30), 5, 0, True)
+    assert shape in autotune.CANDIDATES
+    assert autotune.cache_path().exists()
