@@ -124,13 +124,15 @@ int md200_run_device(md200_engine *engine, const double *thickness, const double
  *                                 non-decreasing; the total is at most capacity x
  *                                 the engine's periods)
  *   modes [models]              : mode count of model b, 1 .. the engine's nmodes
+ *   bounds [models, 2]          : search windows as in md200_run, or NULL (automatic)
  * Outputs: per trace (CSR order) flags, levels, counts [traces]; velocity (and
  * group, group_flags) hold, for model b, a [modes[b]][T_b] block (mode, period),
  * the blocks concatenated in model order (sum of modes[b] T_b values).
- * Trace semantics are those of md200_run; windows are computed on the device. */
+ * Trace semantics are those of md200_run. */
 int md200_run_ragged(md200_engine *engine, const double *thickness, const double *vp, const double *vs,
                      const double *rho, int models, const int *period_offsets, const double *periods,
-                     const int *modes, double c_tol_rel, double f_accept, int wave, double *velocity,
+                     const int *modes, const double *bounds, double c_tol_rel, double f_accept, int wave,
+                     double *velocity,
                      unsigned *flags, int *levels, int *counts, double *group, unsigned *group_flags,
                      unsigned long long *stats, int nstats);
 
@@ -143,7 +145,8 @@ int md200_run_ragged(md200_engine *engine, const double *thickness, const double
 int md200_run_ragged_device(md200_engine *engine, const double *thickness, const double *vp,
                             const double *vs, const double *rho, int models, int traces,
                             const int *period_offsets, const double *periods, const int *modes,
-                            const long long *out_offsets, double c_tol_rel, double f_accept, int wave,
+                            const long long *out_offsets, const double *bounds, double c_tol_rel,
+                            double f_accept, int wave,
                             double *velocity, unsigned *flags, int *levels, int *counts, double *group,
                             unsigned *group_flags, unsigned long long *stats, void *stream);
 

@@ -72,9 +72,10 @@ EXPORTS = {
     "md200_stage_times": (_I, [_P, ctypes.POINTER(ctypes.c_double), _I]),
     "md200_kernel_launches": (_I, [_P]),
     "md200_measure_peak": (_I, [_I, _I, ctypes.POINTER(ctypes.c_double)]),
-    "md200_run_ragged": (_I, [_P, _P, _P, _P, _P, _I, _P, _P, _P, _D, _D, _I, _P, _P, _P, _P, _P, _P, _P, _I]),
-    "md200_run_ragged_device": (_I, [_P, _P, _P, _P, _P, _I, _I, _P, _P, _P, _P, _D, _D, _I, _P, _P, _P, _P, _P,
-                                     _P, _P, _P]),
+    "md200_run_ragged": (_I, [_P, _P, _P, _P, _P, _I, _P, _P, _P, _P, _D, _D, _I, _P, _P, _P, _P, _P, _P, _P,
+                              _I]),
+    "md200_run_ragged_device": (_I, [_P, _P, _P, _P, _P, _I, _I, _P, _P, _P, _P, _P, _D, _D, _I, _P, _P, _P, _P,
+                                     _P, _P, _P, _P]),
     "md200_graph_begin": (_I, [_P]),
     "md200_graph_end": (_I, [_P]),
     "md200_graph_launch": (_I, [_P, _P]),
@@ -198,7 +199,8 @@ class Engine:
             c(stats) if stats else None, _stream_arg(stream))
         check(status)
 
-    def run_ragged(self, h, vp, vs, rho, period_offsets, periods, modes, tol, accept, wave, group=False):
+    def run_ragged(self, h, vp, vs, rho, period_offsets, periods, modes, tol, accept, wave, group=False,
+                   bounds=None):
         """Ragged host-array run: model b has periods[period_offsets[b]:period_offsets[b+1]]
         and modes[b] modes.  Returns flat outputs: velocity (and group) as the
         concatenated [modes[b], T_b] blocks, trace arrays in CSR order."""
@@ -216,8 +218,11 @@ class Engine:
         if group:
             out["group_velocity"] = np.empty(cells)
             out["group_velocity_flags"] = np.empty(cells, np.uint32)
+        bnd = None if bounds is None else np.ascontiguousarray(bounds, dtype=np.float64)
+        if bnd is not None and bnd.shape != (B, 2):
+            raise ValueError("bounds must be [models, 2]")
         check(lib().md200_run_ragged(self.handle, *(ptr(a) for a in arrays), B, ptr(off), ptr(per), ptr(md),
-                                     float(tol), float(accept), int(wave), ptr(out["velocity"]), ptr(out["flags"]),
+                                     ptr(bnd), float(tol), float(accept), int(wave), ptr(out["velocity"]), ptr(out["flags"]),
                                      ptr(out["levels"]), ptr(out["counts"]), ptr(out.get("group_velocity")),
                                      ptr(out.get("group_velocity_flags")), ptr(out["stats"]), STAT_COUNT))
         out["stats"] = dict(zip(STAT_NAMES, (int(x) for x in out["stats"])))
@@ -225,12 +230,13 @@ class Engine:
 
     def run_ragged_device(self, h, vp, vs, rho, models, traces, period_offsets, periods, modes, out_offsets, tol,
                           accept, wave, velocity, flags, levels, counts, group=None, group_flags=None, stats=None,
-                          stream=None):
+                          stream=None, bounds=None):
         """Device-pointer ragged run (integer addresses), enqueued on `stream`."""
         c = ctypes.c_void_p
         opt = lambda x: c(x) if x else None
         check(lib().md200_run_ragged_device(self.handle, c(h), c(vp), c(vs), c(rho), int(models), int(traces),
-                                            c(period_offsets), c(periods), c(modes), c(out_offsets), float(tol),
+                                            c(period_offsets), c(periods), c(modes), c(out_offsets), opt(bounds),
+                                            float(tol),
                                             float(accept), int(wave), c(velocity), c(flags), c(levels), c(counts),
                                             opt(group), opt(group_flags), opt(stats), _stream_arg(stream)))
 

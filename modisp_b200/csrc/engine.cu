@@ -671,8 +671,8 @@ int md200_vjp(md200_engine *e, const double *h, const double *vp, const double *
 
 int md200_run_ragged_device(md200_engine *e, const double *h, const double *vp, const double *vs,
                             const double *rho, int models, int traces, const int *period_offsets,
-                            const double *periods, const int *modes, const long long *out_offsets, double tol,
-                            double accept, int wave, double *velocity, unsigned *flags, int *levels, int *counts,
+                            const double *periods, const int *modes, const long long *out_offsets,
+                            const double *bounds, double tol, double accept, int wave, double *velocity, unsigned *flags, int *levels, int *counts,
                             double *group, unsigned *group_flags, unsigned long long *stats, void *stream) {
   if (validate_geometry(e, models)) return 1;
   if (traces < 1 || static_cast<long long>(traces) > static_cast<long long>(e->cap) * e->T)
@@ -687,13 +687,13 @@ int md200_run_ragged_device(md200_engine *e, const double *h, const double *vp, 
   rg.offsets = period_offsets;
   rg.modes = modes;
   rg.outbase = out_offsets;
-  return enqueue(e, h, vp, vs, rho, models, periods, nullptr, tol, accept, wave, velocity, flags, levels, counts,
+  return enqueue(e, h, vp, vs, rho, models, periods, bounds, tol, accept, wave, velocity, flags, levels, counts,
                  group, group_flags, nullptr, nullptr, stats, s, rg);
 }
 
 int md200_run_ragged(md200_engine *e, const double *h, const double *vp, const double *vs, const double *rho,
-                     int models, const int *period_offsets, const double *periods, const int *modes, double tol,
-                     double accept, int wave, double *velocity, unsigned *flags, int *levels, int *counts,
+                     int models, const int *period_offsets, const double *periods, const int *modes,
+                     const double *bounds, double tol, double accept, int wave, double *velocity, unsigned *flags, int *levels, int *counts,
                      double *group, unsigned *group_flags, unsigned long long *stats, int nstats) {
   if (validate_geometry(e, models)) return 1;
   if (!h || !vp || !vs || !rho || !period_offsets || !periods || !modes || !velocity || !flags || !levels ||
@@ -735,13 +735,15 @@ int md200_run_ragged(md200_engine *e, const double *h, const double *vp, const d
   MD200_CK(cudaMemcpy(e->rg_modes, modes, sizeof(int) * B, cudaMemcpyHostToDevice));
   MD200_CK(cudaMemcpy(e->rg_outbase, outbase.data(), sizeof(long long) * B, cudaMemcpyHostToDevice));
   MD200_CK(cudaMemcpy(e->rg_periods, periods, sizeof(double) * traces, cudaMemcpyHostToDevice));
+  if (bounds) MD200_CK(cudaMemcpy(e->in_bounds, bounds, sizeof(double) * 2 * B, cudaMemcpyHostToDevice));
   const bool grp = e->d.group != 0;
   Ragged rg;
   rg.ntraces = traces;
   rg.offsets = e->rg_offsets;
   rg.modes = e->rg_modes;
   rg.outbase = e->rg_outbase;
-  if (enqueue(e, e->in_h, e->in_vp, e->in_vs, e->in_rho, models, e->rg_periods, nullptr, tol, accept, wave,
+  if (enqueue(e, e->in_h, e->in_vp, e->in_vs, e->in_rho, models, e->rg_periods, bounds ? e->in_bounds : nullptr,
+              tol, accept, wave,
               e->out_vel, e->out_flags, e->out_levels, e->out_counts, grp ? e->out_grp : nullptr,
               grp ? e->out_gflags : nullptr, nullptr, nullptr, e->d_stats, s, rg))
     return 1;

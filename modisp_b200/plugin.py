@@ -23,7 +23,7 @@ VERSION = "0.5.0"
 SUPPORTS_FP32 = True
 SUPPORTS_AUTO_ACCURACY = True
 SUPPORTS_CANONICAL_LOWER = True
-SUPPORTS_ROW_PERIODS = False
+SUPPORTS_ROW_PERIODS = True
 SUPPORTS_GROUP_VELOCITY = True
 SUPPORTS_CONTINUATION = True
 __file__ = str(_native.LIBRARY)
@@ -146,13 +146,27 @@ class QeSolver:
         if any(a.shape != h.shape for a in arrays):
             raise ValueError("model shapes differ")
         per = np.ascontiguousarray(periods, dtype=np.float64)
-        if per.ndim != 1 or per.size != self.nf:
-            raise ValueError("periods must be a 1-D array of the engine's period count")
         bnd = np.ascontiguousarray(bounds, dtype=np.float64)
         if bnd.shape != (h.shape[0], 2):
             raise ValueError("bounds must be [B, 2]")
-        out = self._engine.run(h, *arrays, per, bnd, c_tol_rel, f_accept, int(wave),
-                               group=self.group_velocity, prediction=self.continuation)
+        B = h.shape[0]
+        if per.ndim == 2 and per.shape == (B, 1) and self.nf == 1:
+            # one period per model (cpp/cuda/qe.cu:1069-1070): a ragged batch of one trace per model
+            out = self._engine.run_ragged(h, *arrays, np.arange(B + 1, dtype=np.int32), per[:, 0],
+                                          np.full(B, self.nmodes, np.int32), c_tol_rel, f_accept, int(wave),
+                                          group=self.group_velocity, bounds=bnd)
+            shape = (B, self.nmodes, 1)
+            out["velocity"] = out["velocity"].reshape(shape)
+            if self.group_velocity:
+                out["group_velocity"] = out["group_velocity"].reshape(shape)
+                out["group_velocity_flags"] = out["group_velocity_flags"].reshape(shape)
+            for k in ("flags", "levels", "counts"):
+                out[k] = out[k].reshape(B, 1)
+        else:
+            if per.ndim != 1 or per.size != self.nf:
+                raise ValueError("periods must be a 1-D array of the engine's period count")
+            out = self._engine.run(h, *arrays, per, bnd, c_tol_rel, f_accept, int(wave),
+                                   group=self.group_velocity, prediction=self.continuation)
         velocity = out["velocity"].astype(np.float32) if self.single_precision else out["velocity"]
         stats = dict(out["stats"])
         stats.update(strategy="b200_scan", capacity=self.capacity)

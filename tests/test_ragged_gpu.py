@@ -95,6 +95,37 @@ def test_config5_sample_matches_reference(wave):
         assert np.all(np.abs(v[m] - rv[m]) <= 1e-9 * rv[m]), f"model {b}"
 
 
+def test_row_periods_through_the_plugin():
+    """One period per model ([B, 1] periods, SUPPORTS_ROW_PERIODS) equals solving
+    each model at its period in a uniform batch, windows included."""
+    from modisp_b200 import plugin, workloads
+    batch = workloads.crustal_batch(40, workloads.SEED + 13)
+    B, L = batch["thickness"].shape
+    rng = np.random.default_rng(8)
+    per = rng.uniform(0.5, 40., (B, 1))
+    bounds = np.zeros((B, 2))
+    bounds[:, 1] = np.inf
+    bounds[::3, 1] = 3.0  # some truncated windows
+    s = plugin.QeSolver(B, L, 1, 4, 0, 0., .005, True, .001, 0, 1, 1, False, True, .001, False, 4)
+    try:
+        v, flags, _, levels, counts, extras = s.run(batch["thickness"], batch["vp"], batch["vs"], batch["rho"], per,
+                                                    bounds, 1e-10, 1., 0)
+    finally:
+        s.close()
+    assert v.shape == (B, 4, 1) and counts.shape == (B, 1)
+    for b in range(B):
+        one = plugin.QeSolver(1, L, 1, 4, 0, 0., .005, True, .001, 0, 1, 1, False, True, .001, False, 4)
+        try:
+            v1, f1, _, l1, c1, e1 = one.run(batch["thickness"][b:b + 1], batch["vp"][b:b + 1], batch["vs"][b:b + 1],
+                                            batch["rho"][b:b + 1], per[b], bounds[b:b + 1], 1e-10, 1., 0)
+        finally:
+            one.close()
+        np.testing.assert_array_equal(v[b].view(np.uint64), v1[0].view(np.uint64))
+        np.testing.assert_array_equal(extras["group_velocity"][b].view(np.uint64),
+                                      e1["group_velocity"][0].view(np.uint64))
+        assert counts[b, 0] == c1[0, 0] and flags[b, 0] == f1[0, 0]
+
+
 def test_ragged_device_entry_matches_host():
     import torch
     from modisp_b200 import workloads
