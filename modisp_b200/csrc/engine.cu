@@ -71,6 +71,9 @@ struct md200_engine {
   double *rg_periods = nullptr;
   int jac_blocks = 0;
   std::vector<void *> owned;
+  // host-path pipelining: one event per chunk of models
+  static constexpr int MAX_CHUNKS = 8;
+  cudaEvent_t chunk_ev[MAX_CHUNKS] = {};
   // per-stage timing (cudaEvent pairs on the run's stream)
   static constexpr int NSTAGE = 10;
   cudaEvent_t ev[NSTAGE + 1] = {};
@@ -100,6 +103,8 @@ void release(md200_engine *e) {
   e->owned.clear();
   if (e->pinned) cudaFreeHost(e->pinned);
   for (auto &x : e->ev)
+    if (x) cudaEventDestroy(x);
+  for (auto &x : e->chunk_ev)
     if (x) cudaEventDestroy(x);
   if (e->graph_exec) cudaGraphExecDestroy(e->graph_exec);
   if (e->graph) cudaGraphDestroy(e->graph);
@@ -145,7 +150,8 @@ int setup(md200_engine *e) {
       own_alloc(e, &d.trace_list, nt) || own_alloc(e, &d.repair_list, nt) ||
       own_alloc(e, &d.refine_list, 2 * nt * d.KB) ||
       own_alloc(e, &d.group_list, nt * nm) || own_alloc(e, &d.ctr, C_COUNT) ||
-      own_alloc(e, &d.gwin, nt * nm * 2) || own_alloc(e, &e->d_stats, MD200_STAT_COUNT))
+      own_alloc(e, &d.gwin, nt * nm * 2) ||
+      own_alloc(e, &e->d_stats, static_cast<size_t>(MD200_STAT_COUNT) * md200_engine::MAX_CHUNKS))
     return 1;
   // host-path device buffers
   if (own_alloc(e, &e->in_h, static_cast<size_t>(B) * L) ||
@@ -160,7 +166,8 @@ int setup(md200_engine *e) {
     return 1;
   e->pinned_bytes = sizeof(double) * (4 * static_cast<size_t>(B) * L + T + 2 * static_cast<size_t>(B)) +
                     nt * nm * (2 * sizeof(double) + sizeof(unsigned)) + nt * 4 * sizeof(int) +
-                    MD200_STAT_COUNT * sizeof(unsigned long long) + 2 * sizeof(double) * B + 64;
+                    md200_engine::MAX_CHUNKS * MD200_STAT_COUNT * sizeof(unsigned long long) +
+                    2 * sizeof(double) * B + 64;
   MD200_CK(cudaMallocHost(reinterpret_cast<void **>(&e->pinned), e->pinned_bytes));
 
   // launch shapes
@@ -194,6 +201,7 @@ int setup(md200_engine *e) {
   e->prep_warps = 4;
   e->prep_smem = static_cast<size_t>(e->prep_warps) * cap2 * (sizeof(double) + sizeof(int));
   for (auto &x : e->ev) MD200_CK(cudaEventCreate(&x));
+  for (auto &x : e->chunk_ev) MD200_CK(cudaEventCreateWithFlags(&x, cudaEventDisableTiming));
   MD200_CK(cudaFuncSetAttribute(prep_models, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(std::max<size_t>(e->prep_smem, 1024))));
   return 0;
@@ -527,12 +535,13 @@ int md200_run(md200_engine *e, const double *h, const double *vp, const double *
     MD200_CK(cudaMemcpyAsync(e->in_bounds, ph + 4 * B * L + T, sizeof(double) * 2 * B,
                              cudaMemcpyHostToDevice, s));
   const bool grp = e->d.group != 0;
-  if (enqueue(e, e->in_h, e->in_vp, e->in_vs, e->in_rho, models, e->in_per,
-              bounds ? e->in_bounds : nullptr, tol, accept, wave, e->out_vel, e->out_flags,
-              e->out_levels, e->out_counts, grp ? e->out_grp : nullptr, grp ? e->out_gflags : nullptr,
-              prediction_flags ? e->out_pred : nullptr, e->in_bounds + 0, e->d_stats, s))
-    return 1;
-  // outputs back through pinned memory
+  // Large batches run in chunks of models, every chunk's outputs copied back as
+  // soon as it is solved, so the host copies (and first-touch page faults) of
+  // chunk i overlap the solve of chunk i + 1.  Every trace is independent: the
+  // results are those of one run.
+  // (each chunk adds a scan tail, so only batches far larger than the GPU's
+  // resident traces are split)
+  const int nchunk = B >= 65536 ? 4 : 1;
   double *ov = reinterpret_cast<double *>(p);
   double *og = ov + nt * nm;
   unsigned *ogf = reinterpret_cast<unsigned *>(og + nt * nm);
@@ -542,35 +551,60 @@ int md200_run(md200_engine *e, const double *h, const double *vp, const double *
   unsigned *opr = reinterpret_cast<unsigned *>(oct + nt);
   unsigned long long *ost = reinterpret_cast<unsigned long long *>(
       (reinterpret_cast<uintptr_t>(opr + nt) + 7) & ~uintptr_t(7));
-  MD200_CK(cudaMemcpyAsync(ov, e->out_vel, sizeof(double) * nt * nm, cudaMemcpyDeviceToHost, s));
-  MD200_CK(cudaMemcpyAsync(ofl, e->out_flags, sizeof(unsigned) * nt, cudaMemcpyDeviceToHost, s));
-  MD200_CK(cudaMemcpyAsync(olv, e->out_levels, sizeof(int) * nt, cudaMemcpyDeviceToHost, s));
-  MD200_CK(cudaMemcpyAsync(oct, e->out_counts, sizeof(int) * nt, cudaMemcpyDeviceToHost, s));
-  if (grp) {
-    MD200_CK(cudaMemcpyAsync(og, e->out_grp, sizeof(double) * nt * nm, cudaMemcpyDeviceToHost, s));
-    MD200_CK(cudaMemcpyAsync(ogf, e->out_gflags, sizeof(unsigned) * nt * nm, cudaMemcpyDeviceToHost, s));
+  double *obd = reinterpret_cast<double *>(ost + static_cast<size_t>(MD200_STAT_COUNT) * md200_engine::MAX_CHUNKS);
+  auto chunk_begin = [&](int c) { return B * c / nchunk; };
+  for (int c = 0; c < nchunk; ++c) {
+    const size_t b0 = chunk_begin(c), nb = chunk_begin(c + 1) - b0;
+    const size_t cm = b0 * nm * T, ct = b0 * T, cells = nb * nm * T, traces = nb * T;
+    unsigned long long *cstats = e->d_stats + static_cast<size_t>(c) * MD200_STAT_COUNT;
+    if (enqueue(e, e->in_h + b0 * L, e->in_vp + b0 * L, e->in_vs + b0 * L, e->in_rho + b0 * L,
+                static_cast<int>(nb), e->in_per, bounds ? e->in_bounds + 2 * b0 : nullptr, tol, accept, wave,
+                e->out_vel + cm, e->out_flags + ct, e->out_levels + ct, e->out_counts + ct,
+                grp ? e->out_grp + cm : nullptr, grp ? e->out_gflags + cm : nullptr,
+                prediction_flags ? e->out_pred + ct : nullptr, e->in_bounds + 2 * b0, cstats, s))
+      return 1;
+    MD200_CK(cudaMemcpyAsync(ov + cm, e->out_vel + cm, sizeof(double) * cells, cudaMemcpyDeviceToHost, s));
+    MD200_CK(cudaMemcpyAsync(ofl + ct, e->out_flags + ct, sizeof(unsigned) * traces, cudaMemcpyDeviceToHost, s));
+    MD200_CK(cudaMemcpyAsync(olv + ct, e->out_levels + ct, sizeof(int) * traces, cudaMemcpyDeviceToHost, s));
+    MD200_CK(cudaMemcpyAsync(oct + ct, e->out_counts + ct, sizeof(int) * traces, cudaMemcpyDeviceToHost, s));
+    if (grp) {
+      MD200_CK(cudaMemcpyAsync(og + cm, e->out_grp + cm, sizeof(double) * cells, cudaMemcpyDeviceToHost, s));
+      MD200_CK(cudaMemcpyAsync(ogf + cm, e->out_gflags + cm, sizeof(unsigned) * cells, cudaMemcpyDeviceToHost, s));
+    }
+    if (prediction_flags)
+      MD200_CK(cudaMemcpyAsync(opr + ct, e->out_pred + ct, sizeof(unsigned) * traces, cudaMemcpyDeviceToHost, s));
+    // the prep stage wrote the windows it used over the (already consumed) input windows
+    if (bounds_out)
+      MD200_CK(cudaMemcpyAsync(obd + 2 * b0, e->in_bounds + 2 * b0, sizeof(double) * 2 * nb,
+                               cudaMemcpyDeviceToHost, s));
+    MD200_CK(cudaEventRecord(e->chunk_ev[c], s));
   }
-  if (prediction_flags)
-    MD200_CK(cudaMemcpyAsync(opr, e->out_pred, sizeof(unsigned) * nt, cudaMemcpyDeviceToHost, s));
-  // the prep stage wrote the windows it used over the (already consumed) input windows
-  double *obd = reinterpret_cast<double *>(ost + MD200_STAT_COUNT);
-  if (bounds_out)
-    MD200_CK(cudaMemcpyAsync(obd, e->in_bounds, sizeof(double) * 2 * B, cudaMemcpyDeviceToHost, s));
-  MD200_CK(cudaMemcpyAsync(ost, e->d_stats, sizeof(unsigned long long) * MD200_STAT_COUNT,
+  MD200_CK(cudaMemcpyAsync(ost, e->d_stats, sizeof(unsigned long long) * MD200_STAT_COUNT * nchunk,
                            cudaMemcpyDeviceToHost, s));
-  MD200_CK(cudaStreamSynchronize(s));
-  std::memcpy(velocity, ov, sizeof(double) * nt * nm);
-  std::memcpy(flags, ofl, sizeof(unsigned) * nt);
-  std::memcpy(levels, olv, sizeof(int) * nt);
-  std::memcpy(counts, oct, sizeof(int) * nt);
-  if (grp) {
-    std::memcpy(group, og, sizeof(double) * nt * nm);
-    std::memcpy(group_flags, ogf, sizeof(unsigned) * nt * nm);
+  for (int c = 0; c < nchunk; ++c) {
+    MD200_CK(cudaEventSynchronize(e->chunk_ev[c]));
+    const size_t b0 = chunk_begin(c), nb = chunk_begin(c + 1) - b0;
+    const size_t cm = b0 * nm * T, ct = b0 * T, cells = nb * nm * T, traces = nb * T;
+    std::memcpy(velocity + cm, ov + cm, sizeof(double) * cells);
+    std::memcpy(flags + ct, ofl + ct, sizeof(unsigned) * traces);
+    std::memcpy(levels + ct, olv + ct, sizeof(int) * traces);
+    std::memcpy(counts + ct, oct + ct, sizeof(int) * traces);
+    if (grp) {
+      std::memcpy(group + cm, og + cm, sizeof(double) * cells);
+      std::memcpy(group_flags + cm, ogf + cm, sizeof(unsigned) * cells);
+    }
+    if (prediction_flags) std::memcpy(prediction_flags + ct, opr + ct, sizeof(unsigned) * traces);
+    if (bounds_out) std::memcpy(bounds_out + 2 * b0, obd + 2 * b0, sizeof(double) * 2 * nb);
   }
-  if (prediction_flags) std::memcpy(prediction_flags, opr, sizeof(unsigned) * nt);
-  if (bounds_out) std::memcpy(bounds_out, obd, sizeof(double) * 2 * B);
-  if (stats && nstats > 0)
-    std::memcpy(stats, ost, sizeof(unsigned long long) * std::min(nstats, int(MD200_STAT_COUNT)));
+  MD200_CK(cudaStreamSynchronize(s));
+  if (stats && nstats > 0) {
+    const int n = std::min(nstats, int(MD200_STAT_COUNT));
+    for (int i = 0; i < n; ++i) {
+      unsigned long long sum = 0;
+      for (int c = 0; c < nchunk; ++c) sum += ost[static_cast<size_t>(c) * MD200_STAT_COUNT + i];
+      stats[i] = sum;
+    }
+  }
   return 0;
 }
 

@@ -89,3 +89,42 @@ def test_autotuner_on_a_sample(tmp_path, monkeypatch):
     shape = autotune.autotune(sample, np.geomspace(0.5, 50., 30), 5, 0, True)
     assert shape in autotune.CANDIDATES
     assert autotune.cache_path().exists()
+
+
+def test_chunked_host_run_equals_device_run():
+    """The host path solves large batches in pipelined chunks; the results are those
+    of one device-pointer run over the whole batch (bit for bit), stats summed."""
+    import torch
+    from modisp_b200 import _native, workloads
+    batch = workloads.crustal_batch(70000, workloads.SEED + 51, nmin=3, nmax=6)
+    periods = np.geomspace(1., 40., 6)
+    B, L = batch["thickness"].shape
+    o = _native.default_options()
+    o.single_precision = 1
+    o.group_velocity = 1
+    eng = _native.Engine(0, B, L, periods.size, 3, o)
+    try:
+        host = eng.run(batch["thickness"], batch["vp"], batch["vs"], batch["rho"], periods, None, 1e-10, 1., 0,
+                       group=True)
+        dev = torch.device("cuda", 0)
+        x = {k: torch.tensor(batch[k], device=dev) for k in ("thickness", "vp", "vs", "rho")}
+        per = torch.tensor(periods, device=dev)
+        vel = torch.empty((B, 3, periods.size), dtype=torch.float64, device=dev)
+        grp = torch.empty_like(vel)
+        gfl = torch.empty((B, 3, periods.size), dtype=torch.int32, device=dev)
+        fl, lv, ct = (torch.empty((B, periods.size), dtype=torch.int32, device=dev) for _ in range(3))
+        st = torch.zeros(16, dtype=torch.int64, device=dev)
+        eng.run_device(x["thickness"].data_ptr(), x["vp"].data_ptr(), x["vs"].data_ptr(), x["rho"].data_ptr(), B,
+                       per.data_ptr(), 0, 1e-10, 1., 0, vel.data_ptr(), fl.data_ptr(), lv.data_ptr(), ct.data_ptr(),
+                       grp.data_ptr(), gfl.data_ptr(), stats=st.data_ptr(),
+                       stream=torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+    finally:
+        eng.close()
+    np.testing.assert_array_equal(host["velocity"].view(np.uint64), vel.cpu().numpy().view(np.uint64))
+    np.testing.assert_array_equal(host["group_velocity"].view(np.uint64), grp.cpu().numpy().view(np.uint64))
+    np.testing.assert_array_equal(host["counts"], ct.cpu().numpy())
+    np.testing.assert_array_equal(host["flags"], fl.cpu().numpy().astype(np.uint32))
+    stats = st.cpu().numpy()
+    assert host["stats"]["roots"] == stats[10] == int(np.isfinite(host["velocity"]).sum())
+    assert host["stats"]["traces"] == stats[11] == B * periods.size
