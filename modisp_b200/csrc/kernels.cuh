@@ -791,6 +791,307 @@ __device__ __noinline__ int last_cell(const LayerView<T> view, const LayerView<d
 #ifndef MD200_SCAN_MIN_BLOCKS
 #define MD200_SCAN_MIN_BLOCKS 4
 #endif
+
+// ---------------------------------------------------------------------------
+// The scan of one trace as a sequence of 32-sample steps: positions, values,
+// bookkeeping.  One warp runs a trace from start to end (persistent kernel
+// `scan`, the model table in shared memory).  Splitting the steps into rounds
+// of a one-thread-per-sample evaluation kernel and a one-warp-per-trace
+// bookkeeping kernel, with the state in global memory between them, gave the
+// same brackets bit for bit but was slower (45 vs 39 ms for the Rayleigh
+// FP32 scan of 10,000 crustal models): the bookkeeping costs more on its own
+// than interleaved with the evaluations of other warps.
+// ---------------------------------------------------------------------------
+
+// Per-trace scan state carried between steps.
+struct ScanState {
+  long long gi, J;         // next grid index, last grid index
+  int si, nbr, nseg;       // next seed, brackets held, sign changes so far
+  unsigned tfl;            // trace flags
+  int bits;                // 1 have1, 2 hr1, 4 hr2, 8 ex1, 16 finished
+  double c1, F1;           // the last sample (bracketing against the next step)
+  double zoom_right;       // right end of the last zoomed window (windows never overlap)
+  Sample R1, R2;           // the last two regular samples
+};
+constexpr int SS_HAVE1 = 1, SS_HR1 = 2, SS_HR2 = 4, SS_EX1 = 8, SS_FINISHED = 16;
+
+// Trace constants (recomputed wherever a trace is picked up).
+struct TraceCtx {
+  int t, b, K, nsteps, nk, ns;
+  double w, fr, alpha, u_lo, hi;
+  const double4 *kt;
+  const double *sd;
+  double *slot;
+  const double4 *tail;
+};
+
+struct ScanCounters {
+  unsigned long long evals = 0, evals32 = 0, steps = 0, steps32 = 0, zooms = 0;
+};
+
+__device__ __forceinline__ TraceCtx trace_ctx(const Dev &d, int t) {
+  TraceCtx x;
+  x.t = t;
+  x.b = d.tr_model[t];
+  x.K = d.tr_modes[t] + 2;  // nmodes + 2 guard roots
+  const double period = d.tr_period[t];
+  x.w = TWO_PI / period;
+  x.fr = 1. / period;
+  x.nsteps = layer_steps(d.mL[x.b], d.mwater[x.b]);
+  x.kt = d.knot + static_cast<size_t>(x.b) * d.nkmax;
+  x.nk = d.nknot[x.b];
+  x.alpha = d.malpha[x.b];
+  x.u_lo = fma(x.fr, x.kt[0].y, x.alpha * x.kt[0].z);
+  x.sd = d.seed + static_cast<size_t>(x.b) * d.nsmax;
+  x.ns = d.nseed[x.b];
+  x.hi = d.mhi[x.b];
+  x.slot = d.slot + static_cast<size_t>(t) * d.KB * SLOT;
+  x.tail = d.tail + 2 * static_cast<size_t>(t);
+  return x;
+}
+
+__device__ __forceinline__ ScanState scan_start(const Dev &d, const TraceCtx &x) {
+  ScanState st;
+  const double u_hi = fma(x.fr, x.kt[x.nk - 1].y, x.alpha * x.kt[x.nk - 1].z);
+  long long J = static_cast<long long>(ceil((u_hi - x.u_lo) * d.density)) - 1;
+  st.tfl = 0;
+  if (J < 0) J = 0;
+  if (J > JMAX) {
+    J = JMAX;
+    st.tfl |= TRACE_WORKSPACE_LIMIT;
+  }
+  st.J = J;
+  st.gi = 1;
+  st.si = st.nbr = st.nseg = 0;
+  st.bits = 0;
+  st.c1 = st.F1 = 0.;
+  st.zoom_right = -INFINITY;
+  st.R1 = Sample{0., 0.f, 0.f, 0};
+  st.R2 = Sample{0., 0.f, 0.f, 0};
+  return st;
+}
+
+// The next 32 sample positions: grid points and seeds merged in order (this
+// lane's position in c; INFINITY past the window).  Returns the valid-lane mask.
+__device__ __forceinline__ unsigned scan_positions(const TraceCtx &x, ScanState &st, double step, int lane,
+                                                   double *mbuf, int &kfrom, double &c) {
+  const long long gj = st.gi + lane;
+  const double gv = gj <= st.J ? scan_point(x.kt, x.nk, x.fr, x.alpha, x.u_lo + static_cast<double>(gj) * step,
+                                            kfrom)
+                               : INFINITY;
+  const double sv = st.si + lane < x.ns ? x.sd[st.si + lane] : INFINITY;
+  const int rg = warp_rank(sv, gv, false);  // seeds strictly below this scan point
+  const int rs = warp_rank(gv, sv, true);   // scan points at or below this seed
+  const int pg = lane + rg, ps = lane + rs;
+  mbuf[lane] = INFINITY;
+  __syncwarp();
+  if (pg < 32) mbuf[pg] = gv;
+  if (ps < 32) mbuf[ps] = sv;
+  __syncwarp();
+  c = mbuf[lane];
+  __syncwarp();
+  st.gi += __popc(__ballot_sync(FULL, pg < 32 && gv < INFINITY));
+  st.si += __popc(__ballot_sync(FULL, ps < 32 && sv < INFINITY));
+  return __ballot_sync(FULL, c < INFINITY);
+}
+
+// Single-precision position of a sample (FP32 scan): rounded to float and kept
+// below hi, except in the near-cutoff band, whose samples stay at their exact
+// positions and are evaluated in FP64 only.
+__device__ __forceinline__ float scan_position32(double &c, double hi, bool &near_cut) {
+  const bool valid = c < INFINITY;
+  near_cut = valid && c >= hi * (1. - 1e-4);
+  float x = valid ? static_cast<float>(c) : 1.f;
+  if (valid && static_cast<double>(x) > hi) x = nextafterf(x, 0.f);
+  if (valid && !near_cut) c = static_cast<double>(x);
+  return x;
+}
+
+// FP64 completion of a single-precision sample: the near-cutoff band takes the
+// trace's precomputed FP64 values where they match, and sign-uncertain samples
+// (small |g|) and the rest of that band are evaluated in FP64.  Returns true
+// when this lane needed an FP64 evaluation.
+template <int WAVE>
+__device__ __forceinline__ bool scan_complete32(const LayerView<double> &view64, double w, const double4 *tail,
+                                                double c, bool valid, bool near_cut, double &F, double &g, double &M,
+                                                bool &exact) {
+  bool have_tail = false;
+  exact = false;
+  if (near_cut) {
+    const double4 t0 = tail[0], t1 = tail[1];
+    const double4 tv = c == t0.x ? t0 : t1;
+    if (c == tv.x && isfinite(tv.y)) {
+      F = tv.y;
+      g = tv.z;
+      M = tv.w;
+      exact = true;
+      have_tail = true;
+    }
+  }
+  const bool redo = valid && !have_tail && (!(fabs(g) > MD200_REDO_G) || near_cut);
+  if (redo) {
+    F = eval64_outline(view64, WAVE, w, c, &g, &M);
+    exact = true;
+  }
+  return redo;
+}
+
+// One step's bookkeeping: brackets from sign changes, trough tests and zooms,
+// the carries.  `vm`: valid lanes of the step.
+template <class T, int WAVE>
+__device__ __forceinline__ void scan_bookkeep(const Dev &d, const TraceCtx &x, ScanState &st, const LayerView<T> &view,
+                                              const LayerView<double> &view64, int lane, double c, double F,
+                                              double g, double M, bool exact, unsigned vm, ScanCounters &ctr) {
+  constexpr bool single = sizeof(T) == 4;
+  const unsigned lt = lanemask_lt(), le = lt | (1u << lane);
+  const int K = x.K;
+  const bool valid = c < INFINITY;
+  const int nvalid = __popc(vm);
+  if (__any_sync(FULL, valid && !(isfinite(F) && isfinite(g)))) {
+    st.tfl |= TRACE_NONFINITE | TRACE_SEARCH_UNCONVERGED;
+    st.bits |= SS_FINISHED;
+    return;
+  }
+  // ---- sign changes against the immediate left neighbour ----
+  double cl = __shfl_up_sync(FULL, c, 1), Fl = __shfl_up_sync(FULL, F, 1);
+  bool exl = __shfl_up_sync(FULL, exact, 1);
+  const bool vl = lane >= 1 ? lane - 1 < nvalid : (st.bits & SS_HAVE1) != 0;
+  if (lane == 0) {
+    cl = st.c1;
+    Fl = st.F1;
+    exl = (st.bits & SS_EX1) != 0;
+  }
+  const bool sc = valid && vl && (signbit(Fl) != signbit(F));  // +0 counts as positive
+  const unsigned scm = __ballot_sync(FULL, sc);
+  const int myseg = st.nseg + __popc(scm & le);
+  Sample me{c, static_cast<float>(g), static_cast<float>(M),
+            myseg | (exact ? (1 << 29) : 0) | (signbit(F) ? (1 << 30) : 0)};
+  // ---- regular samples and their two regular predecessors ----
+  const bool reg = valid && !(vl && c - cl < 1e-6 * c);
+  const unsigned rmask = __ballot_sync(FULL, reg);
+  const unsigned m1 = rmask & lt;
+  const int j1 = m1 ? 31 - __clz(m1) : -1;
+  const unsigned m2 = j1 >= 0 ? (m1 & ~(1u << j1)) : 0u;
+  const int j2 = m2 ? 31 - __clz(m2) : -1;
+  Sample P1 = shfl_sample(me, j1 & 31), P2 = shfl_sample(me, j2 & 31);
+  bool hp1 = j1 >= 0, hp2 = j2 >= 0;
+  if (j1 < 0) {
+    P1 = st.R1; hp1 = (st.bits & SS_HR1) != 0;
+    P2 = st.R2; hp2 = (st.bits & SS_HR2) != 0;
+  } else if (j2 < 0) {
+    P2 = st.R1; hp2 = (st.bits & SS_HR1) != 0;
+  }
+  // ---- same-sign troughs: V-shaped shape-feature minima, log-magnitude dips ----
+  bool tr = false, trm_ = false;
+  if (reg && hp1 && hp2 && sample_segment(P2) == myseg && sample_segment(P1) == myseg) {
+    const double sgn = sample_sign(P1);
+    tr = trough_may_hide_roots(P2.c, P1.c, c, sgn * P2.g, sgn * P1.g, sgn * static_cast<float>(g),
+                               pair_noise(single, P2, P1), pair_noise(single, P1, me));
+    if (!tr) trm_ = magnitude_dip(P2.c, P1.c, c, P2.M, P1.M, static_cast<float>(M)) > MDIP;
+    tr = tr || trm_;
+  }
+  const unsigned trm = __ballot_sync(FULL, tr), mmode = __ballot_sync(FULL, trm_);
+  unsigned events = scm | trm;
+  while (events && st.nbr < K) {
+    const int i = __ffs(events) - 1;
+    events &= events - 1;
+    if ((scm >> i) & 1u) {
+      if (lane == i) put_bracket(x.slot, st.nbr, cl, c, exl ? Fl : NAN, exact ? F : NAN);
+      ++st.nbr;
+    } else {
+      double x0 = __shfl_sync(FULL, P2.c, i), x1 = __shfl_sync(FULL, P1.c, i);
+      const double x2 = __shfl_sync(FULL, c, i);
+      const double sgn = (__shfl_sync(FULL, P1.seg, i) >> 30) & 1 ? -1. : 1.;
+      double sa = sgn * __shfl_sync(FULL, P2.g, i), ma = __shfl_sync(FULL, P2.M, i);
+      const double sb = sgn * __shfl_sync(FULL, g, i), mb = __shfl_sync(FULL, M, i);
+      if (x0 < st.zoom_right) {  // overlaps the previous window: start at its middle sample
+        x0 = x1;
+        sa = sgn * __shfl_sync(FULL, P1.g, i);
+        ma = __shfl_sync(FULL, P1.M, i);
+      }
+      st.zoom_right = x2;
+      const int mode = (mmode >> i) & 1u;
+      bool dismissed = false;
+      if constexpr (single) {
+        unsigned long long se = 0;
+        dismissed = screen_trough32<WAVE>(view, static_cast<float>(x.w), x0, x2, sa, sb, ma, mb, sgn, mode, lane,
+                                          se);
+        ctr.evals += se;
+        ctr.evals32 += se;
+        ctr.steps += se * x.nsteps;
+        ctr.steps32 += se * x.nsteps;
+      }
+      if (!dismissed) {
+        unsigned long long ze = 0;
+        st.nbr = zoom_trough<WAVE>(view64, x.w, x0, x2, sa, sb, ma, mb, sgn, mode, d.tol, x.slot, st.nbr, K, lane,
+                                   ze);
+        ctr.evals += ze;
+        ctr.steps += ze * x.nsteps;
+        ++ctr.zooms;
+      }
+    }
+  }
+  // ---- carries ----
+  st.nseg += __popc(scm);
+  const int last = nvalid - 1;
+  st.c1 = __shfl_sync(FULL, c, last);
+  st.F1 = __shfl_sync(FULL, F, last);
+  st.bits = (st.bits & ~SS_EX1) | SS_HAVE1 | (__shfl_sync(FULL, exact, last) ? SS_EX1 : 0);
+  if (rmask) {
+    const int h1 = 31 - __clz(rmask);
+    const unsigned rest = rmask & ~(1u << h1);
+    const Sample n1 = shfl_sample(me, h1);
+    const Sample n2 = shfl_sample(me, rest ? 31 - __clz(rest) : 0);
+    if (rest) {
+      st.R2 = n2;
+      st.bits |= SS_HR2;
+    } else {
+      st.R2 = st.R1;
+      st.bits = (st.bits & ~SS_HR2) | ((st.bits & SS_HR1) ? SS_HR2 : 0);
+    }
+    st.R1 = n1;
+    st.bits |= SS_HR1;
+  }
+}
+
+// The end of a trace's scan: the last-cell check and the brackets published
+// for refinement.
+template <class T, int WAVE>
+__device__ __forceinline__ void scan_finish(const Dev &d, const TraceCtx &x, ScanState &st, const LayerView<T> &view,
+                                            const LayerView<double> &view64, int lane, ScanCounters &ctr) {
+  if ((st.bits & SS_FINISHED) && st.nbr < x.K && !(st.tfl & TRACE_SEARCH_UNCONVERGED) && (st.bits & SS_HR1) &&
+      (st.bits & SS_HR2) && st.R2.c < st.R1.c && st.zoom_right <= st.R2.c &&
+      sample_segment(st.R1) == sample_segment(st.R2))
+    st.nbr = last_cell<T, WAVE>(view, view64, x.w, st.R2, st.R1, d.tol, x.slot, st.nbr, x.K, lane, x.nsteps,
+                                ctr.evals, ctr.evals32, ctr.steps, ctr.steps32, ctr.zooms);
+  if (lane == 0) {
+    d.nbr[x.t] = st.nbr;
+    if (st.tfl) atomicOr(&d.tflags[x.t], st.tfl);
+  }
+  if (!(st.tfl & TRACE_SEARCH_UNCONVERGED)) {
+    int base = 0;
+    if (lane == 0) base = atomicAdd(&d.ctr[C_NREFINE], st.nbr);
+    base = __shfl_sync(FULL, base, 0);
+    for (int i = lane; i < st.nbr; i += 32) d.refine_list[base + i] = x.t * d.KB + i;
+  }
+  __syncwarp();
+}
+
+__device__ __forceinline__ void scan_counters_flush(const Dev &d, const ScanCounters &ctr, int lane) {
+  if (lane == 0 && d.stats) {
+    if (ctr.evals) atomicAdd(&d.stats[0], ctr.evals);
+    if (ctr.steps) atomicAdd(&d.stats[2], ctr.steps);
+    if (ctr.evals32) atomicAdd(&d.stats[1], ctr.evals32);
+    if (ctr.steps32) atomicAdd(&d.stats[3], ctr.steps32);
+    if (ctr.zooms) atomicAdd(&d.stats[5], ctr.zooms);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// scan<T, WAVE>: the fused persistent kernel, one warp per trace.
+// Shared memory per warp: EVAL_ROWS * Ls values of T (model table) + 32 doubles
+// (merge buffer).
+// ---------------------------------------------------------------------------
 template <class T, int WAVE>
 __global__ void __launch_bounds__(128, MD200_SCAN_MIN_BLOCKS) scan(Dev d, const int *list, int cursor_id, int count_id) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -799,25 +1100,19 @@ __global__ void __launch_bounds__(128, MD200_SCAN_MIN_BLOCKS) scan(Dev d, const 
   unsigned char *mine = smem_raw + static_cast<size_t>(wib) * (tab_bytes + 32 * sizeof(double));
   T *tab = reinterpret_cast<T *>(mine);
   double *mbuf = reinterpret_cast<double *>(mine + tab_bytes);
-  unsigned long long evals = 0, evals32 = 0, steps = 0, steps32 = 0, zooms = 0;
-  const double density = d.density, step = 1. / density;
+  ScanCounters ctr;
+  const double step = 1. / d.density;
   constexpr bool single = sizeof(T) == 4;
-  const unsigned lt = lanemask_lt(), le = lt | (1u << lane);
 
   for (;;) {
     int q = 0;
     if (lane == 0) q = atomicAdd(&d.ctr[cursor_id], 1);
     q = __shfl_sync(FULL, q, 0);
     if (q >= *(volatile int *)&d.ctr[count_id]) break;
-    const int t = list[q];
-    const int b = d.tr_model[t];
-    const int K = d.tr_modes[t] + 2;  // nmodes + 2 guard roots
-    const double period = d.tr_period[t];
-    const double w = TWO_PI / period, fr = 1. / period;
-    const int L = d.mL[b], water = d.mwater[b];
+    const TraceCtx x = trace_ctx(d, list[q]);
     // stage the model's recurrence rows (16-byte cp.async, coalesced)
     {
-      const T *src = layer_table<T>(d, b);
+      const T *src = layer_table<T>(d, x.b);
       const int n16 = static_cast<int>((static_cast<size_t>(EVAL_ROWS) * d.Ls * sizeof(T)) / 16);
       for (int i = lane; i < n16; i += 32)
         cp_async16(reinterpret_cast<unsigned char *>(tab) + 16 * i,
@@ -825,280 +1120,53 @@ __global__ void __launch_bounds__(128, MD200_SCAN_MIN_BLOCKS) scan(Dev d, const 
       cp_async_wait_all();
       __syncwarp();
     }
-    const LayerView<T> view = make_view<T>(tab, d.Ls, L, water);
+    const LayerView<T> view = make_view<T>(tab, d.Ls, d.mL[x.b], d.mwater[x.b]);
     // FP64 view for zooms and FP64 samples of the single-precision scan (global
     // memory, L1/L2-resident); the FP64 scan reads its shared-memory copy
     LayerView<double> view64;
-    if constexpr (single) view64 = global_view(d, b);
+    if constexpr (single) view64 = global_view(d, x.b);
     else view64 = *reinterpret_cast<const LayerView<double> *>(&view);
-    const int nsteps = layer_steps(L, water);
-    const double4 *kt = d.knot + static_cast<size_t>(b) * d.nkmax;
-    const int nk = d.nknot[b];
-    const double alpha = d.malpha[b];
-    const double u_lo = fma(fr, kt[0].y, alpha * kt[0].z);
-    const double u_hi = fma(fr, kt[nk - 1].y, alpha * kt[nk - 1].z);
-    long long J = static_cast<long long>(ceil((u_hi - u_lo) * density)) - 1;
-    unsigned tfl = 0;
-    if (J < 0) J = 0;
-    if (J > JMAX) {
-      J = JMAX;
-      tfl |= TRACE_WORKSPACE_LIMIT;
-    }
-    const double *sd = d.seed + static_cast<size_t>(b) * d.nsmax;
-    const int ns = d.nseed[b];
-    const double hi = d.mhi[b];
-    double *slot = d.slot + static_cast<size_t>(t) * d.KB * SLOT;
-    const double4 *tail = d.tail + 2 * static_cast<size_t>(t);
-
-    long long gi = 1;
+    ScanState st = scan_start(d, x);
     int kfrom = 0;  // this lane's knot interval (scan_point)
-    int si = 0, nbr = 0, nseg = 0;
-    // carries: the last element (for bracketing) and the last two regular elements
-    bool have1 = false, hr1 = false, hr2 = false, ex1 = false;
-    double c1 = 0., F1 = 0.;
-    Sample R1{0., 0.f, 0.f, 0}, R2{0., 0.f, 0.f, 0};
-    double zoom_right = -INFINITY;  // right end of the last zoomed window (windows never overlap)
-    // one 32-sample step per iteration (S > 1 interleaves S independent
-    // recurrences per lane; measured slower on B200: instruction-cache bound)
-    constexpr int S = 1;
-    bool finished = false;
-    while (nbr < K && !finished) {
-      // ---- next S x 32 sample positions: merge scan points and seeds ----
-      double cs[S];
-      unsigned vm[S];
-#pragma unroll
-      for (int h = 0; h < S; ++h) {
-        const long long gj = gi + lane;
-        const double gv = gj <= J ? scan_point(kt, nk, fr, alpha, u_lo + static_cast<double>(gj) * step, kfrom)
-                                  : INFINITY;
-        const double sv = si + lane < ns ? sd[si + lane] : INFINITY;
-        const int rg = warp_rank(sv, gv, false);  // seeds strictly below this scan point
-        const int rs = warp_rank(gv, sv, true);   // scan points at or below this seed
-        const int pg = lane + rg, ps = lane + rs;
-        mbuf[lane] = INFINITY;
-        __syncwarp();
-        if (pg < 32) mbuf[pg] = gv;
-        if (ps < 32) mbuf[ps] = sv;
-        __syncwarp();
-        cs[h] = mbuf[lane];
-        __syncwarp();
-        gi += __popc(__ballot_sync(FULL, pg < 32 && gv < INFINITY));
-        si += __popc(__ballot_sync(FULL, ps < 32 && sv < INFINITY));
-        vm[h] = __ballot_sync(FULL, cs[h] < INFINITY);
-      }
-      if (!vm[0]) {
-        finished = true;  // the window is exhausted
+    while (st.nbr < x.K && !(st.bits & SS_FINISHED)) {
+      double c;
+      const unsigned vm = scan_positions(x, st, step, lane, mbuf, kfrom, c);
+      if (!vm) {
+        st.bits |= SS_FINISHED;  // the window is exhausted
         break;
       }
-
-      // ---- secular values, shape features and log-magnitudes ----
-      double Fs[S], gs[S], Ms[S];
-      bool exs[S];
+      const bool valid = c < INFINITY;
+      const int nv = __popc(vm);
+      double F, g, M;
+      bool exact;
       if constexpr (single) {
-        float c32[S], F32[S], g32[S], M32[S];
-        bool near_cut[S];
-#pragma unroll
-        for (int h = 0; h < S; ++h) {
-          const bool valid = cs[h] < INFINITY;
-          // near the half-space cutoff the start vector depends on the small radical
-          // sqrt(k^2 - kb^2) directly, which single precision resolves poorly: those
-          // samples are evaluated in FP64 only, at their exact positions
-          near_cut[h] = valid && cs[h] >= hi * (1. - 1e-4);
-          float x = valid ? static_cast<float>(cs[h]) : 1.f;
-          if (valid && static_cast<double>(x) > hi) x = nextafterf(x, 0.f);
-          if (valid && !near_cut[h]) cs[h] = static_cast<double>(x);
-          c32[h] = x;
-        }
-        scan_eval<float, WAVE, S>(view, static_cast<float>(w), c32, F32, g32, M32);
-#pragma unroll
-        for (int h = 0; h < S; ++h) {
-          const bool valid = cs[h] < INFINITY;
-          const int nv = __popc(vm[h]);
-          Fs[h] = F32[h];
-          gs[h] = g32[h];
-          Ms[h] = M32[h];
-          exs[h] = false;
-          evals += nv;
-          evals32 += nv;
-          steps += static_cast<unsigned long long>(nv) * nsteps;
-          steps32 += static_cast<unsigned long long>(nv) * nsteps;
-          // the near-cutoff band takes the precomputed FP64 values where it can
-          bool have_tail = false;
-          if (near_cut[h]) {
-            const double4 t0 = tail[0], t1 = tail[1];
-            const double4 tv = cs[h] == t0.x ? t0 : t1;
-            if (cs[h] == tv.x && isfinite(tv.y)) {
-              Fs[h] = tv.y;
-              gs[h] = tv.z;
-              Ms[h] = tv.w;
-              exs[h] = true;
-              have_tail = true;
-            }
-          }
-          // sign-uncertain single-precision samples (small |g|) and the rest of the
-          // near-cutoff band are evaluated in FP64 here
-          const bool redo = valid && !have_tail && (!(fabs(gs[h]) > MD200_REDO_G) || near_cut[h]);
-          const unsigned rm = __ballot_sync(FULL, redo);
-          if (rm) {
-            if (redo) {
-              Fs[h] = eval64_outline(view64, WAVE, w, cs[h], &gs[h], &Ms[h]);
-              exs[h] = true;
-            }
-            evals += __popc(rm);
-            steps += static_cast<unsigned long long>(__popc(rm)) * nsteps;
-          }
-        }
+        bool near_cut;
+        const float c32 = scan_position32(c, x.hi, near_cut);
+        float F32, g32, M32;
+        scan_eval<float, WAVE, 1>(view, static_cast<float>(x.w), &c32, &F32, &g32, &M32);
+        F = F32;
+        g = g32;
+        M = M32;
+        ctr.evals += nv;
+        ctr.evals32 += nv;
+        ctr.steps += static_cast<unsigned long long>(nv) * x.nsteps;
+        ctr.steps32 += static_cast<unsigned long long>(nv) * x.nsteps;
+        const bool redo = scan_complete32<WAVE>(view64, x.w, x.tail, c, valid, near_cut, F, g, M, exact);
+        const int nr = __popc(__ballot_sync(FULL, redo));
+        ctr.evals += nr;
+        ctr.steps += static_cast<unsigned long long>(nr) * x.nsteps;
       } else {
-        double c64 = cs[0] < INFINITY ? cs[0] : 1.;
-        scan_eval<double, WAVE, 1>(view, w, &c64, Fs, gs, Ms);
-        exs[0] = true;
-        const int nv = __popc(vm[0]);
-        evals += nv;
-        steps += static_cast<unsigned long long>(nv) * nsteps;
+        double c64 = valid ? c : 1.;
+        scan_eval<double, WAVE, 1>(view, x.w, &c64, &F, &g, &M);
+        exact = true;
+        ctr.evals += nv;
+        ctr.steps += static_cast<unsigned long long>(nv) * x.nsteps;
       }
-
-#pragma unroll
-      for (int h = 0; h < S; ++h) {
-        if (nbr >= K) break;
-        if (!vm[h]) {
-          finished = true;
-          break;
-        }
-        const double c = cs[h], F = Fs[h], g = gs[h], M = Ms[h];
-        const bool exact = exs[h];
-        const bool valid = c < INFINITY;
-        const int nvalid = __popc(vm[h]);
-        if (__any_sync(FULL, valid && !(isfinite(F) && isfinite(g)))) {
-          tfl |= TRACE_NONFINITE | TRACE_SEARCH_UNCONVERGED;
-          finished = true;
-          break;
-        }
-        // ---- sign changes against the immediate left neighbour ----
-        double cl = __shfl_up_sync(FULL, c, 1), Fl = __shfl_up_sync(FULL, F, 1);
-        bool exl = __shfl_up_sync(FULL, exact, 1);
-        const bool vl = lane >= 1 ? lane - 1 < nvalid : have1;
-        if (lane == 0) {
-          cl = c1;
-          Fl = F1;
-          exl = ex1;
-        }
-        const bool sc = valid && vl && (signbit(Fl) != signbit(F));  // +0 counts as positive
-        const unsigned scm = __ballot_sync(FULL, sc);
-        const int myseg = nseg + __popc(scm & le);
-        Sample me{c, static_cast<float>(g), static_cast<float>(M),
-                  myseg | (exact ? (1 << 29) : 0) | (signbit(F) ? (1 << 30) : 0)};
-        // ---- regular samples and their two regular predecessors ----
-        const bool reg = valid && !(vl && c - cl < 1e-6 * c);
-        const unsigned rmask = __ballot_sync(FULL, reg);
-        const unsigned m1 = rmask & lt;
-        const int j1 = m1 ? 31 - __clz(m1) : -1;
-        const unsigned m2 = j1 >= 0 ? (m1 & ~(1u << j1)) : 0u;
-        const int j2 = m2 ? 31 - __clz(m2) : -1;
-        Sample P1 = shfl_sample(me, j1 & 31), P2 = shfl_sample(me, j2 & 31);
-        bool hp1 = j1 >= 0, hp2 = j2 >= 0;
-        if (j1 < 0) {
-          P1 = R1; hp1 = hr1;
-          P2 = R2; hp2 = hr2;
-        } else if (j2 < 0) {
-          P2 = R1; hp2 = hr1;
-        }
-        // ---- same-sign troughs: V-shaped shape-feature minima, log-magnitude dips ----
-        bool tr = false, trm_ = false;
-        if (reg && hp1 && hp2 && sample_segment(P2) == myseg && sample_segment(P1) == myseg) {
-          const double sgn = sample_sign(P1);
-          tr = trough_may_hide_roots(P2.c, P1.c, c, sgn * P2.g, sgn * P1.g, sgn * static_cast<float>(g),
-                                     pair_noise(single, P2, P1), pair_noise(single, P1, me));
-          if (!tr) trm_ = magnitude_dip(P2.c, P1.c, c, P2.M, P1.M, static_cast<float>(M)) > MDIP;
-          tr = tr || trm_;
-        }
-        const unsigned trm = __ballot_sync(FULL, tr), mmode = __ballot_sync(FULL, trm_);
-        unsigned events = scm | trm;
-        while (events && nbr < K) {
-          const int i = __ffs(events) - 1;
-          events &= events - 1;
-          if ((scm >> i) & 1u) {
-            if (lane == i) put_bracket(slot, nbr, cl, c, exl ? Fl : NAN, exact ? F : NAN);
-            ++nbr;
-          } else {
-            double x0 = __shfl_sync(FULL, P2.c, i), x1 = __shfl_sync(FULL, P1.c, i);
-            const double x2 = __shfl_sync(FULL, c, i);
-            const double sgn = (__shfl_sync(FULL, P1.seg, i) >> 30) & 1 ? -1. : 1.;
-            double sa = sgn * __shfl_sync(FULL, P2.g, i), ma = __shfl_sync(FULL, P2.M, i);
-            const double sb = sgn * __shfl_sync(FULL, g, i), mb = __shfl_sync(FULL, M, i);
-            if (x0 < zoom_right) {  // overlaps the previous window: start at its middle sample
-              x0 = x1;
-              sa = sgn * __shfl_sync(FULL, P1.g, i);
-              ma = __shfl_sync(FULL, P1.M, i);
-            }
-            zoom_right = x2;
-            const int mode = (mmode >> i) & 1u;
-            bool dismissed = false;
-            if constexpr (single) {
-              unsigned long long se = 0;
-              dismissed = screen_trough32<WAVE>(view, static_cast<float>(w), x0, x2, sa, sb, ma, mb, sgn, mode,
-                                                lane, se);
-              evals += se;
-              evals32 += se;
-              steps += se * nsteps;
-              steps32 += se * nsteps;
-            }
-            if (!dismissed) {
-              unsigned long long ze = 0;
-              nbr = zoom_trough<WAVE>(view64, w, x0, x2, sa, sb, ma, mb, sgn, mode, d.tol, slot, nbr, K, lane, ze);
-              evals += ze;
-              steps += ze * nsteps;
-              ++zooms;
-            }
-          }
-        }
-        // ---- carries ----
-        nseg += __popc(scm);
-        const int last = nvalid - 1;
-        c1 = __shfl_sync(FULL, c, last);
-        F1 = __shfl_sync(FULL, F, last);
-        ex1 = __shfl_sync(FULL, exact, last);
-        have1 = true;
-        if (rmask) {
-          const int h1 = 31 - __clz(rmask);
-          const unsigned rest = rmask & ~(1u << h1);
-          const Sample n1 = shfl_sample(me, h1);
-          const Sample n2 = shfl_sample(me, rest ? 31 - __clz(rest) : 0);
-          if (rest) {
-            R2 = n2;
-            hr2 = true;
-          } else {
-            R2 = R1;
-            hr2 = hr1;
-          }
-          R1 = n1;
-          hr1 = true;
-        }
-      }
+      scan_bookkeep<T, WAVE>(d, x, st, view, view64, lane, c, F, g, M, exact, vm, ctr);
     }
-    if (finished && nbr < K && !(tfl & TRACE_SEARCH_UNCONVERGED) && hr1 && hr2 && R2.c < R1.c &&
-        zoom_right <= R2.c && sample_segment(R1) == sample_segment(R2))
-      nbr = last_cell<T, WAVE>(view, view64, w, R2, R1, d.tol, slot, nbr, K, lane, nsteps, evals, evals32, steps,
-                               steps32, zooms);
-    // ---- publish brackets ----
-    if (lane == 0) {
-      d.nbr[t] = nbr;
-      if (tfl) atomicOr(&d.tflags[t], tfl);
-    }
-    if (!(tfl & TRACE_SEARCH_UNCONVERGED)) {
-      int base = 0;
-      if (lane == 0) base = atomicAdd(&d.ctr[C_NREFINE], nbr);
-      base = __shfl_sync(FULL, base, 0);
-      for (int i = lane; i < nbr; i += 32) d.refine_list[base + i] = t * d.KB + i;
-    }
-    __syncwarp();
+    scan_finish<T, WAVE>(d, x, st, view, view64, lane, ctr);
   }
-  if (lane == 0 && d.stats) {
-    atomicAdd(&d.stats[0], evals);
-    atomicAdd(&d.stats[2], steps);
-    atomicAdd(&d.stats[1], evals32);
-    atomicAdd(&d.stats[3], steps32);
-    atomicAdd(&d.stats[5], zooms);
-  }
+  scan_counters_flush(d, ctr, lane);
 }
 
 // Brent-Dekker bracketed refinement to the reference's stopping width
