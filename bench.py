@@ -64,6 +64,7 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-jacobian", action="store_true")
     p.add_argument("--no-ragged", action="store_true")
+    p.add_argument("--no-config3", action="store_true")
     return p.parse_args()
 
 
@@ -150,7 +151,7 @@ def cpu_baseline(batch, periods, nmodes, sample):
                                      wave=wave, tol=TOL, threads=threads, group_velocity=True)
         elapsed += time.perf_counter() - t
         roots += int(np.isfinite(out["phase_velocity"]).sum())
-    return {"value": roots / elapsed, "unit": "roots/s", "cores": threads, "kind": "reference",
+    return {"value": roots / elapsed, "unit": "roots/s", "cores": threads, "kind": "reference", "seconds": elapsed,
             "sample": f"{sample} models of the same batch x 60 periods x 5 modes, Rayleigh+Love, group velocity, "
                       f"accuracy=high shape-adaptive, c_tol_rel={TOL:g}; {roots} roots in {elapsed:.2f} s"}
 
@@ -160,7 +161,7 @@ def run_reference(args, rank, world):
         return
     batch, periods, nmodes = workload(0, args.models)
     sample = args.cpu_sample
-    vals = []
+    vals, times = [], []
     for step in range(args.warmup + args.steps):
         res = cpu_baseline(batch, periods, nmodes, sample)
         if res is None:
@@ -168,9 +169,10 @@ def run_reference(args, rank, world):
             return
         if step >= args.warmup:
             vals.append(res["value"])
+            times.append(res["seconds"])
     value = statistics.median(vals)
     line = {"metric": METRIC, "value": value, "unit": "roots/s", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": 1e3 * statistics.median(times), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "impl": "reference",
             "config": {"workload": WORKLOAD, "models_per_step": sample, "periods": 60, "nmodes": 5,
                        "c_tol_rel": TOL},
@@ -250,6 +252,76 @@ def jacobian_bench(torch, local, steps, warmup, flush):
 
 
 RAGGED_MODELS = 10_000
+
+
+def config3_bench(torch, local, flush, sample=256, rank=0):
+    """Mixed precision on the 100,000-model batch with 30 % low-velocity-layer models:
+    FP32-scan throughput (one timed step, both waves), agreement of the FP32-scan and
+    plain FP64 engines over the whole batch, and per-root error of the FP32-scan
+    engine against the reference CPU engine on a sample of the batch."""
+    from modisp_b200 import _native, workloads
+    import oracle
+    batch, periods, nmodes = workloads.config3()
+    B, L = batch["thickness"].shape
+    T = periods.size
+    dev = torch.device("cuda", local)
+    x = {k: torch.tensor(batch[k], device=dev) for k in ("thickness", "vp", "vs", "rho")}
+    per = torch.tensor(periods, device=dev)
+    out = {}
+    ms = 0.
+    for single in (1, 0):
+        o = _native.default_options()
+        o.single_precision = single
+        o.group_velocity = 1
+        eng = _native.Engine(local, B, L, T, nmodes, o)
+        stream = torch.cuda.current_stream().cuda_stream
+        for wave in (0, 1):
+            vel = torch.empty((B, nmodes, T), dtype=torch.float64, device=dev)
+            grp = torch.empty_like(vel)
+            gfl = torch.empty((B, nmodes, T), dtype=torch.int32, device=dev)
+            tr = [torch.empty((B, T), dtype=torch.int32, device=dev) for _ in range(3)]
+            args = (x["thickness"].data_ptr(), x["vp"].data_ptr(), x["vs"].data_ptr(), x["rho"].data_ptr(), B,
+                    per.data_ptr(), 0, TOL, 1., wave, vel.data_ptr(), tr[0].data_ptr(), tr[1].data_ptr(),
+                    tr[2].data_ptr(), grp.data_ptr(), gfl.data_ptr())
+            eng.run_device(*args, stream=stream)  # warm-up
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            eng.run_device(*args, stream=stream)
+            b.record()
+            b.synchronize()
+            if single:
+                ms += a.elapsed_time(b)
+            out[single, wave] = (vel.cpu().numpy(), grp.cpu().numpy(), tr[2].cpu().numpy())
+        eng.close()
+    roots = sum(int(np.isfinite(out[1, w][0]).sum()) for w in (0, 1))
+    agree = {"mask_mismatch_traces": 0, "count_mismatches": 0, "max_rel_diff_phase": 0., "max_rel_diff_group": 0.}
+    for w in (0, 1):
+        v32, g32, c32 = out[1, w]
+        v64, g64, c64 = out[0, w]
+        agree["mask_mismatch_traces"] += int(np.any(np.isfinite(v32) != np.isfinite(v64), axis=1).sum())
+        agree["count_mismatches"] += int((c32 != c64).sum())
+        m = np.isfinite(v32) & np.isfinite(v64)
+        agree["max_rel_diff_phase"] = max(agree["max_rel_diff_phase"], float((np.abs(v32[m] - v64[m]) / v64[m]).max()))
+        mg = np.isfinite(g32) & np.isfinite(g64)
+        agree["max_rel_diff_group"] = max(agree["max_rel_diff_group"], float((np.abs(g32[mg] - g64[mg]) / g64[mg]).max()))
+    vs_ref = None
+    if rank == 0 and oracle.reference() is not None:
+        threads = len(os.sched_getaffinity(0))
+        idx = np.linspace(0, B - 1, sample).astype(int)
+        vs_ref = {"sample_models": sample, "mask_mismatch_traces": 0, "count_mismatches": 0, "max_rel_err_phase": 0.}
+        for w in (0, 1):
+            ref = oracle.reference_solve(*(batch[k][idx] for k in ("thickness", "vp", "vs", "rho")), periods, nmodes,
+                                         wave=w, tol=1e-12, threads=threads)
+            v, rv = out[1, w][0][idx], ref["phase_velocity"]
+            vs_ref["mask_mismatch_traces"] += int(np.any(np.isfinite(v) != np.isfinite(rv), axis=1).sum())
+            vs_ref["count_mismatches"] += int((out[1, w][2][idx] != ref["root_count"]).sum())
+            m = np.isfinite(v) & np.isfinite(rv)
+            vs_ref["max_rel_err_phase"] = max(vs_ref["max_rel_err_phase"], float((np.abs(v[m] - rv[m]) / rv[m]).max()))
+    return {"workload": "100,000 models as the crustal batch, 30 % with one low-velocity layer (Vs 20-40 % below "
+                        "the layer above), 60 periods 0.5-50 s, 5 modes, Rayleigh + Love, FP32 scan / FP64 refinement",
+            "value": roots / (ms * 1e-3), "unit": "roots/s", "ms_per_step": ms, "roots_per_step": roots,
+            "fp32_vs_fp64_engine": agree, "fp32_vs_reference": vs_ref}
 
 
 def ragged_bench(torch, local, steps, warmup, flush, models=RAGGED_MODELS):
@@ -463,6 +535,7 @@ def main():
 
     jac = jacobian_bench(torch, local, max(2, args.steps // 2), 2, flush) if not args.no_jacobian else None
     ragged = ragged_bench(torch, local, max(2, args.steps // 2), 2, flush) if not args.no_ragged else None
+    config3 = config3_bench(torch, local, flush, rank=rank) if not args.no_config3 else None
 
     peak32 = _native.measure_peak(local, fp64=False)
     peak64 = _native.measure_peak(local, fp64=True)
@@ -499,6 +572,7 @@ def main():
             "engine_stats": {"rayleigh": e32_stats[0], "love": e32_stats[1]},
             "jacobian": jac,
             "ragged": ragged,
+            "config3": config3,
         }
         print(json.dumps(line))
     if world > 1:

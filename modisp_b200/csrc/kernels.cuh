@@ -1169,58 +1169,127 @@ __global__ void __launch_bounds__(128, MD200_SCAN_MIN_BLOCKS) scan(Dev d, const 
   scan_counters_flush(d, ctr, lane);
 }
 
-// Brent-Dekker bracketed refinement to the reference's stopping width
-// max(16 eps |x|, min(w/64, tol |x| / 8)) (cpp/common/refinement.hpp:341-396).
-__device__ double brent(const LayerView<double> &m, int wave, double w, double a, double b,
-                        double fa, double fb, double tol, int *evaluations) {
-  if (a == b) return fa == 0. ? a : NAN;
-  if (!isfinite(fa) || !isfinite(fb) || ((fa < 0.) == (fb < 0.) && fa != 0. && fb != 0.)) return NAN;
-  if (fa == 0.) return a;
-  if (fb == 0.) return b;
-  const double big = fmax(fabs(a), fabs(b));
-  const double stop = fmax(16. * 2.220446049250313e-16 * big, fmin((b - a) / 64., .125 * tol * big));
-  double c = b, fc = fb, dd = b - a, e = dd;
-  for (int it = 0; it < 160; ++it) {
-    if ((fb < 0.) == (fc < 0.)) {
-      c = a;
-      fc = fa;
-      e = dd = b - a;
-    }
-    if (fabs(fc) < fabs(fb)) {
-      a = b; fa = fb;
-      b = c; fb = fc;
-      c = a; fc = fa;
-    }
-    if (fb == 0.) return b;
-    const double mid = .5 * (c - b), half = .5 * stop;
-    if (fabs(c - b) <= stop) return .5 * (b + c);
-    if (fabs(e) >= half && fabs(fa) > fabs(fb)) {
-      const double s = fb / fa;
-      double p, q;
-      if (a == c) {
-        p = 2. * mid * s;
-        q = 1. - s;
-      } else {
-        const double qa = fa / fc, r = fb / fc;
-        p = s * (2. * mid * qa * (qa - r) - (b - a) * (r - 1.));
-        q = (qa - 1.) * (r - 1.) * (s - 1.);
-      }
-      if (p > 0.) q = -q; else p = -p;
-      const double old = e;
-      e = dd;
-      const double ratio = p / q;
-      if (isfinite(ratio) && 2. * p < fmin(3. * mid * q - fabs(half * q), fabs(old * q))) dd = ratio;
-      else { dd = mid; e = mid; }
+// One refinement sample.  F is the secular value as the recurrence returns it,
+// renormalised by a power of two at every layer; (g, l) stands for g 2^l, with
+// g the shape feature F / |e| and l the base-2 log-magnitude of the
+// unnormalised vector less the evanescent factor exp(sum r h) -- together the
+// function on one smooth scale.  Near a root where the whole vector vanishes (a
+// mode trapped under an evanescent layer) the renormalisation rescales F by its
+// own magnitude: F turns step-like (about +-0.4 on either side of the root),
+// interpolation on it fails and the bracket closes by bisection to a midpoint.
+// Ratios of two samples are therefore taken on the g 2^l scale; bracket ends
+// carried over from the scan have no l (NaN), and ratios involving them use F.
+struct RootSample {
+  double F, g, l;
+};
+__device__ __forceinline__ double sample_ratio(const RootSample &x, const RootSample &y) {
+  const double dl = x.l - y.l;
+  return isnan(dl) ? x.F / y.F : (x.g / y.g) * exp2(dl);
+}
+__device__ __forceinline__ RootSample root_sample(const LayerView<double> &m, int wave, double w, double c) {
+  RootSample r;
+  double lev;
+  r.F = secular<double, double>(m, wave, w / c, w, &r.g, &r.l, &lev);
+  r.l -= lev;
+  return r;
+}
+
+// Refinement of one bracket [a, b] to the reference's stopping width
+// max(16 eps |x|, min(w/64, tol |x| / 8)) by Brent-Dekker
+// (cpp/common/refinement.hpp:341-396) on RootSamples.  End values unknown in
+// FP64 (NaN: brackets of the FP32 scan) are evaluated first, through the one
+// evaluation site the iterations use, so that lanes confirming ends and lanes
+// iterating run one instruction stream.  Returns the root; NaN with
+// *no_bracket set when the confirmed ends have one sign; NaN alone when
+// refinement failed.
+__device__ double refine_bracket(const LayerView<double> &m, int wave, double w, double a, double b, double fa,
+                                 double fb, double tol, int *evaluations, bool *no_bracket) {
+  *no_bracket = false;
+  RootSample sa{fa, fa, NAN}, sb{fb, fb, NAN}, sc{0., 0., NAN};
+  int pending = (isfinite(fa) ? 0 : 1) | (isfinite(fb) ? 0 : 2);
+  const bool confirm = pending != 0;
+  bool started = false;
+  double c = b, dd = 0., e = 0., stop = 0.;
+  for (int it = 0; it < 162; ++it) {
+    double x;
+    if (pending) {
+      x = (pending & 1) ? a : b;
     } else {
-      dd = mid;
-      e = mid;
+      if (!started) {
+        started = true;
+        if (confirm && signbit(sa.F) == signbit(sb.F)) {
+          *no_bracket = true;
+          return NAN;
+        }
+        if (a == b) return sa.F == 0. ? a : NAN;
+        if (!isfinite(sa.F) || !isfinite(sb.F) || ((sa.F < 0.) == (sb.F < 0.) && sa.F != 0. && sb.F != 0.))
+          return NAN;
+        if (sa.F == 0.) return a;
+        if (sb.F == 0.) return b;
+        const double big = fmax(fabs(a), fabs(b));
+        stop = fmax(16. * 2.220446049250313e-16 * big, fmin((b - a) / 64., .125 * tol * big));
+        c = b;
+        sc = sb;
+        dd = e = b - a;
+      }
+      if ((sb.F < 0.) == (sc.F < 0.)) {
+        c = a;
+        sc = sa;
+        e = dd = b - a;
+      }
+      if (fabs(sample_ratio(sc, sb)) < 1.) {  // |f(c)| < |f(b)|
+        a = b; sa = sb;
+        b = c; sb = sc;
+        c = a; sc = sa;
+      }
+      if (sb.F == 0.) return b;
+      const double mid = .5 * (c - b), half = .5 * stop;
+      if (fabs(c - b) <= stop) {
+        // converged bracket [b, c], f(b) and f(c) of opposite signs: its secant
+        // point is second order in the width and needs no evaluation (group
+        // velocities of some roots move by 1e-7 per 1e-11 of root error, so the
+        // midpoint's error of up to stop / 2 would show in them)
+        const double s = b - (c - b) / (sample_ratio(sc, sb) - 1.);
+        return (isfinite(s) && (s - b) * (s - c) <= 0.) ? s : .5 * (b + c);
+      }
+      if (fabs(e) >= half && fabs(sample_ratio(sa, sb)) > 1.) {
+        const double s = sample_ratio(sb, sa);
+        double p, q;
+        if (a == c) {
+          p = 2. * mid * s;
+          q = 1. - s;
+        } else {
+          const double qa = sample_ratio(sa, sc), r = sample_ratio(sb, sc);
+          p = s * (2. * mid * qa * (qa - r) - (b - a) * (r - 1.));
+          q = (qa - 1.) * (r - 1.) * (s - 1.);
+        }
+        if (p > 0.) q = -q; else p = -p;
+        const double old = e;
+        e = dd;
+        const double ratio = p / q;
+        if (isfinite(ratio) && 2. * p < fmin(3. * mid * q - fabs(half * q), fabs(old * q))) dd = ratio;
+        else { dd = mid; e = mid; }
+      } else {
+        dd = mid;
+        e = mid;
+      }
+      a = b;
+      sa = sb;
+      b += fabs(dd) > half ? dd : (mid > 0. ? half : -half);
+      x = b;
     }
-    a = b;
-    fa = fb;
-    b += fabs(dd) > half ? dd : (mid > 0. ? half : -half);
-    fb = eval64(m, wave, w, b, nullptr);
+    const RootSample smp = root_sample(m, wave, w, x);  // the one evaluation site
     ++*evaluations;
-    if (!isfinite(fb)) return NAN;
+    if (pending & 1) {
+      sa = smp;
+      pending &= ~1;
+    } else if (pending & 2) {
+      sb = smp;
+      pending &= ~2;
+    } else {
+      sb = smp;
+      if (!isfinite(sb.F)) return NAN;
+    }
   }
   return NAN;
 }
@@ -1228,7 +1297,7 @@ __device__ double brent(const LayerView<double> &m, int wave, double w, double a
 // ---------------------------------------------------------------------------
 // refine: one thread per bracket.
 // ---------------------------------------------------------------------------
-__global__ void refine(Dev d) {
+__global__ void __launch_bounds__(128, 4) refine(Dev d) {
   const int begin = d.ctr[C_REFINE_BEGIN];
   unsigned long long evals = 0, steps = 0, count = 0;
   for (int i = begin + blockIdx.x * blockDim.x + threadIdx.x; i < *(volatile int *)&d.ctr[C_NREFINE];
@@ -1239,25 +1308,17 @@ __global__ void refine(Dev d) {
     const LayerView<double> m = global_view(d, b);
     const double w = TWO_PI / d.tr_period[t];
     double *sl = d.slot + static_cast<size_t>(id) * SLOT;
-    const double lo = sl[0], hi = sl[1];
-    double flo = sl[2], fhi = sl[3];
     int ev = 0;
-    if (!(isfinite(flo) && isfinite(fhi))) {  // FP32 scan bracket: confirm in FP64
-      if (!isfinite(flo)) { flo = eval64(m, d.wave, w, lo, nullptr); ++ev; }
-      if (!isfinite(fhi)) { fhi = eval64(m, d.wave, w, hi, nullptr); ++ev; }
-      if (signbit(flo) == signbit(fhi)) {
-        atomicOr(&d.tflags[t], INTERNAL_REPAIR);
-        sl[4] = NAN;
-        evals += ev;
-        steps += static_cast<unsigned long long>(ev) * layer_steps(m.L, m.water);
-        continue;
-      }
-    }
-    const double r = brent(m, d.wave, w, lo, hi, flo, fhi, d.tol, &ev);
-    sl[4] = r;
-    if (!isfinite(r)) atomicOr(&d.tflags[t], TRACE_REFINEMENT_FAILED);
+    bool no_bracket;
+    const double r = refine_bracket(m, d.wave, w, sl[0], sl[1], sl[2], sl[3], d.tol, &ev, &no_bracket);
     evals += ev;
     steps += static_cast<unsigned long long>(ev) * layer_steps(m.L, m.water);
+    sl[4] = r;
+    if (no_bracket) {  // the FP32 scan's sign change does not hold in FP64
+      atomicOr(&d.tflags[t], INTERNAL_REPAIR);
+      continue;
+    }
+    if (!isfinite(r)) atomicOr(&d.tflags[t], TRACE_REFINEMENT_FAILED);
     ++count;
   }
   if (d.stats && (evals || count)) {

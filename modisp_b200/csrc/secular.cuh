@@ -380,9 +380,50 @@ struct RayleighEntries {
 // and the return value is r h (value part), the exponent factored out; at
 // k = kv the limits 1, h, 0.  r = sqrt((k + kv)|k - kv|).  scale is 1 unless
 // evanescent.
+//
+// Near k = kv derivative-carrying numbers take the power series in
+// y = (k^2 - kv^2) h^2 instead, unscaled and without the square root:
+//   cs = C(y), sr = h S(y), rs = (k^2 - kv^2) h S(y),
+//   C(y) = sum y^n / (2n)!, S(y) = sum y^n / (2n+1)!
+// (cos and sin for y < 0, cosh and sinh for y > 0).  The direct form takes
+// sin(r h) / r through r = sqrt(|k^2 - kv^2|), and the two terms of its
+// derivative cancel to a relative error of about eps / (r h)^2: for a root 1e-8
+// below a layer's velocity that moved group velocities by 1e-6.  Plain numbers
+// (values) keep the direct forms, so root sets are unaffected.  Truncation after
+// y^5 leaves < 1e-20 relative error for |y| < WAVE_SERIES_Y.
+constexpr double WAVE_SERIES_Y = 1e-2;
+
+template <class N, class T>
+MD200_FN bool wave_series(const N &k, const N &kv, T h, N *cs, N *sr, N *rs) {
+  using BT = typename Base<N>::type;
+  const N D = (k + kv) * (k - kv);
+  const N y = (D * h) * h;
+  const BT yv = val(y);
+  if (!(yv < BT(WAVE_SERIES_Y) && yv > -BT(WAVE_SERIES_Y))) return false;
+  N C = y * BT(1. / 3628800.) + BT(1. / 40320.);  // 1/10!, 1/8!
+  C = C * y + BT(1. / 720.);
+  C = C * y + BT(1. / 24.);
+  C = C * y + BT(0.5);
+  *cs = C * y + BT(1);
+  N S = y * BT(1. / 39916800.) + BT(1. / 362880.);  // 1/11!, 1/9!
+  S = S * y + BT(1. / 5040.);
+  S = S * y + BT(1. / 120.);
+  S = S * y + BT(1. / 6.);
+  S = S * y + BT(1);
+  *sr = S * h;
+  *rs = (D * S) * h;
+  return true;
+}
+
 template <class N, class T>
 MD200_FN typename Base<N>::type wave_block(const N &k, const N &kv, T h, N *cs, N *sr, N *rs, N *scale) {
   using BT = typename Base<N>::type;
+  if constexpr (IsDual<N>::value) {
+    if (wave_series<N, T>(k, kv, h, cs, sr, rs)) {
+      *scale = lift_one<N>();
+      return BT(0);
+    }
+  }
   N r, ir;
   radical(k, kv, &r, &ir);
   *scale = lift_one<N>();
@@ -613,6 +654,10 @@ template <class N, class T>
 MD200_FN void water_top(const N &k, const N &w, T h0, T ivp0, N *cp, N *wv) {
   using B = typename Base<N>::type;
   const N ka = w * ivp0;
+  if constexpr (IsDual<N>::value) {
+    N rs;
+    if (wave_series<N, T>(k, ka, h0, cp, wv, &rs)) return;
+  }
   N rf, irf;
   radical(k, ka, &rf, &irf);
   if (val(k) < val(ka)) {
@@ -656,10 +701,11 @@ MD200_FN void rayleigh_start(N e[5], const N &k, const N &k2, const N &w, const 
 // With `lmag`, also the base-2 logarithm of the magnitude |e| of the
 // unnormalised vector: it is smooth across ordinary roots and dips
 // logarithmically where the whole vector nearly vanishes, the signature of a
-// close root pair.
+// close root pair.  With `levan`, the part of that logarithm the evanescent
+// scaling factored out (base 2 of exp(sum r h)).
 template <class N, class T, int S>
 MD200_FN void rayleigh_multi(const LayerView<T> &m, const N *k, const N &w, N *F, N *shape,
-                             typename Base<N>::type *lmag) {
+                             typename Base<N>::type *lmag, typename Base<N>::type *levan = nullptr) {
   using B = typename Base<N>::type;
   const B tiny = sizeof(B) == 4 ? B(1e-30) : B(1e-40);
   const N iw = lift_one<N>() / w;
@@ -711,6 +757,7 @@ MD200_FN void rayleigh_multi(const LayerView<T> &m, const N *k, const N &w, N *F
 #pragma unroll
   for (int s = 0; s < S; ++s) {
     if (lmag) lmag[s] = static_cast<B>(ex[s]) + ev[s] * B(1.4426950408889634);
+    if (levan) levan[s] = ev[s] * B(1.4426950408889634);
     if (m.water) {
       N cp, wv;
       water_top<N, T>(k[s], w, m.h(0), m.ivp(0), &cp, &wv);
@@ -733,9 +780,9 @@ MD200_FN void rayleigh_multi(const LayerView<T> &m, const N *k, const N &w, N *F
 
 template <class N, class T>
 MD200_FN N rayleigh_secular(const LayerView<T> &m, const N &k, const N &w, N *shape,
-                            typename Base<N>::type *lmag = nullptr) {
+                            typename Base<N>::type *lmag = nullptr, typename Base<N>::type *levan = nullptr) {
   N F;
-  rayleigh_multi<N, T, 1>(m, &k, w, &F, shape, lmag);
+  rayleigh_multi<N, T, 1>(m, &k, w, &F, shape, lmag, levan);
   return F;
 }
 
@@ -751,7 +798,7 @@ MD200_FN typename Base<N>::type love_entries(const N &k, const N &kj, T h, N *cq
 // Love secular values (SH propagator) and shape features of S samples.
 template <class N, class T, int S>
 MD200_FN void love_multi(const LayerView<T> &m, const N *k, const N &w, N *F, N *shape,
-                         typename Base<N>::type *lmag) {
+                         typename Base<N>::type *lmag, typename Base<N>::type *levan = nullptr) {
   using B = typename Base<N>::type;
   const B tiny = sizeof(B) == 4 ? B(1e-30) : B(1e-40);
   const int last = m.L - 1;
@@ -804,15 +851,16 @@ MD200_FN void love_multi(const LayerView<T> &m, const N *k, const N &w, N *F, N 
     if (shape) shape[s] = e[s][0] * m_rsqrt(norm2 + lift_one<N>() * tiny);
     if (lmag)
       lmag[s] = static_cast<B>(ex[s]) + ev[s] * B(1.4426950408889634) + B(0.5) * m_log2(val(norm2) + tiny);
+    if (levan) levan[s] = ev[s] * B(1.4426950408889634);
     F[s] = e[s][0];
   }
 }
 
 template <class N, class T>
 MD200_FN N love_secular(const LayerView<T> &m, const N &k, const N &w, N *shape,
-                        typename Base<N>::type *lmag = nullptr) {
+                        typename Base<N>::type *lmag = nullptr, typename Base<N>::type *levan = nullptr) {
   N F;
-  love_multi<N, T, 1>(m, &k, w, &F, shape, lmag);
+  love_multi<N, T, 1>(m, &k, w, &F, shape, lmag, levan);
   return F;
 }
 
@@ -826,8 +874,8 @@ MD200_FN void secular_multi(const LayerView<T> &m, const N *k, const N &w, N *F,
 
 template <class N, class T>
 MD200_FN N secular(const LayerView<T> &m, int wave, const N &k, const N &w, N *shape,
-                   typename Base<N>::type *lmag = nullptr) {
-  return wave ? love_secular<N, T>(m, k, w, shape, lmag) : rayleigh_secular<N, T>(m, k, w, shape, lmag);
+                   typename Base<N>::type *lmag = nullptr, typename Base<N>::type *levan = nullptr) {
+  return wave ? love_secular<N, T>(m, k, w, shape, lmag, levan) : rayleigh_secular<N, T>(m, k, w, shape, lmag, levan);
 }
 
 }  // namespace md200

@@ -474,6 +474,30 @@ static cld cx_root_term(cld k, cld kb) { /* (k + kb) * |k - kb| with a real-part
   return creall(k) >= creall(kb) ? (k + kb) * (k - kb) : (k + kb) * (kb - k);
 }
 
+/* Near k = kv the wave blocks are taken as power series in y = (k^2 - kv^2) h^2,
+ * unscaled and without the square root: cs = C(y), sr = h S(y),
+ * rs = (k^2 - kv^2) h S(y), C = sum y^n / (2n)!, S = sum y^n / (2n+1)!
+ * (cos / sin for y < 0, cosh / sinh for y > 0).  The direct form's complex-step
+ * derivative of sin(r h) / r cancels to a relative error of about
+ * eps / (r h)^2; the series has no such cancellation.  Terms up to y^8 leave
+ * < 1e-28 relative truncation error for |y| < 1e-2. */
+static int cx_series(cld k, cld kv, cld h, cld *cs, cld *sr, cld *rs) {
+  const cld D = (k + kv) * (k - kv), y = D * h * h;
+  if (!(fabsl(creall(y)) < 1e-2L)) return 0;
+  long double inv_fact[18];
+  inv_fact[0] = 1.L;
+  for (int n = 1; n < 18; ++n) inv_fact[n] = inv_fact[n - 1] / (long double)n;
+  cld C = 0.L, S = 0.L;
+  for (int n = 8; n >= 0; --n) {
+    C = C * y + inv_fact[2 * n];
+    S = S * y + inv_fact[2 * n + 1];
+  }
+  *cs = C;
+  *sr = S * h;
+  *rs = D * S * h;
+  return 1;
+}
+
 static cld cx_rayleigh(const cld *d, const cld *a, const cld *b, const cld *rho, int L,
                        cld wvno, cld omega) {
   const cld wvno2 = wvno * wvno;
@@ -499,7 +523,8 @@ static cld cx_rayleigh(const cld *d, const cld *a, const cld *b, const cld *rho,
     rb = csqrtl(cx_root_term(wvno, xkb));
     const cld dp = d[m], p = ra * dp, q = rb * dp;
     cld cosp, w, x, cosq, y, z, pex = 0.L, sex = 0.L;
-    if (creall(wvno) < creall(xka)) {
+    if (cx_series(wvno, xka, dp, &cosp, &w, &x)) {
+    } else if (creall(wvno) < creall(xka)) {
       const cld sp = csinl(p);
       cosp = ccosl(p);
       w = sp / ra;
@@ -514,7 +539,8 @@ static cld cx_rayleigh(const cld *d, const cld *a, const cld *b, const cld *rho,
       w = sp / ra;
       x = ra * sp;
     }
-    if (creall(wvno) < creall(xkb)) {
+    if (cx_series(wvno, xkb, dp, &cosq, &y, &z)) {
+    } else if (creall(wvno) < creall(xkb)) {
       const cld sq = csinl(q);
       cosq = ccosl(q);
       y = sq / rb;
@@ -578,8 +604,9 @@ static cld cx_rayleigh(const cld *d, const cld *a, const cld *b, const cld *rho,
     const cld ka = omega / a[0];
     const cld rf = csqrtl(cx_root_term(wvno, ka));
     const cld p = rf * d[0];
-    cld cp, w;
-    if (creall(wvno) < creall(ka)) {
+    cld cp, w, unused;
+    if (cx_series(wvno, ka, d[0], &cp, &w, &unused)) {
+    } else if (creall(wvno) < creall(ka)) {
       cp = ccosl(p);
       w = csinl(p) / rf;
     } else if (creall(wvno) == creall(ka)) {
@@ -605,7 +632,8 @@ static cld cx_love(const cld *h, const cld *vs, const cld *rho, int L, cld omega
     const cld mu = rho[j] * vs[j] * vs[j], ka = omega / vs[j];
     const cld r = csqrtl(cx_root_term(k, ka)), q = r * h[j];
     cld cq, y, z;
-    if (creall(k) < creall(ka)) {
+    if (cx_series(k, ka, h[j], &cq, &y, &z)) {
+    } else if (creall(k) < creall(ka)) {
       const cld sn = csinl(q);
       cq = ccosl(q);
       y = sn / r;
