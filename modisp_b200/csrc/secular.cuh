@@ -389,25 +389,27 @@ struct RayleighEntries {
 // sin(r h) / r through r = sqrt(|k^2 - kv^2|), and the two terms of its
 // derivative cancel to a relative error of about eps / (r h)^2: for a root 1e-8
 // below a layer's velocity that moved group velocities by 1e-6.  Plain numbers
-// (values) keep the direct forms, so root sets are unaffected.  Truncation after
-// y^5 leaves < 1e-20 relative error for |y| < WAVE_SERIES_Y.
-constexpr double WAVE_SERIES_Y = 1e-2;
+// (values) keep the direct forms, so root sets are unaffected.  Every dual type
+// takes the same branch (the adjoint Jacobians recompute blocks in several
+// number types, which must agree on the scaling).  The band is narrow because
+// thin layers at long periods have small y at every velocity, and the series
+// costs more than the direct form in the adjoint's nested duals: at
+// |y| = WAVE_SERIES_Y the direct form's cancellation is eps / |y| ~ 2e-12, and
+// truncation after y^3 leaves < 3e-21 relative error inside the band.
+constexpr double WAVE_SERIES_Y = 1e-4;
 
 template <class N, class T>
 MD200_FN bool wave_series(const N &k, const N &kv, T h, N *cs, N *sr, N *rs) {
   using BT = typename Base<N>::type;
+  const BT kk = val(k), kvv = val(kv), hh = val(h);
+  const BT yv = (((kk + kvv) * (kk - kvv)) * hh) * hh;  // the value part of y, decided on first
+  if (!(yv < BT(WAVE_SERIES_Y) && yv > -BT(WAVE_SERIES_Y))) return false;
   const N D = (k + kv) * (k - kv);
   const N y = (D * h) * h;
-  const BT yv = val(y);
-  if (!(yv < BT(WAVE_SERIES_Y) && yv > -BT(WAVE_SERIES_Y))) return false;
-  N C = y * BT(1. / 3628800.) + BT(1. / 40320.);  // 1/10!, 1/8!
-  C = C * y + BT(1. / 720.);
-  C = C * y + BT(1. / 24.);
+  N C = y * BT(1. / 720.) + BT(1. / 24.);  // 1/6!, 1/4!
   C = C * y + BT(0.5);
   *cs = C * y + BT(1);
-  N S = y * BT(1. / 39916800.) + BT(1. / 362880.);  // 1/11!, 1/9!
-  S = S * y + BT(1. / 5040.);
-  S = S * y + BT(1. / 120.);
+  N S = y * BT(1. / 5040.) + BT(1. / 120.);  // 1/7!, 1/5!
   S = S * y + BT(1. / 6.);
   S = S * y + BT(1);
   *sr = S * h;
