@@ -41,7 +41,7 @@ constexpr int LEVEL_FP64 = 20, LEVEL_FP32 = 21, LEVEL_REPAIRED = 22, LEVEL_CONTI
 // Device counters (int) used by the work lists.
 enum Counter {
   C_SCAN_CURSOR = 0, C_NTRACE, C_NREFINE, C_REFINE_BEGIN, C_NGROUP, C_REPAIR_CURSOR, C_NREPAIR,
-  C_JFAIL, C_GROUP_BEGIN, C_NSUSPECT, C_COUNT
+  C_JFAIL, C_GROUP_BEGIN, C_NSUSPECT, C_REFINE_CURSOR, C_COUNT
 };
 
 struct Dev {

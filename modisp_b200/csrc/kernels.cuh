@@ -1196,130 +1196,209 @@ __device__ __forceinline__ RootSample root_sample(const LayerView<double> &m, in
 
 // Refinement of one bracket [a, b] to the reference's stopping width
 // max(16 eps |x|, min(w/64, tol |x| / 8)) by Brent-Dekker
-// (cpp/common/refinement.hpp:341-396) on RootSamples.  End values unknown in
-// FP64 (NaN: brackets of the FP32 scan) are evaluated first, through the one
-// evaluation site the iterations use, so that lanes confirming ends and lanes
-// iterating run one instruction stream.  Returns the root; NaN with
-// *no_bracket set when the confirmed ends have one sign; NaN alone when
-// refinement failed.
-__device__ double refine_bracket(const LayerView<double> &m, int wave, double w, double a, double b, double fa,
-                                 double fb, double tol, int *evaluations, bool *no_bracket) {
-  *no_bracket = false;
-  RootSample sa{fa, fa, NAN}, sb{fb, fb, NAN}, sc{0., 0., NAN};
-  int pending = (isfinite(fa) ? 0 : 1) | (isfinite(fb) ? 0 : 2);
-  const bool confirm = pending != 0;
-  bool started = false;
-  double c = b, dd = 0., e = 0., stop = 0.;
-  for (int it = 0; it < 162; ++it) {
-    double x;
-    if (pending) {
-      x = (pending & 1) ? a : b;
-    } else {
-      if (!started) {
-        started = true;
-        if (confirm && signbit(sa.F) == signbit(sb.F)) {
-          *no_bracket = true;
-          return NAN;
-        }
-        if (a == b) return sa.F == 0. ? a : NAN;
-        if (!isfinite(sa.F) || !isfinite(sb.F) || ((sa.F < 0.) == (sb.F < 0.) && sa.F != 0. && sb.F != 0.))
-          return NAN;
-        if (sa.F == 0.) return a;
-        if (sb.F == 0.) return b;
-        const double big = fmax(fabs(a), fabs(b));
-        stop = fmax(16. * 2.220446049250313e-16 * big, fmin((b - a) / 64., .125 * tol * big));
-        c = b;
-        sc = sb;
-        dd = e = b - a;
-      }
-      if ((sb.F < 0.) == (sc.F < 0.)) {
-        c = a;
-        sc = sa;
-        e = dd = b - a;
-      }
-      if (fabs(sample_ratio(sc, sb)) < 1.) {  // |f(c)| < |f(b)|
-        a = b; sa = sb;
-        b = c; sb = sc;
-        c = a; sc = sa;
-      }
-      if (sb.F == 0.) return b;
-      const double mid = .5 * (c - b), half = .5 * stop;
-      if (fabs(c - b) <= stop) {
-        // converged bracket [b, c], f(b) and f(c) of opposite signs: its secant
-        // point is second order in the width and needs no evaluation (group
-        // velocities of some roots move by 1e-7 per 1e-11 of root error, so the
-        // midpoint's error of up to stop / 2 would show in them)
-        const double s = b - (c - b) / (sample_ratio(sc, sb) - 1.);
-        return (isfinite(s) && (s - b) * (s - c) <= 0.) ? s : .5 * (b + c);
-      }
-      if (fabs(e) >= half && fabs(sample_ratio(sa, sb)) > 1.) {
-        const double s = sample_ratio(sb, sa);
-        double p, q;
-        if (a == c) {
-          p = 2. * mid * s;
-          q = 1. - s;
-        } else {
-          const double qa = sample_ratio(sa, sc), r = sample_ratio(sb, sc);
-          p = s * (2. * mid * qa * (qa - r) - (b - a) * (r - 1.));
-          q = (qa - 1.) * (r - 1.) * (s - 1.);
-        }
-        if (p > 0.) q = -q; else p = -p;
-        const double old = e;
-        e = dd;
-        const double ratio = p / q;
-        if (isfinite(ratio) && 2. * p < fmin(3. * mid * q - fabs(half * q), fabs(old * q))) dd = ratio;
-        else { dd = mid; e = mid; }
-      } else {
-        dd = mid;
-        e = mid;
-      }
-      a = b;
-      sa = sb;
-      b += fabs(dd) > half ? dd : (mid > 0. ? half : -half);
-      x = b;
-    }
-    const RootSample smp = root_sample(m, wave, w, x);  // the one evaluation site
-    ++*evaluations;
-    if (pending & 1) {
-      sa = smp;
-      pending &= ~1;
-    } else if (pending & 2) {
-      sb = smp;
-      pending &= ~2;
-    } else {
-      sb = smp;
-      if (!isfinite(sb.F)) return NAN;
-    }
+// (cpp/common/refinement.hpp:341-396) on RootSamples, written as a state
+// machine: brent_advance either asks for the function at a point or finishes,
+// brent_absorb takes the sample.  End values unknown in FP64 (NaN: brackets of
+// the FP32 scan) are asked for first.  At most BRENT_MAX_EVALS evaluations.
+constexpr int BRENT_MAX_EVALS = 162;
+enum BrentStep { BRENT_EVAL = 0, BRENT_DONE = 1, BRENT_NO_BRACKET = 2 };
+struct BrentState {
+  double a, b, c, dd, e, stop;
+  RootSample sa, sb, sc;
+  int pending;  // bit 0: f(a) unknown, bit 1: f(b) unknown
+  int evals;
+  bool confirm, started, failed;
+};
+
+__device__ __forceinline__ void brent_init(BrentState &st, double a, double b, double fa, double fb) {
+  st.a = a;
+  st.b = b;
+  st.c = b;
+  st.dd = st.e = st.stop = 0.;
+  st.sa = RootSample{fa, fa, NAN};
+  st.sb = RootSample{fb, fb, NAN};
+  st.sc = RootSample{0., 0., NAN};
+  st.pending = (isfinite(fa) ? 0 : 1) | (isfinite(fb) ? 0 : 2);
+  st.confirm = st.pending != 0;
+  st.started = st.failed = false;
+  st.evals = 0;
+}
+
+__device__ __forceinline__ void brent_absorb(BrentState &st, const RootSample &smp) {
+  ++st.evals;
+  if (st.pending & 1) {
+    st.sa = smp;
+    st.pending &= ~1;
+  } else if (st.pending & 2) {
+    st.sb = smp;
+    st.pending &= ~2;
+  } else {
+    st.sb = smp;
+    if (!isfinite(smp.F)) st.failed = true;
   }
-  return NAN;
+}
+
+// BRENT_EVAL: evaluate at *x next.  BRENT_DONE: *root (NaN when refinement
+// failed).  BRENT_NO_BRACKET: the confirmed FP64 ends have one sign.
+__device__ __forceinline__ int brent_advance(BrentState &st, double tol, double *x, double *root) {
+  if (st.pending) {
+    *x = (st.pending & 1) ? st.a : st.b;
+    return BRENT_EVAL;
+  }
+  *root = NAN;
+  if (st.failed) return BRENT_DONE;
+  double a = st.a, b = st.b, c = st.c, dd = st.dd, e = st.e;
+  RootSample sa = st.sa, sb = st.sb, sc = st.sc;
+  if (!st.started) {
+    st.started = true;
+    if (st.confirm && signbit(sa.F) == signbit(sb.F)) return BRENT_NO_BRACKET;
+    if (a == b) {
+      if (sa.F == 0.) *root = a;
+      return BRENT_DONE;
+    }
+    if (!isfinite(sa.F) || !isfinite(sb.F) || ((sa.F < 0.) == (sb.F < 0.) && sa.F != 0. && sb.F != 0.))
+      return BRENT_DONE;
+    if (sa.F == 0.) { *root = a; return BRENT_DONE; }
+    if (sb.F == 0.) { *root = b; return BRENT_DONE; }
+    const double big = fmax(fabs(a), fabs(b));
+    st.stop = fmax(16. * 2.220446049250313e-16 * big, fmin((b - a) / 64., .125 * tol * big));
+    c = b;
+    sc = sb;
+    dd = e = b - a;
+  }
+  if (st.evals >= BRENT_MAX_EVALS) return BRENT_DONE;
+  if ((sb.F < 0.) == (sc.F < 0.)) {
+    c = a;
+    sc = sa;
+    e = dd = b - a;
+  }
+  if (fabs(sample_ratio(sc, sb)) < 1.) {  // |f(c)| < |f(b)|
+    a = b; sa = sb;
+    b = c; sb = sc;
+    c = a; sc = sa;
+  }
+  if (sb.F == 0.) { *root = b; return BRENT_DONE; }
+  const double mid = .5 * (c - b), half = .5 * st.stop;
+  if (fabs(c - b) <= st.stop) {
+    // converged bracket [b, c], f(b) and f(c) of opposite signs: its secant
+    // point is second order in the width and needs no evaluation (group
+    // velocities of some roots move by 1e-7 per 1e-11 of root error, so the
+    // midpoint's error of up to stop / 2 would show in them)
+    const double s = b - (c - b) / (sample_ratio(sc, sb) - 1.);
+    *root = (isfinite(s) && (s - b) * (s - c) <= 0.) ? s : .5 * (b + c);
+    return BRENT_DONE;
+  }
+  if (fabs(e) >= half && fabs(sample_ratio(sa, sb)) > 1.) {
+    const double s = sample_ratio(sb, sa);
+    double p, q;
+    if (a == c) {
+      p = 2. * mid * s;
+      q = 1. - s;
+    } else {
+      const double qa = sample_ratio(sa, sc), r = sample_ratio(sb, sc);
+      p = s * (2. * mid * qa * (qa - r) - (b - a) * (r - 1.));
+      q = (qa - 1.) * (r - 1.) * (s - 1.);
+    }
+    if (p > 0.) q = -q; else p = -p;
+    const double old = e;
+    e = dd;
+    const double ratio = p / q;
+    if (isfinite(ratio) && 2. * p < fmin(3. * mid * q - fabs(half * q), fabs(old * q))) dd = ratio;
+    else { dd = mid; e = mid; }
+  } else {
+    dd = mid;
+    e = mid;
+  }
+  a = b;
+  sa = sb;
+  b += fabs(dd) > half ? dd : (mid > 0. ? half : -half);
+  st.a = a; st.b = b; st.c = c; st.dd = dd; st.e = e;
+  st.sa = sa; st.sb = sb; st.sc = sc;
+  *x = b;
+  return BRENT_EVAL;
 }
 
 // ---------------------------------------------------------------------------
-// refine: one thread per bracket.
+// refine: one bracket per lane, lanes refilled from the bracket list.
+// Brackets converge in different numbers of evaluations; with one fixed bracket
+// per thread half the lanes of a warp idled on average.  Here every loop
+// iteration is one secular evaluation for all lanes that have work (one call
+// site), and a lane whose bracket finishes takes the next one from the list
+// (warp-aggregated atomic on C_REFINE_CURSOR) in the same iteration.  Each
+// bracket follows the same arithmetic as on its own, so results do not depend
+// on the schedule.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128, 4) refine(Dev d) {
-  const int begin = d.ctr[C_REFINE_BEGIN];
-  unsigned long long evals = 0, steps = 0, count = 0;
-  for (int i = begin + blockIdx.x * blockDim.x + threadIdx.x; i < *(volatile int *)&d.ctr[C_NREFINE];
-       i += gridDim.x * blockDim.x) {
-    const int id = d.refine_list[i];
-    const int t = id / d.KB;
-    const int b = d.tr_model[t];
-    const LayerView<double> m = global_view(d, b);
-    const double w = TWO_PI / d.tr_period[t];
-    double *sl = d.slot + static_cast<size_t>(id) * SLOT;
-    int ev = 0;
-    bool no_bracket;
-    const double r = refine_bracket(m, d.wave, w, sl[0], sl[1], sl[2], sl[3], d.tol, &ev, &no_bracket);
-    evals += ev;
-    steps += static_cast<unsigned long long>(ev) * layer_steps(m.L, m.water);
-    sl[4] = r;
-    if (no_bracket) {  // the FP32 scan's sign change does not hold in FP64
-      atomicOr(&d.tflags[t], INTERNAL_REPAIR);
-      continue;
-    }
-    if (!isfinite(r)) atomicOr(&d.tflags[t], TRACE_REFINEMENT_FAILED);
+struct RefineLane {
+  BrentState st;
+  LayerView<double> m;
+  double w;
+  double *sl;
+  int id, t;
+  bool eval, exhausted;
+};
+
+__device__ __forceinline__ void refine_step(Dev &d, RefineLane &L, double *x, unsigned long long &count) {
+  if (L.id < 0 || L.eval) return;
+  double root;
+  const int r = brent_advance(L.st, d.tol, x, &root);
+  if (r == BRENT_EVAL) {
+    L.eval = true;
+    return;
+  }
+  L.sl[4] = r == BRENT_DONE ? root : NAN;
+  if (r == BRENT_NO_BRACKET) {  // the FP32 scan's sign change does not hold in FP64
+    atomicOr(&d.tflags[L.t], INTERNAL_REPAIR);
+  } else {
+    if (!isfinite(root)) atomicOr(&d.tflags[L.t], TRACE_REFINEMENT_FAILED);
     ++count;
+  }
+  L.id = -1;
+}
+
+__device__ __forceinline__ void refine_fetch(Dev &d, RefineLane &L, int end, int lane) {
+  const bool need = L.id < 0 && !L.exhausted;
+  const unsigned nm = __ballot_sync(FULL, need);
+  if (!nm) return;
+  const int leader = __ffs(nm) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(&d.ctr[C_REFINE_CURSOR], __popc(nm));
+  base = __shfl_sync(FULL, base, leader);
+  if (!need) return;
+  const int i = base + __popc(nm & lanemask_lt());
+  if (i >= end) {
+    L.exhausted = true;
+    return;
+  }
+  L.id = d.refine_list[i];
+  L.t = L.id / d.KB;
+  L.m = global_view(d, d.tr_model[L.t]);
+  L.w = TWO_PI / d.tr_period[L.t];
+  L.sl = d.slot + static_cast<size_t>(L.id) * SLOT;
+  brent_init(L.st, L.sl[0], L.sl[1], L.sl[2], L.sl[3]);
+}
+
+__global__ void __launch_bounds__(128, 4) refine(Dev d) {
+  const int lane = threadIdx.x & 31;
+  const int end = d.ctr[C_NREFINE];
+  unsigned long long evals = 0, steps = 0, count = 0;
+  RefineLane L;
+  L.id = -1;
+  L.exhausted = false;
+  for (;;) {
+    double x = 0.;
+    L.eval = false;
+    refine_step(d, L, &x, count);
+    refine_fetch(d, L, end, lane);
+    refine_step(d, L, &x, count);
+    refine_fetch(d, L, end, lane);
+    refine_step(d, L, &x, count);
+    if (__all_sync(FULL, !L.eval && L.exhausted)) break;
+    if (L.eval) {
+      const RootSample smp = root_sample(L.m, d.wave, L.w, x);  // the one evaluation site
+      brent_absorb(L.st, smp);
+      ++evals;
+      steps += layer_steps(L.m.L, L.m.water);
+    }
   }
   if (d.stats && (evals || count)) {
     atomicAdd(&d.stats[0], evals);
@@ -1334,7 +1413,7 @@ __global__ void __launch_bounds__(128, 4) refine(Dev d) {
 __global__ void collect_repairs(Dev d) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t == 0) {
-    d.ctr[C_REFINE_BEGIN] = d.ctr[C_NREFINE];
+    d.ctr[C_REFINE_BEGIN] = d.ctr[C_REFINE_CURSOR] = d.ctr[C_NREFINE];
   }
   if (t >= d.n_traces) return;
   const unsigned fl = d.tflags[t];
@@ -1480,7 +1559,7 @@ __global__ void assemble(Dev d, const int *list = nullptr, int count_id = 0) {
 __global__ void continuity_screen(Dev d) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t == 0) {
-    d.ctr[C_REFINE_BEGIN] = d.ctr[C_NREFINE];
+    d.ctr[C_REFINE_BEGIN] = d.ctr[C_REFINE_CURSOR] = d.ctr[C_NREFINE];
     d.ctr[C_GROUP_BEGIN] = d.ctr[C_NGROUP];
   }
   if (t >= d.n_traces) return;
