@@ -65,6 +65,7 @@ def parse():
     p.add_argument("--no-jacobian", action="store_true")
     p.add_argument("--no-ragged", action="store_true")
     p.add_argument("--no-config3", action="store_true")
+    p.add_argument("--no-reliability", action="store_true")
     return p.parse_args()
 
 
@@ -324,6 +325,108 @@ def config3_bench(torch, local, flush, sample=256, rank=0):
             "fp32_vs_fp64_engine": agree, "fp32_vs_reference": vs_ref}
 
 
+def hbm_peak_gbs():
+    """Measured HBM copy bandwidth of this pool's B200s (MEASURED_PEAKS.json), else the fallback."""
+    try:
+        return float(json.loads((Path(__file__).resolve().parent / "MEASURED_PEAKS.json").read_text())["hbm_gbs"]), \
+            "measured"
+    except (OSError, ValueError, KeyError):
+        return 6650., "fallback"
+
+
+def reliability_bench(torch, local, steps, flush, rank=0, sample=300):
+    """Cross-period mode-reliability checks of a solved crustal batch (10,000 models
+    x 5 modes x 60 periods, Rayleigh, FP32-scan engine): the kernel on device buffers
+    timed with CUDA events (L2 flushed before each step), the public
+    check_mode_reliability on host arrays (copies included, wall clock), and the
+    oracle port on a bounded sample of the same result, whose flags the kernel's
+    must match bit for bit (the checks are per model, so a sample of models is a
+    sample of the job)."""
+    from modisp_b200 import _native, workloads
+    from modisp_b200.reliability import check_mode_reliability, period_plan
+    import oracle.reliability as orel
+    batch, periods, nmodes = workloads.config2()
+    B, L = batch["thickness"].shape
+    T = periods.size
+    o = _native.default_options()
+    o.single_precision = 1
+    eng = _native.Engine(local, B, L, T, nmodes, o)
+    out = eng.run(batch["thickness"], batch["vp"], batch["vs"], batch["rho"], periods, None, TOL, 1., 0)
+    eng.close()
+    v = np.ascontiguousarray(out["velocity"], dtype=np.float64)
+    tf = np.ascontiguousarray(out["flags"], dtype=np.uint32)
+    cnt = np.ascontiguousarray(out["counts"], dtype=np.int64)
+    dev = torch.device("cuda", local)
+    v_d = torch.tensor(v, device=dev)
+    tf_d = torch.tensor(tf.view(np.int32), device=dev)
+    cnt_d = torch.tensor(cnt, device=dev)
+    fl_d = torch.empty((B, nmodes, T), dtype=torch.int16, device=dev)
+    as_d = torch.empty((B, nmodes, T), dtype=torch.uint8, device=dev)
+    plan, order, _ = period_plan(periods)
+    stream = torch.cuda.current_stream().cuda_stream
+
+    plan_d = torch.tensor(plan.view(np.uint8), device=dev)
+    order_d = torch.tensor(order, device=dev)
+
+    def device_call():  # plan uploaded by the call (stream-ordered scratch)
+        _native.mode_reliability_device(v_d.data_ptr(), tf_d.data_ptr(), cnt_d.data_ptr(), B, nmodes, T, plan, order,
+                                        .005, .1, .05, fl_d.data_ptr(), as_d.data_ptr(), stream)
+
+    def kernel_call():  # plan already on the device: the kernel alone
+        _native.mode_reliability_planned(v_d.data_ptr(), tf_d.data_ptr(), cnt_d.data_ptr(), B, nmodes, T,
+                                         plan_d.data_ptr(), order_d.data_ptr(), .005, .1, .05, fl_d.data_ptr(),
+                                         as_d.data_ptr(), stream)
+
+    def timed(call):
+        for _ in range(3):
+            call()
+        total = 0.
+        for _ in range(steps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            call()
+            b.record()
+            b.synchronize()
+            total += a.elapsed_time(b)
+        return total / steps
+
+    ms_upload = timed(device_call)
+    ms = timed(kernel_call)
+    check_mode_reliability(v, periods, trace_flags=tf, root_count=cnt, device=local)  # warm-up
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        res = check_mode_reliability(v, periods, trace_flags=tf, root_count=cnt, device=local)
+    wall = (time.perf_counter() - t0) / steps
+    same_device = bool(np.array_equal(fl_d.cpu().numpy().view(np.uint16), res.flags))
+    cells = B * nmodes * T
+    algorithmic = cells * (8 + 2 + 1) + B * T * (4 + 8)  # roots in; flags, assessed out; trace flags, counts in
+    peak, peak_kind = hbm_peak_gbs()
+    line = {"workload": "check_mode_reliability of a solved 10,000-model crustal result (5 modes x 60 periods, "
+                        "Rayleigh, FP32-scan engine), default thresholds",
+            "cells_per_step": cells, "flagged_fraction": float((res.flags != 0).mean()),
+            "value": cells / (ms * 1e-3), "unit": "cells/s", "ms_per_step": ms,
+            "roofline": {"bound": "hbm", "kernel": "mode_reliability", "achieved": algorithmic / (ms * 1e-3) / 1e9,
+                         "peak": peak, "unit": "GB/s", "frac": algorithmic / (ms * 1e-3) / 1e9 / peak,
+                         "peak_kind": peak_kind, "algorithmic_bytes": algorithmic},
+            "ms_per_step_with_plan_upload": ms_upload,
+            "e2e": {"value": cells / wall, "unit": "cells/s", "ms_per_step": wall * 1e3,
+                    "h2d_bytes_per_step": v.nbytes + tf.nbytes + cnt.nbytes + plan.nbytes + order.nbytes,
+                    "d2h_bytes_per_step": cells * 3},
+            "device_and_host_entry_agree": same_device}
+    if rank == 0:
+        idx = np.linspace(0, B - 1, sample).astype(int)
+        t0 = time.perf_counter()
+        want = orel.check(v[idx], periods, tf[idx], cnt[idx])
+        cpu_s = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": sample * nmodes * T / cpu_s, "unit": "cells/s", "cores": 1, "kind": "port",
+                                "sample": f"{sample} of the 10,000 models ({sample * nmodes * T} cells), the oracle's "
+                                          f"numpy restatement vectorised as the reference's; {cpu_s:.2f} s"}
+        line["matches_oracle_on_sample"] = bool(np.array_equal(res.flags[idx], want[0]) and
+                                                np.array_equal(res.assessed[idx], want[1]))
+    return line
+
+
 def ragged_bench(torch, local, steps, warmup, flush, models=RAGGED_MODELS):
     """Large uneven batch: smooth-gradient models of 30-100 thin layers, each with its
     own 50-120 periods inside 0.2-100 s and 1-10 modes, Rayleigh + Love, FP32 scan /
@@ -536,6 +639,8 @@ def main():
     jac = jacobian_bench(torch, local, max(2, args.steps // 2), 2, flush) if not args.no_jacobian else None
     ragged = ragged_bench(torch, local, max(2, args.steps // 2), 2, flush) if not args.no_ragged else None
     config3 = config3_bench(torch, local, flush, rank=rank) if not args.no_config3 else None
+    reliability = (reliability_bench(torch, local, max(3, args.steps), flush, rank=rank)
+                   if not args.no_reliability else None)
 
     peak32 = _native.measure_peak(local, fp64=False)
     peak64 = _native.measure_peak(local, fp64=True)
@@ -573,6 +678,7 @@ def main():
             "jacobian": jac,
             "ragged": ragged,
             "config3": config3,
+            "reliability": reliability,
         }
         print(json.dumps(line))
     if world > 1:

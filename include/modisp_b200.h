@@ -17,6 +17,7 @@
 #ifndef MODISP_B200_H
 #define MODISP_B200_H
 #include <stddef.h>
+#include <stdint.h>
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -252,6 +253,63 @@ int md200_group_roots(const double *thickness, const double *vp, const double *v
                       const double *rho, int layers, int wave, double period,
                       const double *roots, int known, int modes, double close_rtol,
                       double *group, unsigned *group_flags);
+
+/* ---- Cross-period mode-reliability checks ------------------------------ *
+ * Replace check_mode_reliability (python/modisp/reliability.py:49-145): flags
+ * [B][K][T] (ModeReliabilityFlag bits, :12-24) and an "assessed" mask for a
+ * result's phase velocities, without editing them.  The period order is a plan
+ * of T entries (stable sort, distinct periods, gaps, prediction ratios); the
+ * Python layer builds it with the reference's own numpy arithmetic, and
+ * md200_reliability_plan builds it in C (libm log / log1p, which can differ from
+ * numpy's in the last bit of a ratio). */
+#define MD200_PLAN_FIRST 1     /* first period in sorted order: unassessed */
+#define MD200_PLAN_DUPLICATE 2 /* equal to the previous distinct period */
+#define MD200_PLAN_GAP 4       /* log gap to the previous period above the limit */
+#define MD200_PLAN_PREDICT 8   /* linear prediction from the two previous periods */
+typedef struct {
+  int32_t prev;      /* previous distinct period (index into periods), -1 for the first */
+  int32_t older;     /* the distinct period before prev, when MD200_PLAN_PREDICT */
+  int32_t kind;      /* MD200_PLAN_* bits */
+  int32_t dup_begin; /* a distinct period's duplicates are order[dup_begin .. dup_end) */
+  int32_t dup_end;
+  int32_t reserved;
+  double ratio;      /* log_gap(prev, t) / log_gap(older, prev), when MD200_PLAN_PREDICT */
+} md200_period_plan;
+
+/* Plan for periods[T] (finite, positive): plan[T], order[T] (stable sort).
+ * reliability.py:7-9 (log gap) and :107-144 (period walk). */
+int md200_reliability_plan(const double *periods, int T, double max_log_period_gap,
+                           md200_period_plan *plan, int32_t *order);
+
+/* The checks on host arrays: velocity [B][K][T] (positive or NaN), trace_flags
+ * [B][T] (NULL: none), root_count [B][T] (NULL: finite roots per trace), plan and
+ * order from a plan builder.  Outputs flags [B][K][T] (uint16) and assessed
+ * [B][K][T] (0/1).  Device buffers are allocated and freed on a private stream. */
+int md200_mode_reliability(int device, const double *velocity, const uint32_t *trace_flags,
+                           const int64_t *root_count, int B, int K, int T,
+                           const md200_period_plan *plan, const int32_t *order,
+                           double close_root_rtol, double max_relative_step, double prediction_rtol,
+                           uint16_t *flags, uint8_t *assessed);
+
+/* The same on device buffers (velocity, trace_flags, root_count, flags, assessed;
+ * plan and order stay host arrays), enqueued on `stream` (NULL: the legacy
+ * stream) and not waited for.  The plan is uploaded to stream-ordered scratch. */
+int md200_mode_reliability_device(const double *velocity, const uint32_t *trace_flags,
+                                  const int64_t *root_count, int B, int K, int T,
+                                  const md200_period_plan *plan, const int32_t *order,
+                                  double close_root_rtol, double max_relative_step,
+                                  double prediction_rtol, uint16_t *flags, uint8_t *assessed,
+                                  void *stream);
+
+/* The same with the plan and order already on the device (from a plan
+ * uploaded once for many checks with the same periods): only the kernel is
+ * enqueued.  The plan's indices are trusted: build it with a plan builder. */
+int md200_mode_reliability_planned(const double *velocity, const uint32_t *trace_flags,
+                                   const int64_t *root_count, int B, int K, int T,
+                                   const md200_period_plan *plan, const int32_t *order,
+                                   double close_root_rtol, double max_relative_step,
+                                   double prediction_rtol, uint16_t *flags, uint8_t *assessed,
+                                   void *stream);
 
 /* md200_group_roots without any device allocation.  No counterpart in the
  * reference: it exists for callers that cannot call cudaMalloc -- code whose GPU

@@ -16,5 +16,6 @@ from .api import (  # noqa: F401
     TRACE_AUTO_RELAXED, LEVEL_FP64_SCAN, LEVEL_FP32_SCAN, LEVEL_FP32_REPAIRED, LEVEL_CONTINUATION,
 )
 from ._native import BackendUnavailableError  # noqa: F401
+from .reliability import ModeReliability, ModeReliabilityFlag, check_mode_reliability  # noqa: F401
 
 __version__ = "0.5.0"

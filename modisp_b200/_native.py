@@ -83,7 +83,15 @@ EXPORTS = {
     "md200_jacobian": (_I, [_P, _P, _P, _P, _P, _I, _P, _I, _P, _P, _P, _P, ctypes.POINTER(_I)]),
     "md200_vjp_device": (_I, [_P, _P, _P, _P, _P, _I, _P, _I, _P, _P, _P, _P, _P, _P]),
     "md200_vjp": (_I, [_P, _P, _P, _P, _P, _I, _P, _I, _P, _P, _P, _P, _P]),
+    "md200_reliability_plan": (_I, [_P, _I, _D, _P, _P]),
+    "md200_mode_reliability": (_I, [_I, _P, _P, _P, _I, _I, _I, _P, _P, _D, _D, _D, _P, _P]),
+    "md200_mode_reliability_device": (_I, [_P, _P, _P, _I, _I, _I, _P, _P, _D, _D, _D, _P, _P, _P]),
+    "md200_mode_reliability_planned": (_I, [_P, _P, _P, _I, _I, _I, _P, _P, _D, _D, _D, _P, _P, _P]),
 }
+# md200_period_plan (include/modisp_b200.h)
+PERIOD_PLAN = np.dtype([("prev", np.int32), ("older", np.int32), ("kind", np.int32), ("dup_begin", np.int32),
+                        ("dup_end", np.int32), ("reserved", np.int32), ("ratio", np.float64)])
+PLAN_FIRST, PLAN_DUPLICATE, PLAN_GAP, PLAN_PREDICT = 1, 2, 4, 8
 STAGES = ("prep", "trace_list", "scan", "refine", "repair_select", "repair_scan", "repair_refine",
           "assemble", "group_velocity", "continuity")
 
@@ -361,6 +369,50 @@ def group_roots(h, vp, vs, rho, wave, period, roots, modes, close_rtol=.005):
     check(lib().md200_group_roots(*(ptr(a) for a in arrays), arrays[0].size, int(wave), float(period),
                                   ptr(r), r.size, int(modes), float(close_rtol), ptr(group), ptr(flags)))
     return group, flags
+
+
+def reliability_plan(periods, max_log_period_gap: float):
+    """The C plan builder (libm logarithms): (plan [T] PERIOD_PLAN, order [T] int32)."""
+    p = np.ascontiguousarray(periods, dtype=np.float64).ravel()
+    plan = np.zeros(p.size, PERIOD_PLAN)
+    order = np.zeros(p.size, np.int32)
+    check(lib().md200_reliability_plan(ptr(p), p.size, float(max_log_period_gap), ptr(plan), ptr(order)))
+    return plan, order
+
+
+def mode_reliability(velocity, plan, order, trace_flags=None, root_count=None, close_root_rtol=.005,
+                     max_relative_step=.1, prediction_rtol=.05, device: int = 0):
+    """Flags [B,K,T] uint16 and assessed [B,K,T] bool for host arrays (md200_mode_reliability)."""
+    v = np.ascontiguousarray(velocity, dtype=np.float64)
+    B, K, T = v.shape
+    tf = None if trace_flags is None else np.ascontiguousarray(trace_flags, dtype=np.uint32)
+    cnt = None if root_count is None else np.ascontiguousarray(root_count, dtype=np.int64)
+    plan = np.ascontiguousarray(plan, dtype=PERIOD_PLAN)
+    order = np.ascontiguousarray(order, dtype=np.int32)
+    flags = np.empty(v.shape, np.uint16)
+    assessed = np.empty(v.shape, np.uint8)
+    check(lib().md200_mode_reliability(int(device), ptr(v), ptr(tf), ptr(cnt), B, K, T, ptr(plan), ptr(order),
+                                       float(close_root_rtol), float(max_relative_step), float(prediction_rtol),
+                                       ptr(flags), ptr(assessed)))
+    return flags, assessed.astype(bool)
+
+
+def mode_reliability_device(velocity, trace_flags, root_count, B, K, T, plan, order, close_root_rtol,
+                            max_relative_step, prediction_rtol, flags, assessed, stream=None):
+    """md200_mode_reliability_device on device pointers (ints); plan/order are host arrays."""
+    plan = np.ascontiguousarray(plan, dtype=PERIOD_PLAN)
+    order = np.ascontiguousarray(order, dtype=np.int32)
+    check(lib().md200_mode_reliability_device(velocity, trace_flags, root_count, int(B), int(K), int(T), ptr(plan),
+                                              ptr(order), float(close_root_rtol), float(max_relative_step),
+                                              float(prediction_rtol), flags, assessed, _stream_arg(stream)))
+
+
+def mode_reliability_planned(velocity, trace_flags, root_count, B, K, T, plan, order, close_root_rtol,
+                             max_relative_step, prediction_rtol, flags, assessed, stream=None):
+    """md200_mode_reliability_planned: every argument a device pointer (int)."""
+    check(lib().md200_mode_reliability_planned(velocity, trace_flags, root_count, int(B), int(K), int(T), plan, order,
+                                               float(close_root_rtol), float(max_relative_step),
+                                               float(prediction_rtol), flags, assessed, _stream_arg(stream)))
 
 
 def kernel_report(layers: int, single_precision: bool = False) -> dict:

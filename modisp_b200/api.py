@@ -142,6 +142,12 @@ class DispersionBatch:
         self.status[rejected] = SolveStatus.REJECTED
         self.mode_convention = "ascending roots in the reported search interval"
 
+    def check_modes(self, **options):
+        """Cross-period mode-reliability checks of this result on the GPU
+        (python/modisp/__init__.py:126-127); see modisp_b200.reliability."""
+        from .reliability import check_mode_reliability
+        return check_mode_reliability(self, **options)
+
     @property
     def n_models(self):
         return self.phase_velocity.shape[0]

@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <mutex>
 #include <cstdio>
 #include <cstring>
@@ -17,6 +18,7 @@
 #include "modisp_b200.h"
 #include "kernels.cuh"
 #include "adjoint.cuh"
+#include "reliability.cuh"
 
 using namespace md200;
 
@@ -980,6 +982,176 @@ int md200_group_roots(const double *h, const double *vp, const double *vs, const
   cudaFree(dtab);
   cudaFree(dgrp);
   cudaFree(dfl);
+  if (err != cudaSuccess) return fail(std::string("modisp_b200 CUDA: ") + cudaGetErrorString(err));
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Cross-period mode-reliability checks (python/modisp/reliability.py:49-145)
+// ---------------------------------------------------------------------------
+namespace {
+
+// ln(b / a) for a <= b, through log1p for small gaps (reliability.py:7-9)
+double log_gap(double a, double b) { return b - a < a ? std::log1p((b - a) / a) : std::log(b) - std::log(a); }
+
+// Every index the kernel will follow must lie inside the arrays.
+bool plan_ok(const md200_period_plan *plan, const int32_t *order, int T) {
+  for (int t = 0; t < T; ++t) {
+    const md200_period_plan &p = plan[t];
+    if (order[t] < 0 || order[t] >= T) return false;
+    if (!(p.kind & MD200_PLAN_FIRST) && (p.prev < 0 || p.prev >= T)) return false;
+    if ((p.kind & MD200_PLAN_PREDICT) && (p.older < 0 || p.older >= T || !std::isfinite(p.ratio))) return false;
+    if (p.dup_begin < 0 || p.dup_end < p.dup_begin || p.dup_end > T) return false;
+  }
+  return true;
+}
+
+int reliability_args(ReliabilityArgs &r, int B, int K, int T, const md200_period_plan *plan, const int32_t *order,
+                     double close_rtol, double max_step, double pred_rtol) {
+  if (B < 1 || K < 1 || T < 1) return fail("modisp_b200: expected velocity [B,K,T] with B, K, T >= 1");
+  if (!plan || !order || !plan_ok(plan, order, T)) return fail("modisp_b200: invalid period plan");
+  if (!(close_rtol > 0.) || !(max_step > 0.) || !(pred_rtol > 0.) || !std::isfinite(close_rtol) ||
+      !std::isfinite(max_step) || !std::isfinite(pred_rtol))
+    return fail("modisp_b200: tolerances must be finite and positive");
+  r.B = B;
+  r.K = K;
+  r.T = T;
+  r.close_rtol = close_rtol;
+  r.max_step = max_step;
+  r.pred_rtol = pred_rtol;
+  return 0;
+}
+
+}  // namespace
+
+int md200_reliability_plan(const double *periods, int T, double max_log_period_gap, md200_period_plan *plan,
+                           int32_t *order) {
+  if (T < 1) return fail("modisp_b200: no periods");
+  for (int t = 0; t < T; ++t)
+    if (!std::isfinite(periods[t]) || !(periods[t] > 0.)) return fail("modisp_b200: periods must be finite and positive");
+  std::vector<int32_t> idx(T);
+  for (int t = 0; t < T; ++t) idx[t] = t;
+  std::stable_sort(idx.begin(), idx.end(), [&](int32_t a, int32_t b) { return periods[a] < periods[b]; });
+  std::vector<int32_t> unique;
+  int32_t group = -1;  // position in order of the current distinct period
+  for (int q = 0; q < T; ++q) {
+    const int32_t t = idx[q];
+    order[q] = t;
+    md200_period_plan &p = plan[t];
+    p = md200_period_plan{-1, -1, 0, 0, 0, 0, 0.};
+    if (unique.empty()) {
+      p.kind = MD200_PLAN_FIRST;
+    } else {
+      const int32_t prev = unique.back();
+      p.prev = prev;
+      if (periods[t] == periods[prev]) {
+        p.kind = MD200_PLAN_DUPLICATE;
+        plan[prev].dup_end = q + 1;
+        continue;
+      }
+      const double lg = log_gap(periods[prev], periods[t]);
+      if (lg > max_log_period_gap) p.kind |= MD200_PLAN_GAP;
+      if (unique.size() >= 2) {
+        const int32_t older = unique[unique.size() - 2];
+        const double den = log_gap(periods[older], periods[prev]);
+        if (den <= max_log_period_gap && lg <= max_log_period_gap) {
+          p.kind |= MD200_PLAN_PREDICT;
+          p.older = older;
+          p.ratio = lg / den;
+        }
+      }
+    }
+    group = q;
+    p.dup_begin = p.dup_end = group + 1;
+    unique.push_back(t);
+  }
+  return 0;
+}
+
+int md200_mode_reliability_planned(const double *velocity, const uint32_t *trace_flags, const int64_t *root_count,
+                                   int B, int K, int T, const md200_period_plan *plan, const int32_t *order,
+                                   double close_root_rtol, double max_relative_step, double prediction_rtol,
+                                   uint16_t *flags, uint8_t *assessed, void *stream) {
+  if (B < 1 || K < 1 || T < 1 || !plan || !order)
+    return fail("modisp_b200: expected velocity [B,K,T] with B, K, T >= 1 and a device plan");
+  if (!(close_root_rtol > 0.) || !(max_relative_step > 0.) || !(prediction_rtol > 0.) ||
+      !std::isfinite(close_root_rtol) || !std::isfinite(max_relative_step) || !std::isfinite(prediction_rtol))
+    return fail("modisp_b200: tolerances must be finite and positive");
+  ReliabilityArgs r{velocity, trace_flags, root_count, plan, order, B, K, T, close_root_rtol, max_relative_step,
+                    prediction_rtol, flags, assessed};
+  const size_t n = static_cast<size_t>(B) * T;
+  mode_reliability<<<static_cast<unsigned>((n + 255) / 256), 256, 0,
+                     stream ? static_cast<cudaStream_t>(stream) : cudaStreamLegacy>>>(r);
+  MD200_CK(cudaGetLastError());
+  return 0;
+}
+
+int md200_mode_reliability_device(const double *velocity, const uint32_t *trace_flags, const int64_t *root_count,
+                                  int B, int K, int T, const md200_period_plan *plan, const int32_t *order,
+                                  double close_root_rtol, double max_relative_step, double prediction_rtol,
+                                  uint16_t *flags, uint8_t *assessed, void *stream) {
+  ReliabilityArgs r{};
+  if (reliability_args(r, B, K, T, plan, order, close_root_rtol, max_relative_step, prediction_rtol)) return 1;
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : cudaStreamLegacy;
+  void *dplan = nullptr;
+  const size_t plan_bytes = sizeof(md200_period_plan) * T, order_bytes = sizeof(int32_t) * T;
+  MD200_CK(cudaMallocAsync(&dplan, plan_bytes + order_bytes, s));
+  cudaError_t err = cudaMemcpyAsync(dplan, plan, plan_bytes, cudaMemcpyHostToDevice, s);
+  if (err == cudaSuccess)
+    err = cudaMemcpyAsync(static_cast<char *>(dplan) + plan_bytes, order, order_bytes, cudaMemcpyHostToDevice, s);
+  int status = 0;
+  if (err == cudaSuccess)
+    status = md200_mode_reliability_planned(
+        velocity, trace_flags, root_count, B, K, T, static_cast<const md200_period_plan *>(dplan),
+        reinterpret_cast<const int32_t *>(static_cast<char *>(dplan) + plan_bytes), close_root_rtol,
+        max_relative_step, prediction_rtol, flags, assessed, s);
+  const cudaError_t err2 = cudaFreeAsync(dplan, s);
+  if (status) return status;
+  if (err == cudaSuccess) err = err2;
+  if (err != cudaSuccess) return fail(std::string("modisp_b200 CUDA: ") + cudaGetErrorString(err));
+  return 0;
+}
+
+int md200_mode_reliability(int device, const double *velocity, const uint32_t *trace_flags,
+                           const int64_t *root_count, int B, int K, int T, const md200_period_plan *plan,
+                           const int32_t *order, double close_root_rtol, double max_relative_step,
+                           double prediction_rtol, uint16_t *flags, uint8_t *assessed) {
+  ReliabilityArgs check{};
+  if (reliability_args(check, B, K, T, plan, order, close_root_rtol, max_relative_step, prediction_rtol)) return 1;
+  MD200_CK(cudaSetDevice(device));
+  cudaStream_t s = nullptr;
+  MD200_CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  const size_t cells = static_cast<size_t>(B) * K * T, traces = static_cast<size_t>(B) * T;
+  double *dv = nullptr;
+  uint32_t *dtf = nullptr;
+  int64_t *dcnt = nullptr;
+  uint16_t *dfl = nullptr;
+  uint8_t *das = nullptr;
+  cudaError_t err = cudaMallocAsync(&dv, sizeof(double) * cells, s);
+  if (err == cudaSuccess && trace_flags) err = cudaMallocAsync(&dtf, sizeof(uint32_t) * traces, s);
+  if (err == cudaSuccess && root_count) err = cudaMallocAsync(&dcnt, sizeof(int64_t) * traces, s);
+  if (err == cudaSuccess) err = cudaMallocAsync(&dfl, sizeof(uint16_t) * cells, s);
+  if (err == cudaSuccess) err = cudaMallocAsync(&das, sizeof(uint8_t) * cells, s);
+  if (err == cudaSuccess) err = cudaMemcpyAsync(dv, velocity, sizeof(double) * cells, cudaMemcpyHostToDevice, s);
+  if (err == cudaSuccess && dtf)
+    err = cudaMemcpyAsync(dtf, trace_flags, sizeof(uint32_t) * traces, cudaMemcpyHostToDevice, s);
+  if (err == cudaSuccess && dcnt)
+    err = cudaMemcpyAsync(dcnt, root_count, sizeof(int64_t) * traces, cudaMemcpyHostToDevice, s);
+  int status = 0;
+  if (err == cudaSuccess)
+    status = md200_mode_reliability_device(dv, dtf, dcnt, B, K, T, plan, order, close_root_rtol, max_relative_step,
+                                           prediction_rtol, dfl, das, s);
+  if (err == cudaSuccess && !status)
+    err = cudaMemcpyAsync(flags, dfl, sizeof(uint16_t) * cells, cudaMemcpyDeviceToHost, s);
+  if (err == cudaSuccess && !status)
+    err = cudaMemcpyAsync(assessed, das, sizeof(uint8_t) * cells, cudaMemcpyDeviceToHost, s);
+  for (void *ptr : {static_cast<void *>(dv), static_cast<void *>(dtf), static_cast<void *>(dcnt),
+                    static_cast<void *>(dfl), static_cast<void *>(das)})
+    if (ptr) cudaFreeAsync(ptr, s);
+  const cudaError_t sync = cudaStreamSynchronize(s);
+  cudaStreamDestroy(s);
+  if (status) return status;
+  if (err == cudaSuccess) err = sync;
   if (err != cudaSuccess) return fail(std::string("modisp_b200 CUDA: ") + cudaGetErrorString(err));
   return 0;
 }

@@ -21,10 +21,17 @@ Outputs (all small .npz files, committed):
 * ``fixture_<name>.npz``: the reference test suite's own frozen fixtures
   (tests/data/accuracy_high_cpu_linux/*.npz, tests/data/witness_*.npz,
   tests/data/B10000_*.npz) repacked with their inputs and expected roots.
+* ``reliability_<case>.npz``: inputs and outputs of the reference's cross-period
+  mode-reliability checks (python/modisp/reliability.py, loaded from its file):
+  the cases of the reference's own tests, seeded synthetic batches (unsorted and
+  duplicate periods, gaps, NaNs, crossing ranks, failure and uncertainty bits,
+  negative counts, every option non-default) and two reference-solver results.
+  ``--only reliability`` regenerates just these.
 """
 from __future__ import annotations
 
 import argparse
+import importlib.util
 import sys
 from pathlib import Path
 
@@ -105,10 +112,102 @@ def repack_reference_fixtures(reference: Path):
         print("fixture", path.stem)
 
 
+def load_reference_reliability(reference: Path):
+    spec = importlib.util.spec_from_file_location("reference_reliability",
+                                                  reference / "python" / "modisp" / "reliability.py")
+    module = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(module)
+    return module
+
+
+def synthetic_reliability(seed, B, K, T, duplicates=True, gaps=True):
+    """Mode curves with the defects the checks look for, in shuffled period order."""
+    rng = np.random.default_rng(seed)
+    p = np.sort(np.exp(rng.uniform(np.log(.5), np.log(50.), T)))
+    if gaps:
+        p[T // 2:] *= np.exp(.6)  # one gap above the default 0.25 log units
+    if duplicates:
+        p[3] = p[2]
+        p[T - 2] = p[T - 3]
+    base = 1. + np.arange(K)[None, :, None] * (.35 + .1 * rng.random((B, 1, 1)))
+    v = base * (1. + .25 * np.log(p)[None, None, :] / np.log(50.)) + 1e-3 * rng.standard_normal((B, K, T))
+    v[rng.random(v.shape) < .01] = np.nan  # holes
+    hi = rng.random((B, T)) < .03  # lost top modes
+    v[:, -1, :][hi] = np.nan
+    if K >= 2:
+        swap = rng.random((B, T)) < .03  # crossing ranks
+        v[:, [0, 1], :] = np.where(swap[:, None, :], v[:, [1, 0], :], v[:, [0, 1], :])
+    if K >= 3:
+        close = rng.random((B, T)) < .03  # near-degenerate pairs
+        v[:, 2, :] = np.where(close, v[:, 1, :] * (1. + 1e-3), v[:, 2, :])
+    jump = rng.random((B, K, T)) < .02  # step jumps
+    v = np.where(jump, v * 1.3, v)
+    if duplicates:
+        dup_noise = rng.random((B, K)) < .2  # duplicates that disagree
+        v[:, :, 3] = np.where(dup_noise, v[:, :, 2] * (1. + 1e-6), v[:, :, 2])
+    order = rng.permutation(T)
+    tf = (rng.integers(0, 2, (B, T)) * rng.choice([1, 2, 4, 8, 2048, 4096, 1 << 20], (B, T))).astype(np.uint32)
+    tf[rng.random((B, T)) < .7] = 0
+    counts = np.isfinite(v).sum(axis=1).astype(np.int32)
+    counts[rng.random((B, T)) < .03] = -1
+    counts[rng.random((B, T)) < .03] += 1
+    return v[:, :, order], p[order], tf[:, order], counts[:, order]
+
+
+def save_reliability_case(rel, name, velocity, periods, trace_flags=None, root_count=None, **options):
+    r = rel.check_mode_reliability(velocity, periods, trace_flags=trace_flags, root_count=root_count, **options)
+    extra = {}
+    if trace_flags is not None:
+        extra["trace_flags"] = np.asarray(trace_flags)
+    if root_count is not None:
+        extra["root_count"] = np.asarray(root_count)
+    np.savez_compressed(HERE / f"reliability_{name}.npz", velocity=np.asarray(velocity, float),
+                        periods=np.asarray(periods, float), flags=r.flags, assessed=r.assessed,
+                        previous_index=r.previous_index, sorted_order=r.sorted_order,
+                        options=np.array([options.get(k, d) for k, d in RELIABILITY_DEFAULTS]), **extra)
+    print(f"reliability_{name}: {int((r.flags != 0).sum())} flagged of {r.flags.size}")
+
+
+# option names and the reference's defaults, in the order stored in the fixtures
+RELIABILITY_DEFAULTS = (("close_root_rtol", .005), ("max_relative_step", .1), ("prediction_rtol", .05),
+                        ("max_log_period_gap", .25))
+
+
+def save_reliability_cases(reference: Path):
+    rel = load_reference_reliability(reference)
+    # the reference test suite's cases (tests/test_reliability.py)
+    save_reliability_case(rel, "sort_dup_gap", np.array([[[1.02, 1., 1.01, 1.01, 1.2], [2.02, 2., 2.01, 2.01, 2.2]]]),
+                          np.array([1.2, 1., 1.1, 1.1, 4.]))
+    bad = np.array([[[1.02, 1., 1.01, 1.01 + 1e-4, 1.2], [2.02, 2., 2.01, 2.01, 2.2]]])
+    save_reliability_case(rel, "dup_mismatch", bad, np.array([1.2, 1., 1.1, 1.1, 4.]))
+    save_reliability_case(rel, "birth_rank_failure", np.array([[[1., 1.3, 1.8], [1.4, 1.8, np.nan], [2., 2.05, 2.1]]]),
+                          np.array([1., 1.1, 1.2]), trace_flags=np.array([[0, 4096, 4]], dtype=np.uint32))
+    p = np.array([1e100, np.nextafter(1e100, np.inf), np.nextafter(np.nextafter(1e100, np.inf), np.inf)])
+    save_reliability_case(rel, "adjacent_periods", np.ones((1, 1, 3)), p)
+    # seeded synthetic batches
+    v, p, tf, counts = synthetic_reliability(workloads.SEED + 21, 40, 6, 25)
+    save_reliability_case(rel, "synthetic_full", v, p, trace_flags=tf, root_count=counts)
+    save_reliability_case(rel, "synthetic_plain", v, p)
+    save_reliability_case(rel, "synthetic_options", v, p, trace_flags=tf, root_count=counts, close_root_rtol=.02,
+                          max_relative_step=.03, prediction_rtol=.01, max_log_period_gap=.5)
+    v1, p1, tf1, c1 = synthetic_reliability(workloads.SEED + 22, 7, 1, 9, duplicates=False)
+    save_reliability_case(rel, "single_mode", v1, p1, trace_flags=tf1, root_count=c1)
+    save_reliability_case(rel, "single_period", v[:, :, :1], p[:1], trace_flags=tf[:, :1], root_count=counts[:, :1])
+    # reference-solver results
+    for case in ("lvz48_rayleigh", "crustal48_love"):
+        f = np.load(HERE / f"ref_{case}.npz")
+        save_reliability_case(rel, case, f["phase_velocity"], f["periods"], trace_flags=f["trace_flags"],
+                              root_count=f["root_count"])
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--only", choices=["reliability"])
     args = ap.parse_args()
+    if args.only == "reliability":
+        save_reliability_cases(Path(args.reference))
+        return
     if oracle.reference() is None:
         raise SystemExit("build the reference CPU engine first: make -C oracle")
     model, periods = workloads.quickstart()
@@ -135,6 +234,7 @@ def main():
     save_jacobian_case("config4_love", subset(c4, np.arange(4, 6)), periods4, nmodes4, 1)
     save_jacobian_case("water_rayleigh", subset(water_models(), np.arange(2)), np.geomspace(0.5, 20., 12), 3, 0)
     repack_reference_fixtures(Path(args.reference))
+    save_reliability_cases(Path(args.reference))
 
 
 if __name__ == "__main__":
