@@ -142,6 +142,12 @@ class DispersionBatch:
         self.status[rejected] = SolveStatus.REJECTED
         self.mode_convention = "ascending roots in the reported search interval"
 
+    @property
+    def auto_relaxed(self):
+        """Traces whose accepted search used a wider automatic sampling tolerance
+        (python/modisp/__init__.py:129-132); None unless accuracy is "auto"."""
+        return (self.trace_flags & TRACE_AUTO_RELAXED) != 0 if self.accuracy == "auto" else None
+
     def check_modes(self, **options):
         """Cross-period mode-reliability checks of this result on the GPU
         (python/modisp/__init__.py:126-127); see modisp_b200.reliability."""
