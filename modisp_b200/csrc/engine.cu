@@ -13,6 +13,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "modisp_b200.h"
@@ -38,6 +39,38 @@ int fail(const std::string &msg) {
       return fail(std::string("modisp_b200 CUDA: ") + cudaGetErrorString(err__) + " (" +  \
                   #call + ")");                                                            \
   } while (0)
+
+// Host copies between pinned staging and the caller's arrays, spread over up to
+// 8 threads: the caller's output arrays are usually fresh (first-touch page
+// faults) and a single core copies them at a fraction of the memory bandwidth.
+struct HostCopy {
+  void *dst;
+  const void *src;
+  size_t bytes;
+};
+void parallel_copy(const std::vector<HostCopy> &jobs) {
+  size_t total = 0;
+  for (const HostCopy &j : jobs) total += j.bytes;
+  const unsigned hw = std::thread::hardware_concurrency();
+  const unsigned nth = static_cast<unsigned>(std::min<size_t>(std::min(8u, hw ? hw : 1u), total >> 21));
+  auto part = [&](size_t lo, size_t hi) {  // byte range [lo, hi) of the jobs laid end to end
+    size_t off = 0;
+    for (const HostCopy &j : jobs) {
+      const size_t a = std::max(lo, off), b = std::min(hi, off + j.bytes);
+      if (a < b) std::memcpy(static_cast<char *>(j.dst) + (a - off), static_cast<const char *>(j.src) + (a - off), b - a);
+      off += j.bytes;
+    }
+  };
+  if (nth <= 1) {
+    part(0, total);
+    return;
+  }
+  std::vector<std::thread> pool;
+  pool.reserve(nth - 1);
+  for (unsigned t = 1; t < nth; ++t) pool.emplace_back(part, total * t / nth, total * (t + 1) / nth);
+  part(0, total / nth);
+  for (std::thread &th : pool) th.join();
+}
 
 template <class T>
 cudaError_t dalloc(T **p, size_t count) {
@@ -521,12 +554,15 @@ int md200_run(md200_engine *e, const double *h, const double *vp, const double *
   // stage inputs through pinned memory
   unsigned char *p = e->pinned;
   double *ph = reinterpret_cast<double *>(p);
-  std::memcpy(ph, h, sizeof(double) * B * L);
-  std::memcpy(ph + B * L, vp, sizeof(double) * B * L);
-  std::memcpy(ph + 2 * B * L, vs, sizeof(double) * B * L);
-  std::memcpy(ph + 3 * B * L, rho, sizeof(double) * B * L);
-  std::memcpy(ph + 4 * B * L, periods, sizeof(double) * T);
-  if (bounds) std::memcpy(ph + 4 * B * L + T, bounds, sizeof(double) * 2 * B);
+  {
+    std::vector<HostCopy> in = {{ph, h, sizeof(double) * B * L},
+                                {ph + B * L, vp, sizeof(double) * B * L},
+                                {ph + 2 * B * L, vs, sizeof(double) * B * L},
+                                {ph + 3 * B * L, rho, sizeof(double) * B * L},
+                                {ph + 4 * B * L, periods, sizeof(double) * T}};
+    if (bounds) in.push_back({ph + 4 * B * L + T, bounds, sizeof(double) * 2 * B});
+    parallel_copy(in);
+  }
   cudaStream_t s = e->stream;
   MD200_CK(cudaMemcpyAsync(e->in_h, ph, sizeof(double) * B * L, cudaMemcpyHostToDevice, s));
   MD200_CK(cudaMemcpyAsync(e->in_vp, ph + B * L, sizeof(double) * B * L, cudaMemcpyHostToDevice, s));
@@ -587,16 +623,17 @@ int md200_run(md200_engine *e, const double *h, const double *vp, const double *
     MD200_CK(cudaEventSynchronize(e->chunk_ev[c]));
     const size_t b0 = chunk_begin(c), nb = chunk_begin(c + 1) - b0;
     const size_t cm = b0 * nm * T, ct = b0 * T, cells = nb * nm * T, traces = nb * T;
-    std::memcpy(velocity + cm, ov + cm, sizeof(double) * cells);
-    std::memcpy(flags + ct, ofl + ct, sizeof(unsigned) * traces);
-    std::memcpy(levels + ct, olv + ct, sizeof(int) * traces);
-    std::memcpy(counts + ct, oct + ct, sizeof(int) * traces);
+    std::vector<HostCopy> out = {{velocity + cm, ov + cm, sizeof(double) * cells},
+                                 {flags + ct, ofl + ct, sizeof(unsigned) * traces},
+                                 {levels + ct, olv + ct, sizeof(int) * traces},
+                                 {counts + ct, oct + ct, sizeof(int) * traces}};
     if (grp) {
-      std::memcpy(group + cm, og + cm, sizeof(double) * cells);
-      std::memcpy(group_flags + cm, ogf + cm, sizeof(unsigned) * cells);
+      out.push_back({group + cm, og + cm, sizeof(double) * cells});
+      out.push_back({group_flags + cm, ogf + cm, sizeof(unsigned) * cells});
     }
-    if (prediction_flags) std::memcpy(prediction_flags + ct, opr + ct, sizeof(unsigned) * traces);
-    if (bounds_out) std::memcpy(bounds_out + 2 * b0, obd + 2 * b0, sizeof(double) * 2 * nb);
+    if (prediction_flags) out.push_back({prediction_flags + ct, opr + ct, sizeof(unsigned) * traces});
+    if (bounds_out) out.push_back({bounds_out + 2 * b0, obd + 2 * b0, sizeof(double) * 2 * nb});
+    parallel_copy(out);
   }
   MD200_CK(cudaStreamSynchronize(s));
   if (stats && nstats > 0) {

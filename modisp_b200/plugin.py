@@ -14,6 +14,9 @@ missing engine library raises BackendUnavailableError on load.
 """
 from __future__ import annotations
 
+import threading
+from concurrent.futures import ThreadPoolExecutor
+
 import numpy as np
 
 from . import _native
@@ -80,6 +83,28 @@ def _review_groups(packed, layers, modes, wave, secular, period, lo, hi, rtol, c
     group, flags = _native.group_roots(h, vp, vs, rho, int(wave), float(period), roots, modes,
                                        float(close_rtol))
     return group, flags, int(np.count_nonzero(flags == 0))
+
+
+_cast_pool = None
+_cast_lock = threading.Lock()
+
+
+def _to_float32(a):
+    """float32 copy of a float64 array (the reference's FP32-mode output type),
+    converted in slices on 8 threads for large arrays: numpy releases the GIL
+    while casting, and the rounding is the same as astype's."""
+    global _cast_pool
+    if a.size < 1 << 20:
+        return a.astype(np.float32)
+    with _cast_lock:
+        if _cast_pool is None:
+            _cast_pool = ThreadPoolExecutor(8, thread_name_prefix="md200-cast")
+    out = np.empty(a.shape, np.float32)
+    src, dst = a.reshape(-1), out.reshape(-1)
+    step = -(-src.size // 8)
+    list(_cast_pool.map(lambda i: np.copyto(dst[i * step:(i + 1) * step], src[i * step:(i + 1) * step],
+                                            casting="same_kind"), range(8)))
+    return out
 
 
 class QeSolver:
@@ -167,7 +192,7 @@ class QeSolver:
                 raise ValueError("periods must be a 1-D array of the engine's period count")
             out = self._engine.run(h, *arrays, per, bnd, c_tol_rel, f_accept, int(wave),
                                    group=self.group_velocity, prediction=self.continuation)
-        velocity = out["velocity"].astype(np.float32) if self.single_precision else out["velocity"]
+        velocity = _to_float32(out["velocity"]) if self.single_precision else out["velocity"]
         stats = dict(out["stats"])
         stats.update(strategy="b200_scan", capacity=self.capacity)
         extras = dict(group_velocity=out.get("group_velocity"),
