@@ -4,7 +4,6 @@ Tests marked ``gpu`` need an sm_100 GPU and the built engine library; everything
 else runs on the CPU.  The oracle (``oracle/``) is the checker: the C
 restatement and, where built, the reference CPU engine in ``oracle/_ref``.
 """
-import os
 import sys
 from pathlib import Path
 
@@ -13,7 +12,6 @@ import pytest
 
 ROOT = Path(__file__).resolve().parents[1]
 GOLDEN = Path(__file__).resolve().parent / "golden"
-REFERENCE = Path(os.environ.get("MODISP_REFERENCE", "/root/reference"))
 if str(ROOT) not in sys.path:
     sys.path.insert(0, str(ROOT))
 
