@@ -104,7 +104,6 @@ struct md200_engine {
   int *rg_offsets = nullptr, *rg_modes = nullptr;
   long long *rg_outbase = nullptr;
   double *rg_periods = nullptr;
-  int jac_blocks = 0;
   std::vector<void *> owned;
   // host-path pipelining: one event per chunk of models
   static constexpr int MAX_CHUNKS = 8;
@@ -415,14 +414,12 @@ int jacobian_enqueue(md200_engine *e, const double *h, const double *vp, const d
   prep_models<<<(B + pw - 1) / pw, 32 * pw, e->prep_smem, s>>>(d, e->sortcap, 0);
   MD200_CK(cudaGetLastError());
   if (grad) MD200_CK(cudaMemsetAsync(grad, 0, sizeof(double) * 4 * static_cast<size_t>(B) * e->L, s));
-  if (!e->jac_blocks) {
-    int sms = 148, occ = 0;
-    MD200_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device));
-    MD200_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, root_jacobians<0>, 128, 0));
-    e->jac_blocks = sms * std::max(1, occ);
-  }
+  // One thread per output cell.  Most cells hold no root and their warps leave at
+  // once; the block scheduler then keeps every SM on root-bearing warps.  A grid
+  // capped at the resident blocks (each thread striding over many cells) left
+  // threads with uneven shares and ran 3.2x slower.
   const long long cells = static_cast<long long>(B) * e->nmodes * e->T;
-  const int blocks = static_cast<int>(std::min<long long>(e->jac_blocks, (cells + 127) / 128));
+  const int blocks = static_cast<int>(std::min<long long>((cells + 127) / 128, 1LL << 30));
   if (wave == 0) root_jacobians<0><<<blocks, 128, 0, s>>>(d, vel, grp, jc, ju, wc, wu, grad, d.ctr + C_JFAIL);
   else root_jacobians<1><<<blocks, 128, 0, s>>>(d, vel, grp, jc, ju, wc, wu, grad, d.ctr + C_JFAIL);
   MD200_CK(cudaGetLastError());
