@@ -273,3 +273,34 @@ def test_engines_agree_on_group_velocity_where_it_is_ill_conditioned(wave):
         if np.isfinite(u):
             worst.append(abs(u64[b, k, f] - u) / u)
     assert worst and max(worst) <= GROUP_RTOL, max(worst)
+
+
+@pytest.mark.parametrize("wave", [0, 1])
+def test_full_config3_batch_engines_agree(wave):
+    """The whole 100,000-model mixed-precision batch (30 % low-velocity layers, 60
+    periods, 5 modes): the FP32-scan engine and the plain FP64 engine, whose roots
+    match the reference on every sampled batch, agree on every mode mask and root
+    count, and on phase and group velocity to the parity tolerance -- a property
+    that holds at any batch size, checked here at the full one."""
+    from modisp_b200 import _native, workloads
+    batch, periods, nmodes = workloads.config3()
+    B, L = batch["thickness"].shape
+    out = {}
+    for single in (1, 0):
+        o = _native.default_options()
+        o.single_precision, o.group_velocity = single, 1
+        eng = _native.Engine(0, B, L, periods.size, nmodes, o)
+        try:
+            out[single] = eng.run(batch["thickness"], batch["vp"], batch["vs"], batch["rho"], periods, None, 1e-10, 1.,
+                                  wave, group=True)
+        finally:
+            eng.close()
+    a, b = out[1], out[0]
+    np.testing.assert_array_equal(np.isfinite(a["velocity"]), np.isfinite(b["velocity"]))
+    np.testing.assert_array_equal(a["counts"], b["counts"])
+    m = np.isfinite(b["velocity"])
+    assert m.sum() > 2_000_000
+    assert np.max(np.abs(a["velocity"][m] - b["velocity"][m]) / b["velocity"][m]) <= PHASE_RTOL
+    g = np.isfinite(a["group_velocity"]) & np.isfinite(b["group_velocity"])
+    np.testing.assert_array_equal(np.isfinite(a["group_velocity"]), np.isfinite(b["group_velocity"]))
+    assert np.max(np.abs(a["group_velocity"][g] - b["group_velocity"][g]) / b["group_velocity"][g]) <= GROUP_RTOL
