@@ -1114,8 +1114,17 @@ int md200_mode_reliability_planned(const double *velocity, const uint32_t *trace
   ReliabilityArgs r{velocity, trace_flags, root_count, plan, order, B, K, T, close_root_rtol, max_relative_step,
                     prediction_rtol, flags, assessed};
   const size_t n = static_cast<size_t>(B) * T;
-  mode_reliability<<<static_cast<unsigned>((n + 255) / 256), 256, 0,
-                     stream ? static_cast<cudaStream_t>(stream) : cudaStreamLegacy>>>(r);
+  const unsigned grid = static_cast<unsigned>((n + 255) / 256);
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : cudaStreamLegacy;
+  switch (K) {  // the roots of a trace in registers, loops unrolled to the exact K
+#define MD200_RELIABILITY_CASE(KK) \
+  case KK: mode_reliability_small<KK><<<grid, 256, 0, s>>>(r); break;
+    MD200_RELIABILITY_CASE(1) MD200_RELIABILITY_CASE(2) MD200_RELIABILITY_CASE(3) MD200_RELIABILITY_CASE(4)
+    MD200_RELIABILITY_CASE(5) MD200_RELIABILITY_CASE(6) MD200_RELIABILITY_CASE(7) MD200_RELIABILITY_CASE(8)
+    MD200_RELIABILITY_CASE(9) MD200_RELIABILITY_CASE(10) MD200_RELIABILITY_CASE(11) MD200_RELIABILITY_CASE(12)
+#undef MD200_RELIABILITY_CASE
+    default: mode_reliability<<<grid, 256, 0, s>>>(r);
+  }
   MD200_CK(cudaGetLastError());
   return 0;
 }

@@ -164,4 +164,130 @@ __global__ void mode_reliability(ReliabilityArgs r) {
   }
 }
 
+// The same checks with a trace's roots at t, prev and older held in registers,
+// for a mode count fixed at compile time (KM = K; loops unrolled exactly): the
+// kernel above reloads them from L1 in every rank comparison and is
+// issue-bound.  Same arithmetic, same flags.
+template <int KM>
+__global__ void __launch_bounds__(256) mode_reliability_small(ReliabilityArgs r) {
+  const size_t gid = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (gid >= static_cast<size_t>(r.B) * r.T) return;
+  const int b = static_cast<int>(gid / r.T), t = static_cast<int>(gid - static_cast<size_t>(b) * r.T);
+  const int K = r.K, T = r.T;
+  const double *vb = r.v + static_cast<size_t>(b) * K * T;
+  const md200_period_plan pl = r.plan[t];
+  const bool first = (pl.kind & MD200_PLAN_FIRST) != 0, dup = (pl.kind & MD200_PLAN_DUPLICATE) != 0;
+  const bool predict = (pl.kind & MD200_PLAN_PREDICT) != 0;
+  const int prev = first ? t : pl.prev, older = predict ? pl.older : t;
+  double x[KM], a[KM], o[KM];
+  int nx = 0, na = 0;
+#pragma unroll
+  for (int k = 0; k < KM; ++k) {
+    x[k] = a[k] = o[k] = NAN;
+    if (k < K) {
+      x[k] = vb[static_cast<size_t>(k) * T + t];
+      a[k] = vb[static_cast<size_t>(k) * T + prev];
+      if (predict) o[k] = vb[static_cast<size_t>(k) * T + older];
+      nx += isfinite(x[k]);
+      na += isfinite(a[k]);
+    }
+  }
+  const uint32_t tf = r.tflags ? r.tflags[static_cast<size_t>(b) * T + t] : 0u;
+  const int64_t cnt = r.counts ? r.counts[static_cast<size_t>(b) * T + t] : nx;
+  const bool fail = (tf & RF_FAILURE_TRACE_BITS) != 0 || cnt < 0;
+  bool fail_prev = false, changed = false;
+  if (!first) {
+    const uint32_t tfp = r.tflags ? r.tflags[static_cast<size_t>(b) * T + prev] : 0u;
+    const int64_t cntp = r.counts ? r.counts[static_cast<size_t>(b) * T + prev] : na;
+    fail_prev = (tfp & RF_FAILURE_TRACE_BITS) != 0 || cntp < 0;
+    changed = cntp != cnt;
+#pragma unroll
+    for (int k = 0; k < KM; ++k)
+      if (k < K && isfinite(a[k]) != isfinite(x[k])) changed = true;
+  }
+  uint32_t f[KM];
+  bool as[KM];
+#pragma unroll
+  for (int k = 0; k < KM; ++k) {
+    f[k] = 0;
+    as[k] = false;
+    if (k >= K) continue;
+    const bool fx = isfinite(x[k]);
+    if (!fx) f[k] |= RF_NONFINITE;
+    if (fail) f[k] |= RF_NUMERICAL_FAILURE;
+    if (tf & RF_UNCERTAIN_TRACE_BITS) f[k] |= RF_SEARCH_UNCERTAIN;
+    if (k + 1 < K) {
+      const double gap = __dsub_rn(x[k + 1], x[k]);
+      if (isfinite(gap)) {
+        if (gap <= __dmul_rn(r.close_rtol, x[k + 1])) f[k] |= RF_CLOSE_ROOT;
+        if (gap <= 0.) f[k] |= RF_RANK_AMBIGUOUS;
+      }
+    }
+    if (k > 0) {
+      const double gap = __dsub_rn(x[k], x[k - 1]);
+      if (isfinite(gap)) {
+        if (gap <= __dmul_rn(r.close_rtol, x[k])) f[k] |= RF_CLOSE_ROOT;
+        if (gap <= 0.) f[k] |= RF_RANK_AMBIGUOUS;
+      }
+    }
+    if (first) {
+      f[k] |= RF_UNASSESSED;
+    } else {
+      const bool both = isfinite(a[k]) && fx;
+      if (changed) f[k] |= RF_ROOT_COUNT_CHANGE;
+      if (dup) {
+        if (dup_mismatch(a[k], x[k])) f[k] |= RF_DUPLICATE_MISMATCH;
+        as[k] = both && !fail && !fail_prev;
+      } else {
+        if (pl.kind & MD200_PLAN_GAP) f[k] |= RF_PERIOD_GAP;
+        else as[k] = both && !fail && !fail_prev;
+        if (both && __ddiv_rn(fabs(__dsub_rn(x[k], a[k])), fmax(a[k], x[k])) > r.max_step) f[k] |= RF_STEP_JUMP;
+        if (predict && both && isfinite(o[k])) {
+          const double predicted = __dadd_rn(a[k], __dmul_rn(__dsub_rn(a[k], o[k]), pl.ratio));
+          if (fabs(__dsub_rn(x[k], predicted)) > __dmul_rn(r.pred_rtol, x[k])) f[k] |= RF_PREDICTION_MISMATCH;
+        }
+      }
+    }
+  }
+  if (!dup)
+    for (int q = pl.dup_begin; q < pl.dup_end; ++q) {
+      const int td = r.order[q];
+#pragma unroll
+      for (int k = 0; k < KM; ++k)
+        if (k < K && dup_mismatch(x[k], vb[static_cast<size_t>(k) * T + td])) f[k] |= RF_DUPLICATE_MISMATCH;
+    }
+  if (!first && !dup && na > 0) {
+    // nearest-rank agreement (first minimum on ties, as numpy's argmin)
+#pragma unroll
+    for (int j = 0; j < KM; ++j) {
+      if (j >= K || !isfinite(x[j])) continue;
+      int ibest = -1;
+      double cbest = 0., abest = 0.;
+#pragma unroll
+      for (int i = 0; i < KM; ++i) {
+        if (i >= K || !isfinite(a[i])) continue;
+        const double cost = fabs(__dsub_rn(a[i], x[j]));
+        if (ibest < 0 || cost < cbest) { ibest = i; cbest = cost; abest = a[i]; }
+      }
+      int jbest = -1;
+      double dbest = 0.;
+#pragma unroll
+      for (int q = 0; q < KM; ++q) {
+        if (q >= K || !isfinite(x[q])) continue;
+        const double cost = fabs(__dsub_rn(abest, x[q]));
+        if (jbest < 0 || cost < dbest) { jbest = q; dbest = cost; }
+      }
+      if (ibest != j || jbest != j) f[j] |= RF_RANK_AMBIGUOUS;
+    }
+  }
+  uint16_t *fb = r.flags + static_cast<size_t>(b) * K * T;
+  uint8_t *ab = r.assessed + static_cast<size_t>(b) * K * T;
+#pragma unroll
+  for (int k = 0; k < KM; ++k)
+    if (k < K) {
+      fb[static_cast<size_t>(k) * T + t] = static_cast<uint16_t>(f[k]);
+      ab[static_cast<size_t>(k) * T + t] = as[k];
+    }
+}
+
 }  // namespace md200
