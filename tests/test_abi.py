@@ -155,3 +155,27 @@ def test_autotuner_picks_the_fastest_shape_and_caches_it(tmp_path, monkeypatch):
 
     with pytest.raises(RuntimeError, match="changed"):
         autotune.autotune(sample, [1., 2., 3.], 3, 0, True, timer=bad_timer, use_cache=False)
+
+
+def test_header_compiles_as_c_and_plan_layout_matches(tmp_path):
+    """The C ABI header is plain C99, and md200_period_plan has the field offsets
+    and size of the numpy dtype the Python layer fills."""
+    import shutil
+    import subprocess
+    from modisp_b200 import _native
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    src = tmp_path / "layout.c"
+    src.write_text('#include <stddef.h>\n#include <stdio.h>\n#include "modisp_b200.h"\n'
+                   'int main(void) { printf("%zu %zu %zu %zu %zu %zu\\n", sizeof(md200_period_plan), '
+                   'offsetof(md200_period_plan, older), offsetof(md200_period_plan, kind), '
+                   'offsetof(md200_period_plan, dup_begin), offsetof(md200_period_plan, dup_end), '
+                   'offsetof(md200_period_plan, ratio)); return 0; }\n')
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-std=c99", "-Wall", "-Werror", "-pedantic", f"-I{ROOT / 'include'}", str(src), "-o",
+                    str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+    dt = _native.PERIOD_PLAN
+    assert got == [dt.itemsize, dt.fields["older"][1], dt.fields["kind"][1], dt.fields["dup_begin"][1],
+                   dt.fields["dup_end"][1], dt.fields["ratio"][1]]
