@@ -66,9 +66,14 @@ void parallel_copy(const std::vector<HostCopy> &jobs) {
     return;
   }
   std::vector<std::thread> pool;
-  pool.reserve(nth - 1);
-  for (unsigned t = 1; t < nth; ++t) pool.emplace_back(part, total * t / nth, total * (t + 1) / nth);
+  unsigned started = 1;
+  try {  // no exception may leave a C entry point: ranges without a thread are copied here
+    pool.reserve(nth - 1);
+    for (; started < nth; ++started) pool.emplace_back(part, total * started / nth, total * (started + 1) / nth);
+  } catch (...) {
+  }
   part(0, total / nth);
+  for (unsigned t = started; t < nth; ++t) part(total * t / nth, total * (t + 1) / nth);
   for (std::thread &th : pool) th.join();
 }
 
