@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <exception>
 #include <cmath>
 #include <mutex>
 #include <cstdio>
@@ -29,6 +30,21 @@ thread_local std::string g_error;
 
 int fail(const std::string &msg) {
   g_error = msg;
+  return 1;
+}
+
+// An exception caught at a C entry point (host allocation failure or a thread
+// that could not start) becomes an error status: none may cross the C ABI.
+int fail_exception() {
+  try {
+    throw;
+  } catch (const std::bad_alloc &) {
+    g_error = "modisp_b200: out of host memory";
+  } catch (const std::exception &ex) {
+    g_error = std::string("modisp_b200: ") + ex.what();
+  } catch (...) {
+    g_error = "modisp_b200: internal error";
+  }
   return 1;
 }
 
@@ -546,107 +562,111 @@ int md200_run(md200_engine *e, const double *h, const double *vp, const double *
               double tol, double accept, int wave, double *velocity, unsigned *flags, int *levels,
               int *counts, double *group, unsigned *group_flags, unsigned *prediction_flags,
               double *bounds_out, unsigned long long *stats, int nstats) {
-  if (validate_geometry(e, models)) return 1;
-  if (!h || !vp || !vs || !rho || !periods || !velocity || !flags || !levels || !counts)
-    return fail("modisp_b200: missing input or output array");
-  if (e->d.group && (!group || !group_flags))
-    return fail("modisp_b200: group-velocity engine needs group output arrays");
-  MD200_CK(cudaSetDevice(e->device));
-  const size_t B = models, L = e->L, T = e->T, nm = e->nmodes, nt = B * T;
-  // stage inputs through pinned memory
-  unsigned char *p = e->pinned;
-  double *ph = reinterpret_cast<double *>(p);
-  {
-    std::vector<HostCopy> in = {{ph, h, sizeof(double) * B * L},
-                                {ph + B * L, vp, sizeof(double) * B * L},
-                                {ph + 2 * B * L, vs, sizeof(double) * B * L},
-                                {ph + 3 * B * L, rho, sizeof(double) * B * L},
-                                {ph + 4 * B * L, periods, sizeof(double) * T}};
-    if (bounds) in.push_back({ph + 4 * B * L + T, bounds, sizeof(double) * 2 * B});
-    parallel_copy(in);
-  }
-  cudaStream_t s = e->stream;
-  MD200_CK(cudaMemcpyAsync(e->in_h, ph, sizeof(double) * B * L, cudaMemcpyHostToDevice, s));
-  MD200_CK(cudaMemcpyAsync(e->in_vp, ph + B * L, sizeof(double) * B * L, cudaMemcpyHostToDevice, s));
-  MD200_CK(cudaMemcpyAsync(e->in_vs, ph + 2 * B * L, sizeof(double) * B * L, cudaMemcpyHostToDevice, s));
-  MD200_CK(cudaMemcpyAsync(e->in_rho, ph + 3 * B * L, sizeof(double) * B * L, cudaMemcpyHostToDevice, s));
-  MD200_CK(cudaMemcpyAsync(e->in_per, ph + 4 * B * L, sizeof(double) * T, cudaMemcpyHostToDevice, s));
-  if (bounds)
-    MD200_CK(cudaMemcpyAsync(e->in_bounds, ph + 4 * B * L + T, sizeof(double) * 2 * B,
-                             cudaMemcpyHostToDevice, s));
-  const bool grp = e->d.group != 0;
-  // Large batches run in chunks of models, every chunk's outputs copied back as
-  // soon as it is solved, so the host copies (and first-touch page faults) of
-  // chunk i overlap the solve of chunk i + 1.  Every trace is independent: the
-  // results are those of one run.
-  // (each chunk adds a scan tail, so only batches far larger than the GPU's
-  // resident traces are split)
-  const int nchunk = B >= 65536 ? 4 : 1;
-  double *ov = reinterpret_cast<double *>(p);
-  double *og = ov + nt * nm;
-  unsigned *ogf = reinterpret_cast<unsigned *>(og + nt * nm);
-  unsigned *ofl = ogf + nt * nm;
-  int *olv = reinterpret_cast<int *>(ofl + nt);
-  int *oct = olv + nt;
-  unsigned *opr = reinterpret_cast<unsigned *>(oct + nt);
-  unsigned long long *ost = reinterpret_cast<unsigned long long *>(
-      (reinterpret_cast<uintptr_t>(opr + nt) + 7) & ~uintptr_t(7));
-  double *obd = reinterpret_cast<double *>(ost + static_cast<size_t>(MD200_STAT_COUNT) * md200_engine::MAX_CHUNKS);
-  auto chunk_begin = [&](int c) { return B * c / nchunk; };
-  for (int c = 0; c < nchunk; ++c) {
-    const size_t b0 = chunk_begin(c), nb = chunk_begin(c + 1) - b0;
-    const size_t cm = b0 * nm * T, ct = b0 * T, cells = nb * nm * T, traces = nb * T;
-    unsigned long long *cstats = e->d_stats + static_cast<size_t>(c) * MD200_STAT_COUNT;
-    if (enqueue(e, e->in_h + b0 * L, e->in_vp + b0 * L, e->in_vs + b0 * L, e->in_rho + b0 * L,
-                static_cast<int>(nb), e->in_per, bounds ? e->in_bounds + 2 * b0 : nullptr, tol, accept, wave,
-                e->out_vel + cm, e->out_flags + ct, e->out_levels + ct, e->out_counts + ct,
-                grp ? e->out_grp + cm : nullptr, grp ? e->out_gflags + cm : nullptr,
-                prediction_flags ? e->out_pred + ct : nullptr, e->in_bounds + 2 * b0, cstats, s))
-      return 1;
-    MD200_CK(cudaMemcpyAsync(ov + cm, e->out_vel + cm, sizeof(double) * cells, cudaMemcpyDeviceToHost, s));
-    MD200_CK(cudaMemcpyAsync(ofl + ct, e->out_flags + ct, sizeof(unsigned) * traces, cudaMemcpyDeviceToHost, s));
-    MD200_CK(cudaMemcpyAsync(olv + ct, e->out_levels + ct, sizeof(int) * traces, cudaMemcpyDeviceToHost, s));
-    MD200_CK(cudaMemcpyAsync(oct + ct, e->out_counts + ct, sizeof(int) * traces, cudaMemcpyDeviceToHost, s));
-    if (grp) {
-      MD200_CK(cudaMemcpyAsync(og + cm, e->out_grp + cm, sizeof(double) * cells, cudaMemcpyDeviceToHost, s));
-      MD200_CK(cudaMemcpyAsync(ogf + cm, e->out_gflags + cm, sizeof(unsigned) * cells, cudaMemcpyDeviceToHost, s));
+  try {
+    if (validate_geometry(e, models)) return 1;
+    if (!h || !vp || !vs || !rho || !periods || !velocity || !flags || !levels || !counts)
+      return fail("modisp_b200: missing input or output array");
+    if (e->d.group && (!group || !group_flags))
+      return fail("modisp_b200: group-velocity engine needs group output arrays");
+    MD200_CK(cudaSetDevice(e->device));
+    const size_t B = models, L = e->L, T = e->T, nm = e->nmodes, nt = B * T;
+    // stage inputs through pinned memory
+    unsigned char *p = e->pinned;
+    double *ph = reinterpret_cast<double *>(p);
+    {
+      std::vector<HostCopy> in = {{ph, h, sizeof(double) * B * L},
+                                  {ph + B * L, vp, sizeof(double) * B * L},
+                                  {ph + 2 * B * L, vs, sizeof(double) * B * L},
+                                  {ph + 3 * B * L, rho, sizeof(double) * B * L},
+                                  {ph + 4 * B * L, periods, sizeof(double) * T}};
+      if (bounds) in.push_back({ph + 4 * B * L + T, bounds, sizeof(double) * 2 * B});
+      parallel_copy(in);
     }
-    if (prediction_flags)
-      MD200_CK(cudaMemcpyAsync(opr + ct, e->out_pred + ct, sizeof(unsigned) * traces, cudaMemcpyDeviceToHost, s));
-    // the prep stage wrote the windows it used over the (already consumed) input windows
-    if (bounds_out)
-      MD200_CK(cudaMemcpyAsync(obd + 2 * b0, e->in_bounds + 2 * b0, sizeof(double) * 2 * nb,
-                               cudaMemcpyDeviceToHost, s));
-    MD200_CK(cudaEventRecord(e->chunk_ev[c], s));
-  }
-  MD200_CK(cudaMemcpyAsync(ost, e->d_stats, sizeof(unsigned long long) * MD200_STAT_COUNT * nchunk,
-                           cudaMemcpyDeviceToHost, s));
-  for (int c = 0; c < nchunk; ++c) {
-    MD200_CK(cudaEventSynchronize(e->chunk_ev[c]));
-    const size_t b0 = chunk_begin(c), nb = chunk_begin(c + 1) - b0;
-    const size_t cm = b0 * nm * T, ct = b0 * T, cells = nb * nm * T, traces = nb * T;
-    std::vector<HostCopy> out = {{velocity + cm, ov + cm, sizeof(double) * cells},
-                                 {flags + ct, ofl + ct, sizeof(unsigned) * traces},
-                                 {levels + ct, olv + ct, sizeof(int) * traces},
-                                 {counts + ct, oct + ct, sizeof(int) * traces}};
-    if (grp) {
-      out.push_back({group + cm, og + cm, sizeof(double) * cells});
-      out.push_back({group_flags + cm, ogf + cm, sizeof(unsigned) * cells});
+    cudaStream_t s = e->stream;
+    MD200_CK(cudaMemcpyAsync(e->in_h, ph, sizeof(double) * B * L, cudaMemcpyHostToDevice, s));
+    MD200_CK(cudaMemcpyAsync(e->in_vp, ph + B * L, sizeof(double) * B * L, cudaMemcpyHostToDevice, s));
+    MD200_CK(cudaMemcpyAsync(e->in_vs, ph + 2 * B * L, sizeof(double) * B * L, cudaMemcpyHostToDevice, s));
+    MD200_CK(cudaMemcpyAsync(e->in_rho, ph + 3 * B * L, sizeof(double) * B * L, cudaMemcpyHostToDevice, s));
+    MD200_CK(cudaMemcpyAsync(e->in_per, ph + 4 * B * L, sizeof(double) * T, cudaMemcpyHostToDevice, s));
+    if (bounds)
+      MD200_CK(cudaMemcpyAsync(e->in_bounds, ph + 4 * B * L + T, sizeof(double) * 2 * B,
+                               cudaMemcpyHostToDevice, s));
+    const bool grp = e->d.group != 0;
+    // Large batches run in chunks of models, every chunk's outputs copied back as
+    // soon as it is solved, so the host copies (and first-touch page faults) of
+    // chunk i overlap the solve of chunk i + 1.  Every trace is independent: the
+    // results are those of one run.
+    // (each chunk adds a scan tail, so only batches far larger than the GPU's
+    // resident traces are split)
+    const int nchunk = B >= 65536 ? 4 : 1;
+    double *ov = reinterpret_cast<double *>(p);
+    double *og = ov + nt * nm;
+    unsigned *ogf = reinterpret_cast<unsigned *>(og + nt * nm);
+    unsigned *ofl = ogf + nt * nm;
+    int *olv = reinterpret_cast<int *>(ofl + nt);
+    int *oct = olv + nt;
+    unsigned *opr = reinterpret_cast<unsigned *>(oct + nt);
+    unsigned long long *ost = reinterpret_cast<unsigned long long *>(
+        (reinterpret_cast<uintptr_t>(opr + nt) + 7) & ~uintptr_t(7));
+    double *obd = reinterpret_cast<double *>(ost + static_cast<size_t>(MD200_STAT_COUNT) * md200_engine::MAX_CHUNKS);
+    auto chunk_begin = [&](int c) { return B * c / nchunk; };
+    for (int c = 0; c < nchunk; ++c) {
+      const size_t b0 = chunk_begin(c), nb = chunk_begin(c + 1) - b0;
+      const size_t cm = b0 * nm * T, ct = b0 * T, cells = nb * nm * T, traces = nb * T;
+      unsigned long long *cstats = e->d_stats + static_cast<size_t>(c) * MD200_STAT_COUNT;
+      if (enqueue(e, e->in_h + b0 * L, e->in_vp + b0 * L, e->in_vs + b0 * L, e->in_rho + b0 * L,
+                  static_cast<int>(nb), e->in_per, bounds ? e->in_bounds + 2 * b0 : nullptr, tol, accept, wave,
+                  e->out_vel + cm, e->out_flags + ct, e->out_levels + ct, e->out_counts + ct,
+                  grp ? e->out_grp + cm : nullptr, grp ? e->out_gflags + cm : nullptr,
+                  prediction_flags ? e->out_pred + ct : nullptr, e->in_bounds + 2 * b0, cstats, s))
+        return 1;
+      MD200_CK(cudaMemcpyAsync(ov + cm, e->out_vel + cm, sizeof(double) * cells, cudaMemcpyDeviceToHost, s));
+      MD200_CK(cudaMemcpyAsync(ofl + ct, e->out_flags + ct, sizeof(unsigned) * traces, cudaMemcpyDeviceToHost, s));
+      MD200_CK(cudaMemcpyAsync(olv + ct, e->out_levels + ct, sizeof(int) * traces, cudaMemcpyDeviceToHost, s));
+      MD200_CK(cudaMemcpyAsync(oct + ct, e->out_counts + ct, sizeof(int) * traces, cudaMemcpyDeviceToHost, s));
+      if (grp) {
+        MD200_CK(cudaMemcpyAsync(og + cm, e->out_grp + cm, sizeof(double) * cells, cudaMemcpyDeviceToHost, s));
+        MD200_CK(cudaMemcpyAsync(ogf + cm, e->out_gflags + cm, sizeof(unsigned) * cells, cudaMemcpyDeviceToHost, s));
+      }
+      if (prediction_flags)
+        MD200_CK(cudaMemcpyAsync(opr + ct, e->out_pred + ct, sizeof(unsigned) * traces, cudaMemcpyDeviceToHost, s));
+      // the prep stage wrote the windows it used over the (already consumed) input windows
+      if (bounds_out)
+        MD200_CK(cudaMemcpyAsync(obd + 2 * b0, e->in_bounds + 2 * b0, sizeof(double) * 2 * nb,
+                                 cudaMemcpyDeviceToHost, s));
+      MD200_CK(cudaEventRecord(e->chunk_ev[c], s));
     }
-    if (prediction_flags) out.push_back({prediction_flags + ct, opr + ct, sizeof(unsigned) * traces});
-    if (bounds_out) out.push_back({bounds_out + 2 * b0, obd + 2 * b0, sizeof(double) * 2 * nb});
-    parallel_copy(out);
-  }
-  MD200_CK(cudaStreamSynchronize(s));
-  if (stats && nstats > 0) {
-    const int n = std::min(nstats, int(MD200_STAT_COUNT));
-    for (int i = 0; i < n; ++i) {
-      unsigned long long sum = 0;
-      for (int c = 0; c < nchunk; ++c) sum += ost[static_cast<size_t>(c) * MD200_STAT_COUNT + i];
-      stats[i] = sum;
+    MD200_CK(cudaMemcpyAsync(ost, e->d_stats, sizeof(unsigned long long) * MD200_STAT_COUNT * nchunk,
+                             cudaMemcpyDeviceToHost, s));
+    for (int c = 0; c < nchunk; ++c) {
+      MD200_CK(cudaEventSynchronize(e->chunk_ev[c]));
+      const size_t b0 = chunk_begin(c), nb = chunk_begin(c + 1) - b0;
+      const size_t cm = b0 * nm * T, ct = b0 * T, cells = nb * nm * T, traces = nb * T;
+      std::vector<HostCopy> out = {{velocity + cm, ov + cm, sizeof(double) * cells},
+                                   {flags + ct, ofl + ct, sizeof(unsigned) * traces},
+                                   {levels + ct, olv + ct, sizeof(int) * traces},
+                                   {counts + ct, oct + ct, sizeof(int) * traces}};
+      if (grp) {
+        out.push_back({group + cm, og + cm, sizeof(double) * cells});
+        out.push_back({group_flags + cm, ogf + cm, sizeof(unsigned) * cells});
+      }
+      if (prediction_flags) out.push_back({prediction_flags + ct, opr + ct, sizeof(unsigned) * traces});
+      if (bounds_out) out.push_back({bounds_out + 2 * b0, obd + 2 * b0, sizeof(double) * 2 * nb});
+      parallel_copy(out);
     }
+    MD200_CK(cudaStreamSynchronize(s));
+    if (stats && nstats > 0) {
+      const int n = std::min(nstats, int(MD200_STAT_COUNT));
+      for (int i = 0; i < n; ++i) {
+        unsigned long long sum = 0;
+        for (int c = 0; c < nchunk; ++c) sum += ost[static_cast<size_t>(c) * MD200_STAT_COUNT + i];
+        stats[i] = sum;
+      }
+    }
+    return 0;
+  } catch (...) {
+    return fail_exception();
   }
-  return 0;
 }
 
 int md200_jacobian_device(md200_engine *e, const double *h, const double *vp, const double *vs,
@@ -770,71 +790,75 @@ int md200_run_ragged(md200_engine *e, const double *h, const double *vp, const d
                      int models, const int *period_offsets, const double *periods, const int *modes,
                      const double *bounds, double tol, double accept, int wave, double *velocity, unsigned *flags, int *levels, int *counts,
                      double *group, unsigned *group_flags, unsigned long long *stats, int nstats) {
-  if (validate_geometry(e, models)) return 1;
-  if (!h || !vp || !vs || !rho || !period_offsets || !periods || !modes || !velocity || !flags || !levels ||
-      !counts)
-    return fail("modisp_b200: missing input or output array");
-  if (e->d.group && (!group || !group_flags))
-    return fail("modisp_b200: group-velocity engine needs group output arrays");
-  // the CSR description, checked here (the device path trusts it)
-  if (period_offsets[0] != 0) return fail("modisp_b200: period_offsets[0] must be 0");
-  std::vector<long long> outbase(models);
-  long long cells = 0;
-  for (int b = 0; b < models; ++b) {
-    const int nb = period_offsets[b + 1] - period_offsets[b];
-    if (nb < 0) return fail("modisp_b200: period_offsets must be non-decreasing");
-    if (modes[b] < 1 || modes[b] > e->nmodes)
-      return fail("modisp_b200: modes[" + std::to_string(b) + "] = " + std::to_string(modes[b]) +
-                  " outside 1.." + std::to_string(e->nmodes));
-    outbase[b] = cells;
-    cells += static_cast<long long>(modes[b]) * nb;
+  try {
+    if (validate_geometry(e, models)) return 1;
+    if (!h || !vp || !vs || !rho || !period_offsets || !periods || !modes || !velocity || !flags || !levels ||
+        !counts)
+      return fail("modisp_b200: missing input or output array");
+    if (e->d.group && (!group || !group_flags))
+      return fail("modisp_b200: group-velocity engine needs group output arrays");
+    // the CSR description, checked here (the device path trusts it)
+    if (period_offsets[0] != 0) return fail("modisp_b200: period_offsets[0] must be 0");
+    std::vector<long long> outbase(models);
+    long long cells = 0;
+    for (int b = 0; b < models; ++b) {
+      const int nb = period_offsets[b + 1] - period_offsets[b];
+      if (nb < 0) return fail("modisp_b200: period_offsets must be non-decreasing");
+      if (modes[b] < 1 || modes[b] > e->nmodes)
+        return fail("modisp_b200: modes[" + std::to_string(b) + "] = " + std::to_string(modes[b]) +
+                    " outside 1.." + std::to_string(e->nmodes));
+      outbase[b] = cells;
+      cells += static_cast<long long>(modes[b]) * nb;
+    }
+    const int traces = period_offsets[models];
+    if (traces < 1 || static_cast<long long>(traces) > static_cast<long long>(e->cap) * e->T)
+      return fail("modisp_b200: ragged trace count " + std::to_string(traces) + " outside 1.." +
+                  std::to_string(static_cast<long long>(e->cap) * e->T) + " (capacity x periods)");
+    for (int t = 0; t < traces; ++t)
+      if (!(periods[t] > 0.)) return fail("modisp_b200: periods must be positive");
+    MD200_CK(cudaSetDevice(e->device));
+    const size_t B = models, L = e->L, capt = static_cast<size_t>(e->cap) * e->T;
+    if (lazy_alloc(e, &e->rg_offsets, static_cast<size_t>(e->cap) + 1) || lazy_alloc(e, &e->rg_modes, e->cap) ||
+        lazy_alloc(e, &e->rg_outbase, e->cap) || lazy_alloc(e, &e->rg_periods, capt))
+      return 1;
+    cudaStream_t s = e->stream;
+    MD200_CK(cudaStreamSynchronize(s));  // the staging buffers below are reused
+    MD200_CK(cudaMemcpy(e->in_h, h, sizeof(double) * B * L, cudaMemcpyHostToDevice));
+    MD200_CK(cudaMemcpy(e->in_vp, vp, sizeof(double) * B * L, cudaMemcpyHostToDevice));
+    MD200_CK(cudaMemcpy(e->in_vs, vs, sizeof(double) * B * L, cudaMemcpyHostToDevice));
+    MD200_CK(cudaMemcpy(e->in_rho, rho, sizeof(double) * B * L, cudaMemcpyHostToDevice));
+    MD200_CK(cudaMemcpy(e->rg_offsets, period_offsets, sizeof(int) * (B + 1), cudaMemcpyHostToDevice));
+    MD200_CK(cudaMemcpy(e->rg_modes, modes, sizeof(int) * B, cudaMemcpyHostToDevice));
+    MD200_CK(cudaMemcpy(e->rg_outbase, outbase.data(), sizeof(long long) * B, cudaMemcpyHostToDevice));
+    MD200_CK(cudaMemcpy(e->rg_periods, periods, sizeof(double) * traces, cudaMemcpyHostToDevice));
+    if (bounds) MD200_CK(cudaMemcpy(e->in_bounds, bounds, sizeof(double) * 2 * B, cudaMemcpyHostToDevice));
+    const bool grp = e->d.group != 0;
+    Ragged rg;
+    rg.ntraces = traces;
+    rg.offsets = e->rg_offsets;
+    rg.modes = e->rg_modes;
+    rg.outbase = e->rg_outbase;
+    if (enqueue(e, e->in_h, e->in_vp, e->in_vs, e->in_rho, models, e->rg_periods, bounds ? e->in_bounds : nullptr,
+                tol, accept, wave,
+                e->out_vel, e->out_flags, e->out_levels, e->out_counts, grp ? e->out_grp : nullptr,
+                grp ? e->out_gflags : nullptr, nullptr, nullptr, e->d_stats, s, rg))
+      return 1;
+    MD200_CK(cudaStreamSynchronize(s));
+    MD200_CK(cudaMemcpy(velocity, e->out_vel, sizeof(double) * cells, cudaMemcpyDeviceToHost));
+    MD200_CK(cudaMemcpy(flags, e->out_flags, sizeof(unsigned) * traces, cudaMemcpyDeviceToHost));
+    MD200_CK(cudaMemcpy(levels, e->out_levels, sizeof(int) * traces, cudaMemcpyDeviceToHost));
+    MD200_CK(cudaMemcpy(counts, e->out_counts, sizeof(int) * traces, cudaMemcpyDeviceToHost));
+    if (grp) {
+      MD200_CK(cudaMemcpy(group, e->out_grp, sizeof(double) * cells, cudaMemcpyDeviceToHost));
+      MD200_CK(cudaMemcpy(group_flags, e->out_gflags, sizeof(unsigned) * cells, cudaMemcpyDeviceToHost));
+    }
+    if (stats && nstats > 0)
+      MD200_CK(cudaMemcpy(stats, e->d_stats, sizeof(unsigned long long) * std::min(nstats, int(MD200_STAT_COUNT)),
+                          cudaMemcpyDeviceToHost));
+    return 0;
+  } catch (...) {
+    return fail_exception();
   }
-  const int traces = period_offsets[models];
-  if (traces < 1 || static_cast<long long>(traces) > static_cast<long long>(e->cap) * e->T)
-    return fail("modisp_b200: ragged trace count " + std::to_string(traces) + " outside 1.." +
-                std::to_string(static_cast<long long>(e->cap) * e->T) + " (capacity x periods)");
-  for (int t = 0; t < traces; ++t)
-    if (!(periods[t] > 0.)) return fail("modisp_b200: periods must be positive");
-  MD200_CK(cudaSetDevice(e->device));
-  const size_t B = models, L = e->L, capt = static_cast<size_t>(e->cap) * e->T;
-  if (lazy_alloc(e, &e->rg_offsets, static_cast<size_t>(e->cap) + 1) || lazy_alloc(e, &e->rg_modes, e->cap) ||
-      lazy_alloc(e, &e->rg_outbase, e->cap) || lazy_alloc(e, &e->rg_periods, capt))
-    return 1;
-  cudaStream_t s = e->stream;
-  MD200_CK(cudaStreamSynchronize(s));  // the staging buffers below are reused
-  MD200_CK(cudaMemcpy(e->in_h, h, sizeof(double) * B * L, cudaMemcpyHostToDevice));
-  MD200_CK(cudaMemcpy(e->in_vp, vp, sizeof(double) * B * L, cudaMemcpyHostToDevice));
-  MD200_CK(cudaMemcpy(e->in_vs, vs, sizeof(double) * B * L, cudaMemcpyHostToDevice));
-  MD200_CK(cudaMemcpy(e->in_rho, rho, sizeof(double) * B * L, cudaMemcpyHostToDevice));
-  MD200_CK(cudaMemcpy(e->rg_offsets, period_offsets, sizeof(int) * (B + 1), cudaMemcpyHostToDevice));
-  MD200_CK(cudaMemcpy(e->rg_modes, modes, sizeof(int) * B, cudaMemcpyHostToDevice));
-  MD200_CK(cudaMemcpy(e->rg_outbase, outbase.data(), sizeof(long long) * B, cudaMemcpyHostToDevice));
-  MD200_CK(cudaMemcpy(e->rg_periods, periods, sizeof(double) * traces, cudaMemcpyHostToDevice));
-  if (bounds) MD200_CK(cudaMemcpy(e->in_bounds, bounds, sizeof(double) * 2 * B, cudaMemcpyHostToDevice));
-  const bool grp = e->d.group != 0;
-  Ragged rg;
-  rg.ntraces = traces;
-  rg.offsets = e->rg_offsets;
-  rg.modes = e->rg_modes;
-  rg.outbase = e->rg_outbase;
-  if (enqueue(e, e->in_h, e->in_vp, e->in_vs, e->in_rho, models, e->rg_periods, bounds ? e->in_bounds : nullptr,
-              tol, accept, wave,
-              e->out_vel, e->out_flags, e->out_levels, e->out_counts, grp ? e->out_grp : nullptr,
-              grp ? e->out_gflags : nullptr, nullptr, nullptr, e->d_stats, s, rg))
-    return 1;
-  MD200_CK(cudaStreamSynchronize(s));
-  MD200_CK(cudaMemcpy(velocity, e->out_vel, sizeof(double) * cells, cudaMemcpyDeviceToHost));
-  MD200_CK(cudaMemcpy(flags, e->out_flags, sizeof(unsigned) * traces, cudaMemcpyDeviceToHost));
-  MD200_CK(cudaMemcpy(levels, e->out_levels, sizeof(int) * traces, cudaMemcpyDeviceToHost));
-  MD200_CK(cudaMemcpy(counts, e->out_counts, sizeof(int) * traces, cudaMemcpyDeviceToHost));
-  if (grp) {
-    MD200_CK(cudaMemcpy(group, e->out_grp, sizeof(double) * cells, cudaMemcpyDeviceToHost));
-    MD200_CK(cudaMemcpy(group_flags, e->out_gflags, sizeof(unsigned) * cells, cudaMemcpyDeviceToHost));
-  }
-  if (stats && nstats > 0)
-    MD200_CK(cudaMemcpy(stats, e->d_stats, sizeof(unsigned long long) * std::min(nstats, int(MD200_STAT_COUNT)),
-                        cudaMemcpyDeviceToHost));
-  return 0;
 }
 
 int md200_graph_begin(md200_engine *e) {
@@ -986,43 +1010,47 @@ int md200_kernel_report(int layers, int single_precision, char *json, int length
 int md200_group_roots(const double *h, const double *vp, const double *vs, const double *rho,
                       int layers, int wave, double period, const double *roots, int known,
                       int modes, double close_rtol, double *group, unsigned *group_flags) {
-  if (layers < 1 || layers > 256 || modes < 1 || modes > 256 || known < 0 || known > 256 ||
-      !(period > 0.))
-    return fail("modisp_b200: invalid review trace");
-  const int L = layers;
-  std::vector<double> tab(static_cast<size_t>(EVAL_ROWS) * L + known + 1, 0.);
-  for (int j = 0; j < L; ++j) {
-    const double s = vs[j];
-    tab[j] = j == L - 1 ? 0. : h[j];
-    tab[L + j] = 1. / vp[j];
-    tab[2 * L + j] = s > 0. ? 1. / s : 0.;
-    tab[3 * L + j] = s * s;
-    tab[4 * L + j] = rho[j];
-    tab[5 * L + j] = 1. / rho[j];
-    tab[6 * L + j] = s > 0. ? 1. / (rho[j] * s * s) : 0.;
+  try {
+    if (layers < 1 || layers > 256 || modes < 1 || modes > 256 || known < 0 || known > 256 ||
+        !(period > 0.))
+      return fail("modisp_b200: invalid review trace");
+    const int L = layers;
+    std::vector<double> tab(static_cast<size_t>(EVAL_ROWS) * L + known + 1, 0.);
+    for (int j = 0; j < L; ++j) {
+      const double s = vs[j];
+      tab[j] = j == L - 1 ? 0. : h[j];
+      tab[L + j] = 1. / vp[j];
+      tab[2 * L + j] = s > 0. ? 1. / s : 0.;
+      tab[3 * L + j] = s * s;
+      tab[4 * L + j] = rho[j];
+      tab[5 * L + j] = 1. / rho[j];
+      tab[6 * L + j] = s > 0. ? 1. / (rho[j] * s * s) : 0.;
+    }
+    for (int j = 0; j < known; ++j) tab[static_cast<size_t>(EVAL_ROWS) * L + j] = roots[j];
+    double *dtab = nullptr, *dgrp = nullptr;
+    unsigned *dfl = nullptr;
+    MD200_CK(cudaMalloc(&dtab, sizeof(double) * tab.size()));
+    cudaError_t err = cudaMalloc(&dgrp, sizeof(double) * modes);
+    if (err == cudaSuccess) err = cudaMalloc(&dfl, sizeof(unsigned) * modes);
+    if (err == cudaSuccess)
+      err = cudaMemcpy(dtab, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice);
+    if (err == cudaSuccess) {
+      group_roots<<<(modes + 31) / 32, 32>>>(dtab, L, vs[0] == 0. ? 1 : 0, wave, TWO_PI / period,
+                                            dtab + static_cast<size_t>(EVAL_ROWS) * L, known, modes,
+                                            close_rtol, dgrp, dfl);
+      err = cudaGetLastError();
+    }
+    if (err == cudaSuccess) err = cudaMemcpy(group, dgrp, sizeof(double) * modes, cudaMemcpyDeviceToHost);
+    if (err == cudaSuccess)
+      err = cudaMemcpy(group_flags, dfl, sizeof(unsigned) * modes, cudaMemcpyDeviceToHost);
+    cudaFree(dtab);
+    cudaFree(dgrp);
+    cudaFree(dfl);
+    if (err != cudaSuccess) return fail(std::string("modisp_b200 CUDA: ") + cudaGetErrorString(err));
+    return 0;
+  } catch (...) {
+    return fail_exception();
   }
-  for (int j = 0; j < known; ++j) tab[static_cast<size_t>(EVAL_ROWS) * L + j] = roots[j];
-  double *dtab = nullptr, *dgrp = nullptr;
-  unsigned *dfl = nullptr;
-  MD200_CK(cudaMalloc(&dtab, sizeof(double) * tab.size()));
-  cudaError_t err = cudaMalloc(&dgrp, sizeof(double) * modes);
-  if (err == cudaSuccess) err = cudaMalloc(&dfl, sizeof(unsigned) * modes);
-  if (err == cudaSuccess)
-    err = cudaMemcpy(dtab, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice);
-  if (err == cudaSuccess) {
-    group_roots<<<(modes + 31) / 32, 32>>>(dtab, L, vs[0] == 0. ? 1 : 0, wave, TWO_PI / period,
-                                          dtab + static_cast<size_t>(EVAL_ROWS) * L, known, modes,
-                                          close_rtol, dgrp, dfl);
-    err = cudaGetLastError();
-  }
-  if (err == cudaSuccess) err = cudaMemcpy(group, dgrp, sizeof(double) * modes, cudaMemcpyDeviceToHost);
-  if (err == cudaSuccess)
-    err = cudaMemcpy(group_flags, dfl, sizeof(unsigned) * modes, cudaMemcpyDeviceToHost);
-  cudaFree(dtab);
-  cudaFree(dgrp);
-  cudaFree(dfl);
-  if (err != cudaSuccess) return fail(std::string("modisp_b200 CUDA: ") + cudaGetErrorString(err));
-  return 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -1065,46 +1093,50 @@ int reliability_args(ReliabilityArgs &r, int B, int K, int T, const md200_period
 
 int md200_reliability_plan(const double *periods, int T, double max_log_period_gap, md200_period_plan *plan,
                            int32_t *order) {
-  if (T < 1) return fail("modisp_b200: no periods");
-  for (int t = 0; t < T; ++t)
-    if (!std::isfinite(periods[t]) || !(periods[t] > 0.)) return fail("modisp_b200: periods must be finite and positive");
-  std::vector<int32_t> idx(T);
-  for (int t = 0; t < T; ++t) idx[t] = t;
-  std::stable_sort(idx.begin(), idx.end(), [&](int32_t a, int32_t b) { return periods[a] < periods[b]; });
-  std::vector<int32_t> unique;
-  int32_t group = -1;  // position in order of the current distinct period
-  for (int q = 0; q < T; ++q) {
-    const int32_t t = idx[q];
-    order[q] = t;
-    md200_period_plan &p = plan[t];
-    p = md200_period_plan{-1, -1, 0, 0, 0, 0, 0.};
-    if (unique.empty()) {
-      p.kind = MD200_PLAN_FIRST;
-    } else {
-      const int32_t prev = unique.back();
-      p.prev = prev;
-      if (periods[t] == periods[prev]) {
-        p.kind = MD200_PLAN_DUPLICATE;
-        plan[prev].dup_end = q + 1;
-        continue;
-      }
-      const double lg = log_gap(periods[prev], periods[t]);
-      if (lg > max_log_period_gap) p.kind |= MD200_PLAN_GAP;
-      if (unique.size() >= 2) {
-        const int32_t older = unique[unique.size() - 2];
-        const double den = log_gap(periods[older], periods[prev]);
-        if (den <= max_log_period_gap && lg <= max_log_period_gap) {
-          p.kind |= MD200_PLAN_PREDICT;
-          p.older = older;
-          p.ratio = lg / den;
+  try {
+    if (T < 1) return fail("modisp_b200: no periods");
+    for (int t = 0; t < T; ++t)
+      if (!std::isfinite(periods[t]) || !(periods[t] > 0.)) return fail("modisp_b200: periods must be finite and positive");
+    std::vector<int32_t> idx(T);
+    for (int t = 0; t < T; ++t) idx[t] = t;
+    std::stable_sort(idx.begin(), idx.end(), [&](int32_t a, int32_t b) { return periods[a] < periods[b]; });
+    std::vector<int32_t> unique;
+    int32_t group = -1;  // position in order of the current distinct period
+    for (int q = 0; q < T; ++q) {
+      const int32_t t = idx[q];
+      order[q] = t;
+      md200_period_plan &p = plan[t];
+      p = md200_period_plan{-1, -1, 0, 0, 0, 0, 0.};
+      if (unique.empty()) {
+        p.kind = MD200_PLAN_FIRST;
+      } else {
+        const int32_t prev = unique.back();
+        p.prev = prev;
+        if (periods[t] == periods[prev]) {
+          p.kind = MD200_PLAN_DUPLICATE;
+          plan[prev].dup_end = q + 1;
+          continue;
+        }
+        const double lg = log_gap(periods[prev], periods[t]);
+        if (lg > max_log_period_gap) p.kind |= MD200_PLAN_GAP;
+        if (unique.size() >= 2) {
+          const int32_t older = unique[unique.size() - 2];
+          const double den = log_gap(periods[older], periods[prev]);
+          if (den <= max_log_period_gap && lg <= max_log_period_gap) {
+            p.kind |= MD200_PLAN_PREDICT;
+            p.older = older;
+            p.ratio = lg / den;
+          }
         }
       }
+      group = q;
+      p.dup_begin = p.dup_end = group + 1;
+      unique.push_back(t);
     }
-    group = q;
-    p.dup_begin = p.dup_end = group + 1;
-    unique.push_back(t);
+    return 0;
+  } catch (...) {
+    return fail_exception();
   }
-  return 0;
 }
 
 int md200_mode_reliability_planned(const double *velocity, const uint32_t *trace_flags, const int64_t *root_count,
