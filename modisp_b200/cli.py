@@ -26,10 +26,6 @@ import sys
 
 import numpy as np
 
-RAGGED_KEYS = ("period_offsets", "periods", "modes", "out_offsets", "phase_velocity", "trace_flags", "search_level",
-               "root_count", "group_velocity", "group_velocity_flags")
-
-
 def _parser():
     from .api import DEFAULT_ACCURACY
     from . import __version__
