@@ -195,3 +195,28 @@ def test_engine_results_and_device_entry_point():
     torch.cuda.synchronize()
     np.testing.assert_array_equal(fl.cpu().numpy().view(np.uint16), want[0])
     np.testing.assert_array_equal(asd.cpu().numpy().astype(bool), want[1])
+
+
+def test_c_entry_points_reject_bad_plans_before_any_device_work():
+    """Every index the kernel follows is checked on the host first: a plan whose
+    indices leave the period array, bad tolerances and bad periods are refused
+    with a message (no GPU needed to see it)."""
+    _native.lib()
+    v = np.ones((1, 2, 3))
+    plan, order, _ = period_plan(np.array([1., 2., 3.]))
+    for field, value in (("prev", 7), ("older", -2), ("dup_end", 9)):
+        bad = plan.copy()
+        t = 2
+        bad[field][t] = value
+        if field == "older":
+            bad["kind"][t] |= _native.PLAN_PREDICT
+        with pytest.raises(RuntimeError, match="invalid period plan"):
+            _native.mode_reliability(v, bad, order)
+    bad_order = order.copy()
+    bad_order[0] = 5
+    with pytest.raises(RuntimeError, match="invalid period plan"):
+        _native.mode_reliability(v, plan, bad_order)
+    with pytest.raises(RuntimeError, match="tolerances must be finite and positive"):
+        _native.mode_reliability(v, plan, order, close_root_rtol=-1.)
+    with pytest.raises(RuntimeError, match="periods must be finite and positive"):
+        _native.reliability_plan(np.array([1., np.nan]), .25)
