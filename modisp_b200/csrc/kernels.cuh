@@ -11,14 +11,21 @@
 //                 order; a same-sign trough of the shape feature (a possible
 //                 hidden close pair) is zoomed into by the whole warp in FP64;
 //                 sign-uncertain FP32 samples are re-evaluated in FP64
-//   refine        one thread per bracket: FP64 endpoint confirmation (FP32
-//                 scans) and FP64 Brent refinement
+//   refine        one bracket per lane, lanes refilled from the bracket list:
+//                 FP64 endpoint confirmation (FP32 scans) and FP64 Brent
+//                 refinement on scale-consistent samples, ending on the secant
+//                 point of the converged bracket
 //   [FP32 only] collect_repairs + scan<double>/refine on the traces whose
 //                 FP32 brackets FP64 did not confirm
 //   assemble      one thread per trace: order, cap and write the roots, flags,
 //                 counts and group-velocity windows
 //   group         one thread per root: FP64 group velocity from forward-mode
 //                 derivatives dF/dk and dF/domega of the secular function
+//   [FP32 only] continuity_screen + scan<double>/refine/assemble/group on the
+//                 traces whose roots break the bilateral envelope of their
+//                 neighbouring periods
+// Outside the run: root_jacobians (adjoint.cuh) and mode_reliability
+// (reliability.cuh) work on a run's results.
 #pragma once
 #include "engine.cuh"
 #include "secular.cuh"
