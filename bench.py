@@ -50,7 +50,7 @@ FLOPS_PER_STEP = {0: 170, 1: 24}
 # DRAM traffic of the FP32 Rayleigh scan, dram__bytes_read.sum + dram__bytes_write.sum
 # from one ncu capture of a 2,000-model launch (120,000 traces: 30.1 MB + 93.0 MB),
 # per trace; scaled to this workload's launch by its trace count.
-SCAN32_DRAM_BYTES_PER_TRACE = (30.053632e6 + 92.991232e6) / 120_000
+SCAN32_DRAM_BYTES_PER_TRACE = (30.661888e6 + 95.3536e6) / 120_000
 
 
 def parse():
