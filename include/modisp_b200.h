@@ -319,10 +319,13 @@ int md200_mode_reliability_planned(const double *velocity, const uint32_t *trace
  * md200_group_roots; the scratch is a static 16 KiB device array (2048 doubles,
  * held by every GPU that loads the library until exit) that must hold
  * 7*layers + known + modes + ceil(modes/2) doubles (e.g. 256 layers with up to
- * 100 roots and modes); larger requests fail with a message and touch nothing.  The first
- * call on a device looks up the array's address (cudaGetSymbolAddress) -- make it
- * before any stream capture.  Calls share the array: calls that overlap on the
- * GPU (from several host threads or processes sharing a context) race. */
+ * 100 roots and modes); larger requests fail with a message and touch nothing.
+ * Every call looks up the array's address on the current device
+ * (cudaGetSymbolAddress), so a device reset between calls does no harm.  Its
+ * copies are synchronous (cudaMemcpy) and its kernel runs on the legacy default
+ * stream.  Calls share the array, which keeps the last call's contents (each
+ * call rewrites what it reads): calls that overlap on the GPU (from several host
+ * threads, or processes sharing a context) race. */
 int md200_group_roots_static(const double *thickness, const double *vp, const double *vs,
                              const double *rho, int layers, int wave, double period,
                              const double *roots, int known, int modes, double close_rtol,

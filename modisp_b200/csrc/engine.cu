@@ -9,7 +9,6 @@
 #include <algorithm>
 #include <exception>
 #include <cmath>
-#include <mutex>
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -454,27 +453,20 @@ namespace {
 // Static scratch for md200_group_roots_static: 2048 doubles (16 KiB), room for
 // 7 x layers (prepared rows) + roots + modes (group velocities) + modes / 2 (flags)
 // -- e.g. 256 layers with up to 100 roots and modes, or 100 layers with any count.
-// Every GPU that loads this library holds it until the process exits.  In host code the symbol is only a handle; the
-// device address comes from cudaGetSymbolAddress, looked up once per device.
+// Every GPU that loads this library holds it until the process exits.  In host
+// code the symbol is only a handle: the device address comes from
+// cudaGetSymbolAddress on the current device.
 // ---------------------------------------------------------------------------
 constexpr int STATIC_SCRATCH_DOUBLES = 2048;
 static __device__ __align__(256) double g_group_scratch[STATIC_SCRATCH_DOUBLES];
 
-std::mutex g_scratch_mutex;
-double *g_scratch_address[64] = {};
-
-// Device address of g_group_scratch on the current device (set-up on first use).
+// Device address of g_group_scratch on the current device.  Looked up on every
+// call (a host-side table lookup, cheap next to the call's synchronous copies):
+// a cached address would go stale if the caller reset the device between calls.
 int static_scratch(double **address) {
-  int device = 0;
-  MD200_CK(cudaGetDevice(&device));
-  if (device < 0 || device >= 64) return fail("modisp_b200: device index beyond the scratch table");
-  std::lock_guard<std::mutex> lock(g_scratch_mutex);
-  if (!g_scratch_address[device]) {
-    void *p = nullptr;
-    MD200_CK(cudaGetSymbolAddress(&p, g_group_scratch));
-    g_scratch_address[device] = static_cast<double *>(p);
-  }
-  *address = g_scratch_address[device];
+  void *p = nullptr;
+  MD200_CK(cudaGetSymbolAddress(&p, g_group_scratch));
+  *address = static_cast<double *>(p);
   return 0;
 }
 
@@ -1269,39 +1261,44 @@ int md200_measure_peak(int device, int fp64, double *flops) {
 int md200_group_roots_static(const double *h, const double *vp, const double *vs, const double *rho,
                              int layers, int wave, double period, const double *roots, int known,
                              int modes, double close_rtol, double *group, unsigned *group_flags) {
-  if (layers < 1 || layers > 256 || modes < 1 || modes > 256 || known < 0 || known > 256 ||
-      !(period > 0.))
-    return fail("modisp_b200: invalid review trace");
-  const int L = layers;
-  // table (7 rows x L) + roots + group velocities + flags (two per double)
-  const int need = EVAL_ROWS * L + known + modes + (modes + 1) / 2;
-  if (need > STATIC_SCRATCH_DOUBLES)
-    return fail("modisp_b200: review trace needs " + std::to_string(need) +
-                " doubles of static scratch, the maximum is " + std::to_string(STATIC_SCRATCH_DOUBLES));
-  double table[STATIC_SCRATCH_DOUBLES];  // host staging on the stack: no heap use either
-  for (int j = 0; j < L; ++j) {
-    const double sv = vs[j];
-    table[j] = j == L - 1 ? 0. : h[j];
-    table[L + j] = 1. / vp[j];
-    table[2 * L + j] = sv > 0. ? 1. / sv : 0.;
-    table[3 * L + j] = sv * sv;
-    table[4 * L + j] = rho[j];
-    table[5 * L + j] = 1. / rho[j];
-    table[6 * L + j] = sv > 0. ? 1. / (rho[j] * sv * sv) : 0.;
+  try {
+    if (layers < 1 || layers > 256 || modes < 1 || modes > 256 || known < 0 || known > 256 ||
+        !(period > 0.))
+      return fail("modisp_b200: invalid review trace");
+    const int L = layers;
+    // table (7 rows x L) + roots + group velocities + flags (two per double)
+    const int need = EVAL_ROWS * L + known + modes + (modes + 1) / 2;
+    if (need > STATIC_SCRATCH_DOUBLES)
+      return fail("modisp_b200: review trace needs " + std::to_string(need) +
+                  " doubles of static scratch, the maximum is " + std::to_string(STATIC_SCRATCH_DOUBLES));
+    double table[STATIC_SCRATCH_DOUBLES];  // host staging on the stack: no heap use either
+    for (int j = 0; j < L; ++j) {
+      const double sv = vs[j];
+      table[j] = j == L - 1 ? 0. : h[j];
+      table[L + j] = 1. / vp[j];
+      table[2 * L + j] = sv > 0. ? 1. / sv : 0.;
+      table[3 * L + j] = sv * sv;
+      table[4 * L + j] = rho[j];
+      table[5 * L + j] = 1. / rho[j];
+      table[6 * L + j] = sv > 0. ? 1. / (rho[j] * sv * sv) : 0.;
+    }
+    for (int j = 0; j < known; ++j) table[EVAL_ROWS * L + j] = roots[j];
+    double *scratch = nullptr;
+    if (static_scratch(&scratch)) return 1;
+    double *dtab = scratch, *dgrp = scratch + EVAL_ROWS * L + known;
+    unsigned *dfl = reinterpret_cast<unsigned *>(dgrp + modes);
+    // the table and roots are rewritten by every call, and the kernel writes every
+    // output slot: nothing left by an earlier call is read
+    MD200_CK(cudaMemcpy(dtab, table, sizeof(double) * (EVAL_ROWS * L + known), cudaMemcpyHostToDevice));
+    group_roots<<<(modes + 31) / 32, 32>>>(dtab, L, vs[0] == 0. ? 1 : 0, wave, TWO_PI / period,
+                                          dtab + EVAL_ROWS * L, known, modes, close_rtol, dgrp, dfl);
+    MD200_CK(cudaGetLastError());
+    MD200_CK(cudaMemcpy(group, dgrp, sizeof(double) * modes, cudaMemcpyDeviceToHost));
+    MD200_CK(cudaMemcpy(group_flags, dfl, sizeof(unsigned) * modes, cudaMemcpyDeviceToHost));
+    return 0;
+  } catch (...) {
+    return fail_exception();
   }
-  for (int j = 0; j < known; ++j) table[EVAL_ROWS * L + j] = roots[j];
-  double *scratch = nullptr;
-  if (static_scratch(&scratch)) return 1;
-  double *dtab = scratch, *dgrp = scratch + EVAL_ROWS * L + known;
-  unsigned *dfl = reinterpret_cast<unsigned *>(dgrp + modes);
-  // every output slot is written by the kernel: nothing needs clearing between calls
-  MD200_CK(cudaMemcpy(dtab, table, sizeof(double) * (EVAL_ROWS * L + known), cudaMemcpyHostToDevice));
-  group_roots<<<(modes + 31) / 32, 32>>>(dtab, L, vs[0] == 0. ? 1 : 0, wave, TWO_PI / period,
-                                        dtab + EVAL_ROWS * L, known, modes, close_rtol, dgrp, dfl);
-  MD200_CK(cudaGetLastError());
-  MD200_CK(cudaMemcpy(group, dgrp, sizeof(double) * modes, cudaMemcpyDeviceToHost));
-  MD200_CK(cudaMemcpy(group_flags, dfl, sizeof(unsigned) * modes, cudaMemcpyDeviceToHost));
-  return 0;
 }
 
 }  // extern "C"

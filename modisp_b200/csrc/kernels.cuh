@@ -1464,33 +1464,32 @@ __global__ void assemble(Dev d, const int *list = nullptr, int count_id = 0) {
   }
   unsigned fl = d.tflags[t];
   const int nbr = d.nbr[t];
-  const double *slot = d.slot + static_cast<size_t>(t) * d.KB * SLOT;
-  // gather, order and cap at K (the K = nmodes + 2 smallest roots)
-  double r[64] = {};
-  int n = 0;
-  const int K = nm + 2;
-  const int cap = K < 64 ? K : 64;
+  // The refined roots sit in the root field of the trace's bracket slots (at most
+  // K = nmodes + 2 of them: the scan stops at K brackets).  They are ordered in
+  // place there, so every mode count the engine accepts (up to 256 + 2 guards)
+  // keeps all of its roots; nothing reads a slot's bracket after assembly (a
+  // re-solved trace is scanned into its slots afresh).
+  double *rs = d.slot + static_cast<size_t>(t) * d.KB * SLOT + 4;
+  auto r = [rs](int i) -> double & { return rs[static_cast<size_t>(i) * SLOT]; };
   bool failed = (fl & (TRACE_SEARCH_UNCONVERGED | INTERNAL_REPAIR)) != 0;
-  auto push = [&](double x) {
-    // insertion into the ascending list, keeping at most `cap` values
-    if (n == cap && !(x < r[n - 1])) return;
-    int i = n < cap ? n++ : n - 1;
-    while (i > 0 && r[i - 1] > x) {
-      r[i] = r[i - 1];
-      --i;
+  for (int s = 0; s < nbr && !failed; ++s)
+    if (!isfinite(r(s))) failed = true;
+  int n = 0;
+  if (!failed) {
+    // insertion sort (brackets arrive in velocity order: nearly sorted already)
+    for (int i = 1; i < nbr; ++i) {
+      const double x = r(i);
+      int j = i;
+      while (j > 0 && r(j - 1) > x) {
+        r(j) = r(j - 1);
+        --j;
+      }
+      r(j) = x;
     }
-    r[i] = x;
-  };
-  for (int s = 0; s < nbr && !failed; ++s) {
-    const double x = slot[static_cast<size_t>(s) * SLOT + 4];
-    if (!isfinite(x)) failed = true;
-    else push(x);
+    // exact duplicates (an exact zero shared by two brackets) collapse to one root
+    for (int i = 0; i < nbr; ++i)
+      if (n == 0 || r(i) != r(n - 1)) r(n++) = r(i);
   }
-  // exact duplicates (an exact zero shared by two brackets) collapse to one root
-  int u = 0;
-  for (int i = 0; i < n; ++i)
-    if (u == 0 || r[i] != r[u - 1]) r[u++] = r[i];
-  n = u;
   const double lo = d.mlo[b], hi = d.mhi[b];
   const LayerView<double> m = global_view(d, b);
   const double vs_hs = layer_table<double>(d, b)[8 * d.Ls + m.L - 1];
@@ -1504,9 +1503,9 @@ __global__ void assemble(Dev d, const int *list = nullptr, int count_id = 0) {
     n = 0;
   }
   for (int i = 1; i < n; ++i)
-    if (r[i] - r[i - 1] <= d.close_rtol * r[i]) fl |= TRACE_CLOSE_ROOT_RISK;
+    if (r(i) - r(i - 1) <= d.close_rtol * r(i)) fl |= TRACE_CLOSE_ROOT_RISK;
   for (int mo = 0; mo < nm; ++mo) {
-    double root = mo < n ? r[mo] : NAN;
+    double root = mo < n ? r(mo) : NAN;
     if (isfinite(root) && root >= .99 * vs_hs) fl |= TRACE_NEAR_CUTOFF;
     if (isfinite(root) && d.accept < 1.) {
       const double v = eval64(m, d.wave, w, root, nullptr);
@@ -1523,11 +1522,11 @@ __global__ void assemble(Dev d, const int *list = nullptr, int count_id = 0) {
         d.gflags[cell] = GROUP_MISSING_ROOT;
       } else {
         // neighbour-midpoint window and close-root test (cpp/cpu/solver.cpp:96-103)
-        const double c = r[mo];
-        const double wl = mo ? .5 * (r[mo - 1] + c) : lo;
-        const double wh = mo + 1 < n ? .5 * (c + r[mo + 1]) : hi;
-        const bool close = (mo && c - r[mo - 1] <= d.close_rtol * c) ||
-                           (mo + 1 < n && r[mo + 1] - c <= d.close_rtol * r[mo + 1]);
+        const double c = r(mo);
+        const double wl = mo ? .5 * (r(mo - 1) + c) : lo;
+        const double wh = mo + 1 < n ? .5 * (c + r(mo + 1)) : hi;
+        const bool close = (mo && c - r(mo - 1) <= d.close_rtol * c) ||
+                           (mo + 1 < n && r(mo + 1) - c <= d.close_rtol * r(mo + 1));
         d.gwin[2 * cell] = wl;
         d.gwin[2 * cell + 1] = wh;
         if (close) {
@@ -1673,6 +1672,13 @@ __global__ void group_roots(const double *tab, int L, int water, int wave, doubl
       (j + 1 < known && roots[j + 1] - c <= close_rtol * roots[j + 1])) {
     group[j] = NAN;
     flags[j] = GROUP_CLOSE_ROOT;
+    return;
+  }
+  // a packed root that is NaN or not positive is a missing root
+  // (cpp/common/group_velocity.hpp:31): k = w / c would be meaningless
+  if (!isfinite(c) || !(c > 0.)) {
+    group[j] = NAN;
+    flags[j] = GROUP_MISSING_ROOT;
     return;
   }
   const LayerView<double> m = make_view<double>(tab, L, L, water);

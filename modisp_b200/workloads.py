@@ -76,6 +76,23 @@ def config4(B=4096):
     return crustal_batch(B, SEED + 4, layers=12), np.geomspace(1., 40., 40), 3
 
 
+def deep_batch(B, seed=SEED + 6):
+    """Deep slow-over-fast models whose short periods carry hundreds of modes:
+    n ~ U{3..5} finite layers of h ~ U(15, 80) km, Vs rising from U(0.4, 0.9) to
+    U(2.5, 3.5) km/s over the stack, a half-space of Vs ~ U(4.2, 4.7) km/s,
+    Vp = Vs U(1.75, 2.2), rho = 1.74 Vp^0.25."""
+    rng = np.random.default_rng(seed)
+    rows = []
+    for _ in range(B):
+        n = int(rng.integers(3, 6))
+        top, bottom = rng.uniform(0.4, 0.9), rng.uniform(2.5, 3.5)
+        vs = np.append(top + (bottom - top) * np.arange(n) / (n - 1), rng.uniform(4.2, 4.7))
+        vp = vs * rng.uniform(1.75, 2.2, n + 1)
+        h = np.append(rng.uniform(15., 80., n), 0.)
+        rows.append((h, vp, vs, _gardner(vp)))
+    return _pad(rows, max(r[0].size for r in rows))
+
+
 def gradient_batch(B, seed=SEED + 5):
     """Smooth-gradient models: n ~ U{30..100} layers of h = 80/n km, Vs(z) = 0.2 + 4.3 z/80
     with +-5 % noise, Vp/rho as above; per-model periods (50-120 geomspaced in a random

@@ -1,9 +1,11 @@
 """Generate the golden fixtures under tests/golden/ from the reference implementation.
 
-Run in a checkout that has the reference source tree (default /root/reference)
-and the reference CPU engine built by ``make -C oracle``:
+Run with the reference CPU engine built by ``make -C oracle`` and, for the
+repacked frozen fixtures and the reliability cases, the path of a reference
+source checkout:
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py --reference <modisp checkout>
+    python tests/golden/make_golden.py --only deep     # no checkout needed
 
 Outputs (all small .npz files, committed):
 
@@ -12,7 +14,9 @@ Outputs (all small .npz files, committed):
   refinement, Love phase strategy, c_tol_rel 1e-12, group velocity at the
   default group_rtol 1e-3).  Cases: the quickstart model (Rayleigh, Love),
   48-model subsets of the crustal batch (Rayleigh, Love), 48 low-velocity-layer
-  models (Rayleigh, Love), six surface-water models (Rayleigh), one crustal model
+  models (Rayleigh, Love), six surface-water models (Rayleigh), four deep
+  slow-over-fast models at 63, 100 and 256 modes (Rayleigh, Love; their short
+  periods hold more roots than the guard-extended mode count), one crustal model
   with a close pair whose shape-feature trough lies in the FP32 scan's FP64 band, and
   one low-velocity-layer model with a pair in the last cell before the cutoff.
 * ``jac_<case>.npz``: phase-velocity Jacobians by central differences (step 1e-6
@@ -200,16 +204,35 @@ def save_reliability_cases(reference: Path):
                               root_count=f["root_count"])
 
 
+def save_deep_cases():
+    """Deep models at mode counts far above the usual five (63, 100 and 256)."""
+    deep = workloads.deep_batch(4)
+    periods = np.geomspace(0.5, 20., 8)
+    for nmodes in (63, 100, 256):
+        for wave, name in ((0, "rayleigh"), (1, "love")):
+            save_reference_case(f"deep4_k{nmodes}_{name}", deep, periods, nmodes, wave)
+
+
+def reference_tree(args):
+    if not args.reference:
+        raise SystemExit("pass --reference <modisp source checkout> (frozen fixtures and reliability cases)")
+    return Path(args.reference)
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
-    ap.add_argument("--only", choices=["reliability"])
+    ap.add_argument("--reference", help="path of the reference (modisp) source checkout")
+    ap.add_argument("--only", choices=["reliability", "deep"])
     args = ap.parse_args()
     if args.only == "reliability":
-        save_reliability_cases(Path(args.reference))
+        save_reliability_cases(reference_tree(args))
         return
     if oracle.reference() is None:
         raise SystemExit("build the reference CPU engine first: make -C oracle")
+    if args.only == "deep":
+        save_deep_cases()
+        return
+    tree = reference_tree(args)
     model, periods = workloads.quickstart()
     save_reference_case("quickstart_rayleigh", model, periods, 2, 0)
     save_reference_case("quickstart_love", model, periods, 2, 1)
@@ -233,8 +256,9 @@ def main():
     save_jacobian_case("config4_rayleigh", subset(c4, np.arange(4)), periods4, nmodes4, 0)
     save_jacobian_case("config4_love", subset(c4, np.arange(4, 6)), periods4, nmodes4, 1)
     save_jacobian_case("water_rayleigh", subset(water_models(), np.arange(2)), np.geomspace(0.5, 20., 12), 3, 0)
-    repack_reference_fixtures(Path(args.reference))
-    save_reliability_cases(Path(args.reference))
+    save_deep_cases()
+    repack_reference_fixtures(tree)
+    save_reliability_cases(tree)
 
 
 if __name__ == "__main__":

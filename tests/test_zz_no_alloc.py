@@ -55,6 +55,33 @@ def test_static_scratch_matches_allocating_entry_point(case, b, f):
         assert other[0] != g_again[finite][0]
 
 
+@pytest.mark.parametrize("fn", ["md200_group_roots_static", "md200_group_roots"])
+def test_nan_and_negative_packed_roots_are_missing_roots(fn):
+    """A packed root that is NaN or not positive is a missing root (the reference's
+    group_velocity, cpp/common/group_velocity.hpp:31), in both entry points."""
+    from modisp_b200 import _native
+    lib = _native.lib()
+    g = load_golden("ref_crustal48_rayleigh")
+    b, f = 3, 10
+    model = [np.ascontiguousarray(g[k][b], dtype=np.float64) for k in ("thickness", "vp", "vs", "rho")]
+    v = g["phase_velocity"][b, :, f]
+    good = v[np.isfinite(v)]
+    assert good.size >= 4
+    # (a root right below a negative one would count as a close pair, as in the
+    # reference's close-root rule, so the negative root comes first)
+    roots = np.ascontiguousarray(np.array([-1.0, good[0], np.nan, good[2], good[3]]))
+    modes = roots.size
+    group = np.full(modes, -1.)
+    flags = np.full(modes, 12345, dtype=np.uint32)
+    status = getattr(lib, fn)(*(_native.ptr(a) for a in model), model[0].size, int(g["wave"]),
+                              float(g["periods"][f]), _native.ptr(roots), roots.size, modes, .005,
+                              _native.ptr(group), _native.ptr(flags))
+    assert status == 0, _native.last_error()
+    np.testing.assert_array_equal(flags[[0, 2]], [1, 1])  # GROUP_MISSING_ROOT
+    assert np.all(np.isnan(group[[0, 2]]))
+    assert np.all(flags[[1, 3, 4]] == 0) and np.all(np.isfinite(group[[1, 3, 4]]))
+
+
 def test_requests_beyond_the_static_scratch_are_rejected():
     from modisp_b200 import _native
     lib = _native.lib()
