@@ -195,6 +195,11 @@ class QeSolver:
         velocity = _to_float32(out["velocity"]) if self.single_precision else out["velocity"]
         stats = dict(out["stats"])
         stats.update(strategy="b200_scan", capacity=self.capacity)
+        if self.group_velocity:
+            # the counters the reference's continuity review adds to
+            # (python/modisp/_continuity.py:112-119, :136-137; cpp/cpu/solver.cpp:748-749)
+            stats["group_evaluations"] = int(stats.get("group_roots", 0))
+            stats["group_invalid"] = int(np.count_nonzero(out["group_velocity_flags"]))
         extras = dict(group_velocity=out.get("group_velocity"),
                       group_velocity_flags=out.get("group_velocity_flags"),
                       prediction_flags=out.get("prediction_flags"))

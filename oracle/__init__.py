@@ -85,6 +85,44 @@ def reference():
     return _REF
 
 
+_WRAPPER = None
+_CUDA = None
+
+
+def reference_wrapper():
+    """The reference's own Python package (``modisp``), unmodified, as the oracle
+    recipe stages it under ``_ref/modisp`` with the reference CPU engine as its
+    ``_cpu``; None where it is not staged.  Its loader finds this repository's
+    ``modisp_cuda`` package for ``backend="cuda"``."""
+    global _WRAPPER
+    if _WRAPPER is None:
+        root = HERE / "_ref"
+        if not (root / "modisp" / "__init__.py").is_file():
+            return None
+        import sys
+        if str(root) not in sys.path:
+            sys.path.insert(0, str(root))
+        import modisp
+        _WRAPPER = modisp
+    return _WRAPPER
+
+
+def reference_cuda():
+    """The reference's own CUDA plugin extension (``_cuda``), compiled for sm_100a
+    from its sources by ``make -C oracle ref-cuda``; None where it is not built.
+    A same-GPU comparator for bench.py, never a checker of results."""
+    global _CUDA
+    if _CUDA is None:
+        hits = sorted(glob.glob(str(HERE / "_ref" / "cuda" / "_cuda*.so")))
+        if not hits:
+            return None
+        spec = importlib.util.spec_from_file_location("_cuda", hits[0])
+        module = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(module)
+        _CUDA = module
+    return _CUDA
+
+
 def _ptr(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
 

@@ -129,17 +129,27 @@ def test_independent_witnesses(name, single_precision):
     np.testing.assert_allclose(out["velocity"].ravel(), expected, rtol=2e-6)
 
 
+@pytest.mark.parametrize("single_precision", [False, True], ids=["fp64", "fp32scan"])
 @pytest.mark.parametrize("name", sorted(p.stem for p in GOLDEN.glob("fixture_0*.npz")))
-def test_reference_frozen_fixtures(name):
-    """The reference suite's frozen high-accuracy cases: same masks and counts, roots to 1e-6."""
+def test_reference_frozen_fixtures(name, single_precision):
+    """The reference suite's frozen high-accuracy cases, in both engines: same masks
+    and counts; roots to 1e-6 of the frozen values (which the reference froze at its
+    default c_tol_rel of 1e-6) and to 1e-9 of the reference engine run live on the
+    same inputs at c_tol_rel 1e-12."""
+    import oracle
     g = load_golden(name)
     case = dict(g)
     case["wave"] = 1 if str(g["wave"]) == "love" else 0
-    out = engine_solve64(case, False)
+    out = engine_solve64(case, single_precision)
     np.testing.assert_array_equal(np.isfinite(out["velocity"]), g["mode_mask"])
     np.testing.assert_array_equal(out["counts"], g["root_count"])
     m = g["mode_mask"]
     np.testing.assert_allclose(out["velocity"][m], g["phase_velocity"][m], rtol=1e-6)
+    if oracle.reference() is not None:
+        ref = oracle.reference_solve(g["thickness"], g["vp"], g["vs"], g["rho"], g["periods"], int(g["nmodes"]),
+                                     wave=case["wave"], tol=1e-12)
+        np.testing.assert_array_equal(ref["search_bounds"], g["search_bounds"])
+        assert_root_parity(ref, out, f"{name} live")
 
 
 @pytest.mark.parametrize("wave", [0, 1])
@@ -178,19 +188,26 @@ def test_live_reference_on_crustal_sample(wave):
             assert_root_parity(ref, engine_solve64(case, sp), f"{name} wave={wave} fp32={sp}")
 
 
-def test_automatic_window_matches_reference_bounds():
-    """The engine's on-device window (no bounds passed) equals the reference's."""
+@pytest.mark.parametrize("single_precision", [False, True], ids=["fp64", "fp32scan"])
+@pytest.mark.parametrize("name", ["ref_crustal48_rayleigh", "ref_crustal48_love", "ref_lvz48_rayleigh",
+                                  "ref_lvz48_love", "ref_water6_rayleigh", "ref_deep4_k63_love",
+                                  "ref_quickstart_love"])
+def test_automatic_window_matches_reference_bounds(name, single_precision):
+    """The engine's on-device window (no bounds passed) is bit-identical to the
+    reference's _cpu.bounds (frozen in the fixture): Rayleigh and Love, crustal,
+    low-velocity-layer and deep models, and the water-top (Scholte) lower bound."""
     from modisp_b200 import _native
-    g = load_golden("ref_crustal48_rayleigh")
+    g = load_golden(name)
     h = g["thickness"]
     o = _native.default_options()
+    o.single_precision = int(single_precision)
     e = _native.Engine(0, h.shape[0], h.shape[1], g["periods"].size, int(g["nmodes"]), o)
     try:
-        out = e.run(h, g["vp"], g["vs"], g["rho"], g["periods"], None, ENGINE_TOL, 1., 0)
+        out = e.run(h, g["vp"], g["vs"], g["rho"], g["periods"], None, ENGINE_TOL, 1., int(g["wave"]))
     finally:
         e.close()
-    np.testing.assert_array_equal(out["bounds"], g["search_bounds"])
-    assert_root_parity(g, out, "automatic window")
+    np.testing.assert_array_equal(out["bounds"].view(np.uint64), g["search_bounds"].view(np.uint64))
+    assert_root_parity(g, out, f"{name} automatic window")
 
 
 def test_solver_api_end_to_end():
@@ -273,6 +290,30 @@ def test_engines_agree_on_group_velocity_where_it_is_ill_conditioned(wave):
         if np.isfinite(u):
             worst.append(abs(u64[b, k, f] - u) / u)
     assert worst and max(worst) <= GROUP_RTOL, max(worst)
+
+
+@pytest.mark.parametrize("wave", [0, 1])
+def test_config3_sample_matches_reference(wave):
+    """512 models spread over the 100,000-model mixed-precision batch (30 % with one
+    low-velocity layer), 60 periods, 5 modes, in both engines, against the reference
+    CPU engine run live at c_tol_rel 1e-12: masks and counts identical, phase within
+    1e-9, group velocity's structural flags identical."""
+    import os
+    import oracle
+    from modisp_b200 import workloads
+    if oracle.reference() is None:
+        pytest.skip("reference CPU engine not built")
+    batch, periods, nmodes = workloads.config3()
+    idx = np.linspace(0, batch["thickness"].shape[0] - 1, 512).astype(int)
+    sample = {k: np.ascontiguousarray(v[idx]) for k, v in batch.items()}
+    ref = oracle.reference_solve(sample["thickness"], sample["vp"], sample["vs"], sample["rho"], periods, nmodes,
+                                 wave=wave, tol=1e-12, threads=len(os.sched_getaffinity(0)), group_velocity=True)
+    case = dict(sample, periods=periods, nmodes=nmodes, wave=wave, search_bounds=ref["search_bounds"])
+    for sp in (False, True):
+        out = engine_solve64(case, sp)
+        assert_root_parity(ref, out, f"config3 sample wave={wave} fp32={sp}")
+        for bit in (1, 16):
+            np.testing.assert_array_equal(out["group_velocity_flags"] & bit, ref["group_velocity_flags"] & bit)
 
 
 @pytest.mark.parametrize("wave", [0, 1])
