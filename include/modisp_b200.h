@@ -22,7 +22,7 @@
 extern "C" {
 #endif
 
-#define MD200_ABI_VERSION 1
+#define MD200_ABI_VERSION 2
 /* Statistics written by md200_run (indices into the stats array). */
 enum md200_stat {
   MD200_STAT_EVALUATIONS = 0,      /* secular evaluations, all precisions */
@@ -67,8 +67,9 @@ typedef struct md200_options {
   int log_points;          /* background log-spaced points per window; <= 0 default */
   int warps_per_block;     /* scan CTA shape; <= 0 default */
   int blocks_per_sm;       /* persistent CTAs per SM; <= 0 default */
-  int continuity_check;    /* FP32 scan: re-scan in FP64 the traces whose roots leave the
-                              +-5 % envelope of both neighbouring periods (default 1) */
+  int continuity_check;    /* FP32 scan: the reference's continuity screen on the results
+                              (cpp/cpu/continuity_screen.hpp:8-67) and an FP64 re-scan of
+                              its suspects (default 1) */
 } md200_options;
 
 /* Fill *options with the defaults of a high-accuracy FP64 engine. */
@@ -94,14 +95,22 @@ md200_engine *md200_create(int device, int capacity, int layers, int periods, in
  *   flags, levels, counts [models, periods]
  *   group, group_flags [models, nmodes, periods] (engine created with group_velocity)
  *   prediction_flags [models, periods] (engine created with continuation)
+ *   continuity_flags [models, periods] uint8: the continuity screen's flags
+ *                            (python/modisp/_continuity.py:6-14; the reference
+ *                            returns them as DispersionBatch.continuity_flags,
+ *                            python/modisp/__init__.py:424-431): REVIEWED 1,
+ *                            REPAIRED 2, UNRESOLVED 4, NO_BILATERAL 8, ENVELOPE 16,
+ *                            CLOSE_FP32 32, PREDICTION 64.  The screen runs in
+ *                            FP32-scan engines with continuity_check; other
+ *                            engines write 0 (unscreened).
  *   bounds_out [models, 2] the windows searched
  *   stats [nstats] counters, see enum md200_stat. */
 int md200_run(md200_engine *engine, const double *thickness, const double *vp, const double *vs,
               const double *rho, int models, const double *periods, const double *bounds,
               double c_tol_rel, double f_accept, int wave, double *velocity, unsigned *flags,
               int *levels, int *counts, double *group, unsigned *group_flags,
-              unsigned *prediction_flags, double *bounds_out, unsigned long long *stats,
-              int nstats);
+              unsigned *prediction_flags, uint8_t *continuity_flags, double *bounds_out,
+              unsigned long long *stats, int nstats);
 
 /* As md200_run, but every array is a device pointer and the work is enqueued on
  * `stream` (a cudaStream_t; NULL selects the engine's own stream, cudaStreamLegacy the
@@ -112,8 +121,8 @@ int md200_run_device(md200_engine *engine, const double *thickness, const double
                      const double *vs, const double *rho, int models, const double *periods,
                      const double *bounds, double c_tol_rel, double f_accept, int wave,
                      double *velocity, unsigned *flags, int *levels, int *counts, double *group,
-                     unsigned *group_flags, unsigned *prediction_flags, double *bounds_out,
-                     unsigned long long *stats, void *stream);
+                     unsigned *group_flags, unsigned *prediction_flags, uint8_t *continuity_flags,
+                     double *bounds_out, unsigned long long *stats, void *stream);
 
 /* Ragged batch (no counterpart in the reference, whose periods are one array
  * shared by every model, python/modisp/__init__.py:285-286; its per-row form
@@ -126,8 +135,9 @@ int md200_run_device(md200_engine *engine, const double *thickness, const double
  *                                 the engine's periods)
  *   modes [models]              : mode count of model b, 1 .. the engine's nmodes
  *   bounds [models, 2]          : search windows as in md200_run, or NULL (automatic)
- * Outputs: per trace (CSR order) flags, levels, counts [traces]; velocity (and
- * group, group_flags) hold, for model b, a [modes[b]][T_b] block (mode, period),
+ * Outputs: per trace (CSR order) flags, levels, counts, continuity_flags
+ * [traces]; velocity (and group, group_flags) hold, for model b, a [modes[b]][T_b]
+ * block (mode, period),
  * the blocks concatenated in model order (sum of modes[b] T_b values).
  * Trace semantics are those of md200_run. */
 int md200_run_ragged(md200_engine *engine, const double *thickness, const double *vp, const double *vs,
@@ -135,7 +145,7 @@ int md200_run_ragged(md200_engine *engine, const double *thickness, const double
                      const int *modes, const double *bounds, double c_tol_rel, double f_accept, int wave,
                      double *velocity,
                      unsigned *flags, int *levels, int *counts, double *group, unsigned *group_flags,
-                     unsigned long long *stats, int nstats);
+                     uint8_t *continuity_flags, unsigned long long *stats, int nstats);
 
 /* Device-pointer form of md200_run_ragged, enqueued on `stream` (NULL = the
  * engine's stream) without a host synchronisation.  `traces` is
@@ -149,7 +159,8 @@ int md200_run_ragged_device(md200_engine *engine, const double *thickness, const
                             const long long *out_offsets, const double *bounds, double c_tol_rel,
                             double f_accept, int wave,
                             double *velocity, unsigned *flags, int *levels, int *counts, double *group,
-                            unsigned *group_flags, unsigned long long *stats, void *stream);
+                            unsigned *group_flags, uint8_t *continuity_flags, unsigned long long *stats,
+                            void *stream);
 
 /* CUDA-graph capture of device-pointer runs (no counterpart in the reference,
  * which launches its stages one by one, cpp/cuda/qe.cu:927-957).  Between
@@ -219,7 +230,8 @@ int md200_vjp(md200_engine *engine, const double *thickness, const double *vp, c
  * Waits for the run to finish. */
 int md200_stage_times(md200_engine *engine, double *ms, int n);
 
-/* Number of kernel launches one md200_run of this engine enqueues. */
+/* Number of kernel launches the engine's last run enqueued (counted as it
+ * launched them); before any run, those of a run without continuity flags. */
 int md200_kernel_launches(md200_engine *engine);
 
 /* Replaces QeSolver.close() (cpp/cuda/qe.cu:1039-1059). */
@@ -243,6 +255,18 @@ int md200_kernel_report(int layers, int single_precision, char *json, int length
  * FMA throughput of `device` in flop/s (FMA = 2), FP64 when fp64 != 0 else FP32
  * -- the roofline denominator for the engine's CUDA-core kernels. */
 int md200_measure_peak(int device, int fp64, double *flops);
+
+/* The continuity screen alone, on host arrays: replaces the reference's
+ * continuity_screen module function (cpp/cpu/continuity_screen.hpp:8-67, bound at
+ * cpp/cpu/solver.cpp:775-777).  periods [T], velocity [B, K, T] float64 (pass
+ * float32 results widened, with single = 1, for the reference's float32 screen:
+ * values compared as float32 and the 16-ULP CLOSE_FP32 rule on), prediction
+ * [B, T] or NULL, bilateral = the envelope rule on.  Outputs flags [B, T] (the
+ * ENVELOPE 16, CLOSE_FP32 32, PREDICTION 64 and NO_BILATERAL 8 bits) and
+ * *suspect = 1 when any trace has one of the first three. */
+int md200_continuity_screen(int device, const double *periods, int T, const double *velocity, int B, int K,
+                            const uint32_t *prediction, int single, int bilateral, uint8_t *flags,
+                            int *suspect);
 
 /* Group velocities of one model's known ordered roots (guards included), for a
  * trace repaired outside the engine: replaces the plugin's _review_groups

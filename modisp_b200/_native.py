@@ -13,7 +13,7 @@ from pathlib import Path
 import numpy as np
 
 LIBRARY = Path(__file__).resolve().parent / "_lib" / "libmodisp_b200.so"
-ABI_VERSION = 1
+ABI_VERSION = 2
 STAT_NAMES = ("evaluations", "evaluations_fp32", "layer_steps", "layer_steps_fp32", "brackets",
               "trough_probes", "probe_pairs", "fp64_repair_traces", "unconverged", "group_roots",
               "roots", "traces", "dual_layer_steps", "continuation_accepted",
@@ -57,8 +57,9 @@ _I = ctypes.c_int
 EXPORTS = {
     "md200_default_options": (None, [ctypes.POINTER(Options)]),
     "md200_create": (_P, [_I, _I, _I, _I, _I, ctypes.POINTER(Options)]),
-    "md200_run": (_I, [_P, _P, _P, _P, _P, _I, _P, _P, _D, _D, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I]),
-    "md200_run_device": (_I, [_P, _P, _P, _P, _P, _I, _P, _P, _D, _D, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "md200_run": (_I, [_P, _P, _P, _P, _P, _I, _P, _P, _D, _D, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I]),
+    "md200_run_device": (_I, [_P, _P, _P, _P, _P, _I, _P, _P, _D, _D, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P,
+                              _P]),
     "md200_destroy": (None, [_P]),
     "md200_last_error": (ctypes.c_char_p, []),
     "md200_device_count": (_I, []),
@@ -72,10 +73,11 @@ EXPORTS = {
     "md200_stage_times": (_I, [_P, ctypes.POINTER(ctypes.c_double), _I]),
     "md200_kernel_launches": (_I, [_P]),
     "md200_measure_peak": (_I, [_I, _I, ctypes.POINTER(ctypes.c_double)]),
+    "md200_continuity_screen": (_I, [_I, _P, _I, _P, _I, _I, _P, _I, _I, _P, ctypes.POINTER(_I)]),
     "md200_run_ragged": (_I, [_P, _P, _P, _P, _P, _I, _P, _P, _P, _P, _D, _D, _I, _P, _P, _P, _P, _P, _P, _P,
-                              _I]),
+                              _P, _I]),
     "md200_run_ragged_device": (_I, [_P, _P, _P, _P, _P, _I, _I, _P, _P, _P, _P, _P, _D, _D, _I, _P, _P, _P, _P,
-                                     _P, _P, _P, _P]),
+                                     _P, _P, _P, _P, _P]),
     "md200_graph_begin": (_I, [_P]),
     "md200_graph_end": (_I, [_P]),
     "md200_graph_launch": (_I, [_P, _P]),
@@ -169,8 +171,10 @@ class Engine:
             raise RuntimeError("engine is closed")
         return self._handle
 
-    def run(self, h, vp, vs, rho, periods, bounds, tol, accept, wave, group=False, prediction=False):
-        """Host-array run; returns a dict of numpy outputs."""
+    def run(self, h, vp, vs, rho, periods, bounds, tol, accept, wave, group=False, prediction=False,
+            continuity=False):
+        """Host-array run; returns a dict of numpy outputs (``continuity_flags``
+        [B, T] uint8 with `continuity`: the continuity screen's flags)."""
         B, L = h.shape
         T, nm = self.periods, self.nmodes
         arrays = [np.ascontiguousarray(x, dtype=np.float64) for x in (h, vp, vs, rho)]
@@ -184,18 +188,21 @@ class Engine:
             out["group_velocity_flags"] = np.empty((B, nm, T), np.uint32)
         if prediction:
             out["prediction_flags"] = np.empty((B, T), np.uint32)
+        if continuity:
+            out["continuity_flags"] = np.empty((B, T), np.uint8)
         status = lib().md200_run(
             self.handle, *(ptr(a) for a in arrays), B, ptr(per), ptr(bnd), float(tol), float(accept),
             int(wave), ptr(out["velocity"]), ptr(out["flags"]), ptr(out["levels"]), ptr(out["counts"]),
             ptr(out.get("group_velocity")), ptr(out.get("group_velocity_flags")),
-            ptr(out.get("prediction_flags")), ptr(out["bounds"]), ptr(out["stats"]), STAT_COUNT)
+            ptr(out.get("prediction_flags")), ptr(out.get("continuity_flags")), ptr(out["bounds"]),
+            ptr(out["stats"]), STAT_COUNT)
         check(status)
         out["stats"] = dict(zip(STAT_NAMES, (int(x) for x in out["stats"])))
         return out
 
     def run_device(self, h, vp, vs, rho, models, periods, bounds, tol, accept, wave, velocity, flags,
                    levels, counts, group=None, group_flags=None, prediction=None, bounds_out=None,
-                   stats=None, stream=None):
+                   stats=None, stream=None, continuity=None):
         """Device-pointer run (integer addresses), enqueued on `stream` (a cudaStream_t
         address; None selects the engine's own stream, 0 the legacy default stream)."""
         c = ctypes.c_void_p
@@ -203,12 +210,12 @@ class Engine:
             self.handle, c(h), c(vp), c(vs), c(rho), int(models), c(periods), c(bounds) if bounds else None,
             float(tol), float(accept), int(wave), c(velocity), c(flags), c(levels), c(counts),
             c(group) if group else None, c(group_flags) if group_flags else None,
-            c(prediction) if prediction else None, c(bounds_out) if bounds_out else None,
-            c(stats) if stats else None, _stream_arg(stream))
+            c(prediction) if prediction else None, c(continuity) if continuity else None,
+            c(bounds_out) if bounds_out else None, c(stats) if stats else None, _stream_arg(stream))
         check(status)
 
     def run_ragged(self, h, vp, vs, rho, period_offsets, periods, modes, tol, accept, wave, group=False,
-                   bounds=None):
+                   bounds=None, continuity=False):
         """Ragged host-array run: model b has periods[period_offsets[b]:period_offsets[b+1]]
         and modes[b] modes.  Returns flat outputs: velocity (and group) as the
         concatenated [modes[b], T_b] blocks, trace arrays in CSR order."""
@@ -226,19 +233,22 @@ class Engine:
         if group:
             out["group_velocity"] = np.empty(cells)
             out["group_velocity_flags"] = np.empty(cells, np.uint32)
+        if continuity:
+            out["continuity_flags"] = np.empty(traces, np.uint8)
         bnd = None if bounds is None else np.ascontiguousarray(bounds, dtype=np.float64)
         if bnd is not None and bnd.shape != (B, 2):
             raise ValueError("bounds must be [models, 2]")
         check(lib().md200_run_ragged(self.handle, *(ptr(a) for a in arrays), B, ptr(off), ptr(per), ptr(md),
                                      ptr(bnd), float(tol), float(accept), int(wave), ptr(out["velocity"]), ptr(out["flags"]),
                                      ptr(out["levels"]), ptr(out["counts"]), ptr(out.get("group_velocity")),
-                                     ptr(out.get("group_velocity_flags")), ptr(out["stats"]), STAT_COUNT))
+                                     ptr(out.get("group_velocity_flags")), ptr(out.get("continuity_flags")),
+                                     ptr(out["stats"]), STAT_COUNT))
         out["stats"] = dict(zip(STAT_NAMES, (int(x) for x in out["stats"])))
         return out
 
     def run_ragged_device(self, h, vp, vs, rho, models, traces, period_offsets, periods, modes, out_offsets, tol,
                           accept, wave, velocity, flags, levels, counts, group=None, group_flags=None, stats=None,
-                          stream=None, bounds=None):
+                          stream=None, bounds=None, continuity=None):
         """Device-pointer ragged run (integer addresses), enqueued on `stream`."""
         c = ctypes.c_void_p
         opt = lambda x: c(x) if x else None
@@ -246,7 +256,8 @@ class Engine:
                                             c(period_offsets), c(periods), c(modes), c(out_offsets), opt(bounds),
                                             float(tol),
                                             float(accept), int(wave), c(velocity), c(flags), c(levels), c(counts),
-                                            opt(group), opt(group_flags), opt(stats), _stream_arg(stream)))
+                                            opt(group), opt(group_flags), opt(continuity), opt(stats),
+                                            _stream_arg(stream)))
 
     def jacobian(self, h, vp, vs, rho, periods, wave, velocity, group=None, want_group=True):
         """Host-array Jacobians of the roots `velocity` [B, nmodes, T]: returns
@@ -358,6 +369,27 @@ def measure_peak(device: int = 0, fp64: bool = False) -> float:
     out = ctypes.c_double()
     check(lib().md200_measure_peak(int(device), int(bool(fp64)), ctypes.byref(out)))
     return float(out.value)
+
+
+def continuity_screen(periods, velocity, prediction=None, bilateral=True, device: int = 0):
+    """The continuity screen on a result (md200_continuity_screen): (flags [B, T]
+    uint8, suspect bool).  float32 velocities are screened as the reference screens
+    float32 results (float32 comparisons and the 16-ULP rule)."""
+    p = np.ascontiguousarray(periods, dtype=np.float64).ravel()
+    v = np.asarray(velocity)
+    single = v.dtype == np.float32
+    v = np.ascontiguousarray(v, dtype=np.float64)
+    if v.ndim != 3 or v.shape[2] != p.size:
+        raise ValueError("continuity screening requires periods[T] and phases[B,K,T]")
+    B, K, T = v.shape
+    pred = None if prediction is None else np.ascontiguousarray(prediction, dtype=np.uint32)
+    if pred is not None and pred.shape != (B, T):
+        raise ValueError("prediction flags must have shape [B,T]")
+    flags = np.empty((B, T), np.uint8)
+    sus = ctypes.c_int()
+    check(lib().md200_continuity_screen(int(device), ptr(p), T, ptr(v), B, K, ptr(pred), int(single),
+                                        int(bool(bilateral)), ptr(flags), ctypes.byref(sus)))
+    return flags, bool(sus.value)
 
 
 def group_roots(h, vp, vs, rho, wave, period, roots, modes, close_rtol=.005):

@@ -91,7 +91,8 @@ class DispersionBatch:
                  secular=None, refinement=None, love_strategy=None, group_velocity=None,
                  group_velocity_flags=None, prediction_flags=None, group_rtol=None,
                  frequency_strategy="independent", frequency_strategy_used="independent",
-                 frequency_strategy_reason="independent frequency search requested", anchor_stride=4):
+                 frequency_strategy_reason="independent frequency search requested", anchor_stride=4,
+                 continuity_flags=None):
         self.phase_velocity = velocity
         self.precision = velocity.dtype.name
         self.refinement = refinement
@@ -110,7 +111,7 @@ class DispersionBatch:
                                     else np.isfinite(group_velocity) & (group_velocity_flags == 0))
         self.group_velocity_valid = self.group_velocity_mask
         self.prediction_flags = prediction_flags
-        self.continuity_flags = None
+        self.continuity_flags = continuity_flags
         self.group_rtol = group_rtol
         self.frequency_strategy = frequency_strategy
         self.frequency_strategy_used = frequency_strategy_used
@@ -337,7 +338,7 @@ class Solver:
     def _engine_for(self, capacity, L, T, nmodes):
         from . import plugin
         key = (self.device, L, T, int(nmodes), self.accuracy, self.close_root_rtol, self.precision,
-               self.group_velocity, self.frequency_strategy, self.anchor_stride,
+               self.group_velocity, self.frequency_strategy, self.anchor_stride, self.continuity_check,
                tuple(sorted(self.tuning.items())))
         if self._engine is not None and self._engine_key[0] == key and self._engine_key[1] >= capacity:
             return self._engine, False
@@ -351,7 +352,7 @@ class Solver:
             self.frequency_strategy == "anchor_continuation", self.anchor_stride,
             scan_density=float(t["scan_density"]), log_points=int(t["log_points"]),
             warps_per_block=int(t["warps_per_block"]), blocks_per_sm=int(t["blocks_per_sm"]),
-            device=self.device)
+            continuity_check=self.continuity_check, device=self.device)
         self._engine_key = (key, capacity)
         return self._engine, True
 
@@ -403,6 +404,9 @@ class Solver:
         bounds = np.empty((B, 2))
         group = np.empty((B, nmodes, per.size)) if self.group_velocity else None
         gflags = np.empty((B, nmodes, per.size), np.uint32) if self.group_velocity else None
+        # the continuity screen runs in the FP32-scan engine (continuity_check)
+        screened = self.precision != "float64" and self.continuity_check
+        cflags = np.empty((B, per.size), np.uint8) if screened else None
         stats = {}
         chunks = 0
         wave_code = int(wave == "love")
@@ -410,7 +414,7 @@ class Solver:
             end = min(B, start + capacity)
             out = engine._engine.run(h[start:end], a[start:end], b[start:end], r[start:end], per,
                                      bounds_in[start:end], self.c_tol_rel, self.f_accept, wave_code,
-                                     group=self.group_velocity)
+                                     group=self.group_velocity, continuity=screened)
             velocity[start:end] = out["velocity"]
             flags[start:end] = out["flags"]
             levels[start:end] = out["levels"]
@@ -419,6 +423,8 @@ class Solver:
             if self.group_velocity:
                 group[start:end] = out["group_velocity"]
                 gflags[start:end] = out["group_velocity_flags"]
+            if screened:
+                cflags[start:end] = out["continuity_flags"]
             for k, v in out["stats"].items():
                 stats[k] = stats.get(k, 0) + int(v)
             chunks += 1
@@ -426,6 +432,8 @@ class Solver:
             raise ValueError("automatic search range could not be constructed")
         if inverse is not None:
             velocity, flags, levels, counts = (x.take(inverse, axis=-1) for x in (velocity, flags, levels, counts))
+            if cflags is not None:
+                cflags = cflags.take(inverse, axis=-1)
             if group is not None:
                 group, gflags = group.take(inverse, axis=-1), gflags.take(inverse, axis=-1)
         if self.cmin is not None or self.cmax is not None:
@@ -454,7 +462,7 @@ class Solver:
             love_strategy=self.love_strategy if wave == "love" else None, group_velocity=group,
             group_velocity_flags=gflags, prediction_flags=None,
             group_rtol=self.group_rtol if self.group_velocity else None,
-            frequency_strategy=self.frequency_strategy, anchor_stride=self.anchor_stride)
+            frequency_strategy=self.frequency_strategy, anchor_stride=self.anchor_stride, continuity_flags=cflags)
         self.last_result = result
         return result
 

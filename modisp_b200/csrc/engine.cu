@@ -114,6 +114,7 @@ struct md200_engine {
          *in_per = nullptr, *in_bounds = nullptr;
   double *out_vel = nullptr, *out_grp = nullptr;
   unsigned *out_flags = nullptr, *out_gflags = nullptr, *out_pred = nullptr;
+  unsigned char *out_cflags = nullptr;
   int *out_levels = nullptr, *out_counts = nullptr;
   unsigned long long *d_stats = nullptr;
   unsigned char *pinned = nullptr;
@@ -132,6 +133,7 @@ struct md200_engine {
   static constexpr int NSTAGE = 10;
   cudaEvent_t ev[NSTAGE + 1] = {};
   bool profiling = false;
+  int last_launches = -1;  // kernels launched by the last run (enqueue)
   // CUDA graph of the calls captured between md200_graph_begin and md200_graph_end
   bool capturing = false;
   cudaGraph_t graph = nullptr;
@@ -216,10 +218,14 @@ int setup(md200_engine *e) {
       own_alloc(e, &e->out_vel, nt * nm) || own_alloc(e, &e->out_grp, nt * nm) ||
       own_alloc(e, &e->out_gflags, nt * nm) || own_alloc(e, &e->out_flags, nt) ||
       own_alloc(e, &e->out_pred, nt) || own_alloc(e, &e->out_levels, nt) ||
-      own_alloc(e, &e->out_counts, nt))
+      own_alloc(e, &e->out_counts, nt) || own_alloc(e, &e->out_cflags, nt))
+    return 1;
+  // roots and counts of continuity suspects before their FP64 re-scan
+  if (d.fp32 && e->o.continuity_check &&
+      (own_alloc(e, &d.cold, nt * nm) || own_alloc(e, &d.ccount, nt)))
     return 1;
   e->pinned_bytes = sizeof(double) * (4 * static_cast<size_t>(B) * L + T + 2 * static_cast<size_t>(B)) +
-                    nt * nm * (2 * sizeof(double) + sizeof(unsigned)) + nt * 4 * sizeof(int) +
+                    nt * nm * (2 * sizeof(double) + sizeof(unsigned)) + nt * 4 * sizeof(int) + nt +
                     md200_engine::MAX_CHUNKS * MD200_STAT_COUNT * sizeof(unsigned long long) +
                     2 * sizeof(double) * B + 64;
   MD200_CK(cudaMallocHost(reinterpret_cast<void **>(&e->pinned), e->pinned_bytes));
@@ -287,7 +293,7 @@ struct Ragged {
 int enqueue(md200_engine *e, const double *h, const double *vp, const double *vs, const double *rho,
             int B, const double *periods, const double *bounds, double tol, double accept, int wave,
             double *vel, unsigned *flags, int *levels, int *counts, double *grp, unsigned *gflags,
-            unsigned *pred, double *bounds_out, unsigned long long *stats, cudaStream_t s,
+            unsigned *pred, unsigned char *cflags, double *bounds_out, unsigned long long *stats, cudaStream_t s,
             const Ragged &rg = Ragged()) {
   if (!(tol > 0.) || !(tol < 1.)) return fail("modisp_b200: c_tol_rel must lie in (0, 1)");
   if (wave != 0 && wave != 1) return fail("modisp_b200: wave must be 0 (Rayleigh) or 1 (Love)");
@@ -318,8 +324,12 @@ int enqueue(md200_engine *e, const double *h, const double *vp, const double *vs
   d.gflags = gflags;
   d.stats = stats;
   d.pred = pred;
+  const bool screen = d.fp32 && e->o.continuity_check;
+  d.cflags = screen ? cflags : nullptr;
+  if (!d.cflags) d.cold = nullptr, d.ccount = nullptr;
   d.bounds_out = bounds_out;
   const int nt = d.n_traces;
+  int nl = 0;  // kernels launched by this run
   MD200_CK(cudaMemsetAsync(d.ctr, 0, sizeof(int) * C_COUNT, s));
   if (stats) MD200_CK(cudaMemsetAsync(stats, 0, sizeof(unsigned long long) * MD200_STAT_COUNT, s));
   // stage marks: 0 prep, 1 init, 2 scan, 3 refine, 4 repair collect, 5 repair scan,
@@ -330,12 +340,15 @@ int enqueue(md200_engine *e, const double *h, const double *vp, const double *vs
   MD200_CK(mark(0));
   const int pw = e->prep_warps;
   prep_models<<<(B + pw - 1) / pw, 32 * pw, e->prep_smem, s>>>(d, e->sortcap, 0);
+  ++nl;
   MD200_CK(cudaGetLastError());
   MD200_CK(mark(1));
   init_traces<<<(nt + 255) / 256, 256, 0, s>>>(d);
+  ++nl;
   MD200_CK(cudaGetLastError());
   if (d.fp32) {
     tail_values<<<(nt + 127) / 128, 128, 0, s>>>(d);
+    ++nl;
     MD200_CK(cudaGetLastError());
   }
   MD200_CK(mark(2));
@@ -346,14 +359,17 @@ int enqueue(md200_engine *e, const double *h, const double *vp, const double *vs
     else if (d.fp32) scan<float, 1><<<grid, block, sm, s>>>(d, d.trace_list, C_SCAN_CURSOR, C_NTRACE);
     else if (wave == 0) scan<double, 0><<<grid, block, sm, s>>>(d, d.trace_list, C_SCAN_CURSOR, C_NTRACE);
     else scan<double, 1><<<grid, block, sm, s>>>(d, d.trace_list, C_SCAN_CURSOR, C_NTRACE);
+    ++nl;
   }
   MD200_CK(cudaGetLastError());
   MD200_CK(mark(3));
   refine<<<e->list_blocks, 128, 0, s>>>(d);
+  ++nl;
   MD200_CK(cudaGetLastError());
   MD200_CK(mark(4));
   if (d.fp32) {
     collect_repairs<<<(nt + 255) / 256, 256, 0, s>>>(d);
+    ++nl;
     MD200_CK(mark(5));
     if (wave == 0)
       scan<double, 0><<<e->scan_blocks64, 32 * e->scan_warps, e->scan_smem64, s>>>(d, d.repair_list,
@@ -361,8 +377,10 @@ int enqueue(md200_engine *e, const double *h, const double *vp, const double *vs
     else
       scan<double, 1><<<e->scan_blocks64, 32 * e->scan_warps, e->scan_smem64, s>>>(d, d.repair_list,
                                                                                  C_REPAIR_CURSOR, C_NREPAIR);
+    ++nl;
     MD200_CK(mark(6));
     refine<<<e->list_blocks, 128, 0, s>>>(d);
+    ++nl;
     MD200_CK(cudaGetLastError());
   } else {
     MD200_CK(mark(5));
@@ -370,18 +388,21 @@ int enqueue(md200_engine *e, const double *h, const double *vp, const double *vs
   }
   MD200_CK(mark(7));
   assemble<<<(nt + 255) / 256, 256, 0, s>>>(d);
+  ++nl;
   MD200_CK(cudaGetLastError());
   MD200_CK(mark(8));
   if (d.group) {
     group_velocity<<<e->list_blocks, 128, 0, s>>>(d);
+    ++nl;
     MD200_CK(cudaGetLastError());
   }
   MD200_CK(mark(9));
-  if (d.fp32 && e->o.continuity_check) {
-    // FP64 continuity recheck: suspects of the bilateral envelope screen are
-    // re-scanned in FP64, refined, assembled and given group velocities again
+  if (screen) {
+    // FP64 continuity recheck: suspects of the continuity screen are re-scanned
+    // in FP64, refined, assembled and given group velocities again
     MD200_CK(cudaMemsetAsync(d.ctr + C_REPAIR_CURSOR, 0, 2 * sizeof(int), s));
     continuity_screen<<<(nt + 255) / 256, 256, 0, s>>>(d);
+    ++nl;
     MD200_CK(cudaGetLastError());
     if (wave == 0)
       scan<double, 0><<<e->scan_blocks64, 32 * e->scan_warps, e->scan_smem64, s>>>(d, d.repair_list,
@@ -389,17 +410,30 @@ int enqueue(md200_engine *e, const double *h, const double *vp, const double *vs
     else
       scan<double, 1><<<e->scan_blocks64, 32 * e->scan_warps, e->scan_smem64, s>>>(d, d.repair_list,
                                                                                  C_REPAIR_CURSOR, C_NREPAIR);
+    ++nl;
     MD200_CK(cudaGetLastError());
     refine<<<e->list_blocks, 128, 0, s>>>(d);
+    ++nl;
     assemble<<<(nt + 255) / 256, 256, 0, s>>>(d, d.repair_list, C_NREPAIR);
+    ++nl;
     MD200_CK(cudaGetLastError());
     if (d.group) {
       group_velocity<<<e->list_blocks, 128, 0, s>>>(d);
+      ++nl;
       MD200_CK(cudaGetLastError());
     }
+    if (d.cflags) {
+      continuity_finish<<<(nt + 255) / 256, 256, 0, s>>>(d);
+      ++nl;
+      MD200_CK(cudaGetLastError());
+    }
+  } else if (cflags) {
+    // no screen in this engine: every trace unscreened
+    MD200_CK(cudaMemsetAsync(cflags, 0, static_cast<size_t>(nt), s));
   }
   MD200_CK(mark(10));
   if (!e->capturing) e->profiling = true;
+  e->last_launches = nl;
   return 0;
 }
 
@@ -539,21 +573,21 @@ int md200_run_device(md200_engine *e, const double *h, const double *vp, const d
                      const double *rho, int models, const double *periods, const double *bounds,
                      double tol, double accept, int wave, double *velocity, unsigned *flags,
                      int *levels, int *counts, double *group, unsigned *group_flags,
-                     unsigned *prediction_flags, double *bounds_out, unsigned long long *stats,
-                     void *stream) {
+                     unsigned *prediction_flags, uint8_t *continuity_flags, double *bounds_out,
+                     unsigned long long *stats, void *stream) {
   if (validate_geometry(e, models)) return 1;
   if (!h || !vp || !vs || !rho || !periods || !velocity || !flags || !levels || !counts)
     return fail("modisp_b200: missing input or output array");
   cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : e->stream;
   return enqueue(e, h, vp, vs, rho, models, periods, bounds, tol, accept, wave, velocity, flags,
-                 levels, counts, group, group_flags, prediction_flags, bounds_out, stats, s);
+                 levels, counts, group, group_flags, prediction_flags, continuity_flags, bounds_out, stats, s);
 }
 
 int md200_run(md200_engine *e, const double *h, const double *vp, const double *vs,
               const double *rho, int models, const double *periods, const double *bounds,
               double tol, double accept, int wave, double *velocity, unsigned *flags, int *levels,
               int *counts, double *group, unsigned *group_flags, unsigned *prediction_flags,
-              double *bounds_out, unsigned long long *stats, int nstats) {
+              uint8_t *continuity_flags, double *bounds_out, unsigned long long *stats, int nstats) {
   try {
     if (validate_geometry(e, models)) return 1;
     if (!h || !vp || !vs || !rho || !periods || !velocity || !flags || !levels || !counts)
@@ -601,6 +635,7 @@ int md200_run(md200_engine *e, const double *h, const double *vp, const double *
     unsigned long long *ost = reinterpret_cast<unsigned long long *>(
         (reinterpret_cast<uintptr_t>(opr + nt) + 7) & ~uintptr_t(7));
     double *obd = reinterpret_cast<double *>(ost + static_cast<size_t>(MD200_STAT_COUNT) * md200_engine::MAX_CHUNKS);
+    unsigned char *ocf = reinterpret_cast<unsigned char *>(obd + 2 * B);
     auto chunk_begin = [&](int c) { return B * c / nchunk; };
     for (int c = 0; c < nchunk; ++c) {
       const size_t b0 = chunk_begin(c), nb = chunk_begin(c + 1) - b0;
@@ -610,7 +645,8 @@ int md200_run(md200_engine *e, const double *h, const double *vp, const double *
                   static_cast<int>(nb), e->in_per, bounds ? e->in_bounds + 2 * b0 : nullptr, tol, accept, wave,
                   e->out_vel + cm, e->out_flags + ct, e->out_levels + ct, e->out_counts + ct,
                   grp ? e->out_grp + cm : nullptr, grp ? e->out_gflags + cm : nullptr,
-                  prediction_flags ? e->out_pred + ct : nullptr, e->in_bounds + 2 * b0, cstats, s))
+                  prediction_flags ? e->out_pred + ct : nullptr, continuity_flags ? e->out_cflags + ct : nullptr,
+                  e->in_bounds + 2 * b0, cstats, s))
         return 1;
       MD200_CK(cudaMemcpyAsync(ov + cm, e->out_vel + cm, sizeof(double) * cells, cudaMemcpyDeviceToHost, s));
       MD200_CK(cudaMemcpyAsync(ofl + ct, e->out_flags + ct, sizeof(unsigned) * traces, cudaMemcpyDeviceToHost, s));
@@ -622,6 +658,8 @@ int md200_run(md200_engine *e, const double *h, const double *vp, const double *
       }
       if (prediction_flags)
         MD200_CK(cudaMemcpyAsync(opr + ct, e->out_pred + ct, sizeof(unsigned) * traces, cudaMemcpyDeviceToHost, s));
+      if (continuity_flags)
+        MD200_CK(cudaMemcpyAsync(ocf + ct, e->out_cflags + ct, traces, cudaMemcpyDeviceToHost, s));
       // the prep stage wrote the windows it used over the (already consumed) input windows
       if (bounds_out)
         MD200_CK(cudaMemcpyAsync(obd + 2 * b0, e->in_bounds + 2 * b0, sizeof(double) * 2 * nb,
@@ -643,6 +681,7 @@ int md200_run(md200_engine *e, const double *h, const double *vp, const double *
         out.push_back({group_flags + cm, ogf + cm, sizeof(unsigned) * cells});
       }
       if (prediction_flags) out.push_back({prediction_flags + ct, opr + ct, sizeof(unsigned) * traces});
+      if (continuity_flags) out.push_back({continuity_flags + ct, ocf + ct, traces});
       if (bounds_out) out.push_back({bounds_out + 2 * b0, obd + 2 * b0, sizeof(double) * 2 * nb});
       parallel_copy(out);
     }
@@ -760,7 +799,8 @@ int md200_run_ragged_device(md200_engine *e, const double *h, const double *vp, 
                             const double *rho, int models, int traces, const int *period_offsets,
                             const double *periods, const int *modes, const long long *out_offsets,
                             const double *bounds, double tol, double accept, int wave, double *velocity, unsigned *flags, int *levels, int *counts,
-                            double *group, unsigned *group_flags, unsigned long long *stats, void *stream) {
+                            double *group, unsigned *group_flags, uint8_t *continuity_flags, unsigned long long *stats,
+                            void *stream) {
   if (validate_geometry(e, models)) return 1;
   if (traces < 1 || static_cast<long long>(traces) > static_cast<long long>(e->cap) * e->T)
     return fail("modisp_b200: ragged trace count " + std::to_string(traces) + " outside 1.." +
@@ -775,13 +815,14 @@ int md200_run_ragged_device(md200_engine *e, const double *h, const double *vp, 
   rg.modes = modes;
   rg.outbase = out_offsets;
   return enqueue(e, h, vp, vs, rho, models, periods, bounds, tol, accept, wave, velocity, flags, levels, counts,
-                 group, group_flags, nullptr, nullptr, stats, s, rg);
+                 group, group_flags, nullptr, continuity_flags, nullptr, stats, s, rg);
 }
 
 int md200_run_ragged(md200_engine *e, const double *h, const double *vp, const double *vs, const double *rho,
                      int models, const int *period_offsets, const double *periods, const int *modes,
                      const double *bounds, double tol, double accept, int wave, double *velocity, unsigned *flags, int *levels, int *counts,
-                     double *group, unsigned *group_flags, unsigned long long *stats, int nstats) {
+                     double *group, unsigned *group_flags, uint8_t *continuity_flags, unsigned long long *stats,
+                     int nstats) {
   try {
     if (validate_geometry(e, models)) return 1;
     if (!h || !vp || !vs || !rho || !period_offsets || !periods || !modes || !velocity || !flags || !levels ||
@@ -833,7 +874,8 @@ int md200_run_ragged(md200_engine *e, const double *h, const double *vp, const d
     if (enqueue(e, e->in_h, e->in_vp, e->in_vs, e->in_rho, models, e->rg_periods, bounds ? e->in_bounds : nullptr,
                 tol, accept, wave,
                 e->out_vel, e->out_flags, e->out_levels, e->out_counts, grp ? e->out_grp : nullptr,
-                grp ? e->out_gflags : nullptr, nullptr, nullptr, e->d_stats, s, rg))
+                grp ? e->out_gflags : nullptr, nullptr, continuity_flags ? e->out_cflags : nullptr, nullptr,
+                e->d_stats, s, rg))
       return 1;
     MD200_CK(cudaStreamSynchronize(s));
     MD200_CK(cudaMemcpy(velocity, e->out_vel, sizeof(double) * cells, cudaMemcpyDeviceToHost));
@@ -844,6 +886,7 @@ int md200_run_ragged(md200_engine *e, const double *h, const double *vp, const d
       MD200_CK(cudaMemcpy(group, e->out_grp, sizeof(double) * cells, cudaMemcpyDeviceToHost));
       MD200_CK(cudaMemcpy(group_flags, e->out_gflags, sizeof(unsigned) * cells, cudaMemcpyDeviceToHost));
     }
+    if (continuity_flags) MD200_CK(cudaMemcpy(continuity_flags, e->out_cflags, traces, cudaMemcpyDeviceToHost));
     if (stats && nstats > 0)
       MD200_CK(cudaMemcpy(stats, e->d_stats, sizeof(unsigned long long) * std::min(nstats, int(MD200_STAT_COUNT)),
                           cudaMemcpyDeviceToHost));
@@ -904,6 +947,8 @@ int md200_stage_times(md200_engine *e, double *ms, int n) {
 
 int md200_kernel_launches(md200_engine *e) {
   if (!e) return -1;
+  if (e->last_launches >= 0) return e->last_launches;  // counted by the last run
+  // before any run: the launches of a run without continuity flags requested
   const int check = e->d.fp32 && e->o.continuity_check ? 4 + (e->d.group ? 1 : 0) : 0;
   return 6 + (e->d.fp32 ? 4 : 0) - (e->d.group ? 0 : 1) + check;
 }
@@ -1226,6 +1271,49 @@ int md200_mode_reliability(int device, const double *velocity, const uint32_t *t
   if (err == cudaSuccess) err = sync;
   if (err != cudaSuccess) return fail(std::string("modisp_b200 CUDA: ") + cudaGetErrorString(err));
   return 0;
+}
+
+int md200_continuity_screen(int device, const double *periods, int T, const double *velocity, int B, int K,
+                            const uint32_t *prediction, int single, int bilateral, uint8_t *flags, int *suspect) {
+  try {
+    if (T < 1 || B < 1 || K < 1 || !periods || !velocity || !flags)
+      return fail("modisp_b200: continuity screening requires periods[T] and phases[B,K,T]");
+    // period order as the reference takes it: ascending as given, else sorted
+    // (cpp/cpu/continuity_screen.hpp:30-34; the same std::sort)
+    std::vector<int> order(T);
+    for (int j = 0; j < T; ++j) order[j] = j;
+    if (bilateral && T > 2 && !std::is_sorted(periods, periods + T))
+      std::sort(order.begin(), order.end(), [&](int i, int j) { return periods[i] < periods[j]; });
+    MD200_CK(cudaSetDevice(device));
+    const size_t traces = static_cast<size_t>(B) * T, cells = traces * K;
+    const size_t bytes = sizeof(double) * (T + cells) + sizeof(int) * (T + 1) + sizeof(unsigned) * traces + traces;
+    unsigned char *buf = nullptr;
+    MD200_CK(cudaMalloc(&buf, bytes));
+    double *dper = reinterpret_cast<double *>(buf), *dvel = dper + T;
+    int *dord = reinterpret_cast<int *>(dvel + cells), *dsus = dord + T;
+    unsigned *dpred = reinterpret_cast<unsigned *>(dsus + 1);
+    unsigned char *dout = reinterpret_cast<unsigned char *>(dpred + traces);
+    cudaError_t err = cudaMemcpy(dper, periods, sizeof(double) * T, cudaMemcpyHostToDevice);
+    if (err == cudaSuccess) err = cudaMemcpy(dvel, velocity, sizeof(double) * cells, cudaMemcpyHostToDevice);
+    if (err == cudaSuccess) err = cudaMemcpy(dord, order.data(), sizeof(int) * T, cudaMemcpyHostToDevice);
+    if (err == cudaSuccess && prediction)
+      err = cudaMemcpy(dpred, prediction, sizeof(unsigned) * traces, cudaMemcpyHostToDevice);
+    if (err == cudaSuccess) err = cudaMemset(dsus, 0, sizeof(int));
+    if (err == cudaSuccess) {
+      continuity_screen_plain<<<static_cast<unsigned>((traces + 255) / 256), 256>>>(
+          dper, dord, T, dvel, B, K, prediction ? dpred : nullptr, single, bilateral, dout, dsus);
+      err = cudaGetLastError();
+    }
+    int sus = 0;
+    if (err == cudaSuccess) err = cudaMemcpy(flags, dout, traces, cudaMemcpyDeviceToHost);
+    if (err == cudaSuccess) err = cudaMemcpy(&sus, dsus, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(buf);
+    if (err != cudaSuccess) return fail(std::string("modisp_b200 CUDA: ") + cudaGetErrorString(err));
+    if (suspect) *suspect = sus;
+    return 0;
+  } catch (...) {
+    return fail_exception();
+  }
 }
 
 int md200_measure_peak(int device, int fp64, double *flops) {

@@ -89,7 +89,16 @@ struct Dev {
   double *gwin;     // [B][nmodes][T][2]
   double *bounds_out;  // [B][2] windows used (optional)
   unsigned *pred;      // [B][T] prediction flags (optional)
+  unsigned char *cflags;  // [B][T] continuity-screen flags (optional; FP32-scan runs)
+  double *cold;        // [n_traces][nmodes] roots of the screen's suspects before their FP64 re-scan
+  int *ccount;         // [n_traces] root counts of those suspects before the re-scan
   unsigned long long *stats;
 };
+
+// Continuity-screen flags (python/modisp/_continuity.py:6-14).
+constexpr unsigned char CONT_REVIEWED = 1, CONT_REPAIRED = 2, CONT_UNRESOLVED = 4, CONT_NO_BILATERAL = 8,
+                        CONT_ENVELOPE = 16, CONT_CLOSE_FP32 = 32, CONT_PREDICTION = 64;
+// PredictionFlag.REVIEW (python/modisp/__init__.py:55-68).
+constexpr unsigned PRED_REVIEW = 4096;
 
 }  // namespace md200

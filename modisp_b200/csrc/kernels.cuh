@@ -1414,14 +1414,25 @@ __global__ void __launch_bounds__(128, 4) refine(Dev d) {
   }
 }
 
+// Every pass after the first re-solves a set of traces: its scan appends
+// brackets to the refine list and its assembly roots to the group list.  The
+// previous pass's entries are consumed by then, so each pass restarts both lists
+// at zero and needs at most one pass's capacity (KB brackets and nmodes roots per
+// trace).  Called by the first thread of the pass's collecting kernel.
+__device__ __forceinline__ void restart_refine_list(const Dev &d) {
+  d.ctr[C_NREFINE] = d.ctr[C_REFINE_BEGIN] = d.ctr[C_REFINE_CURSOR] = 0;
+}
+__device__ __forceinline__ void restart_lists(const Dev &d) {
+  restart_refine_list(d);
+  d.ctr[C_NGROUP] = d.ctr[C_GROUP_BEGIN] = 0;
+}
+
 // ---------------------------------------------------------------------------
 // collect_repairs: traces whose FP32 scan FP64 did not confirm.
 // ---------------------------------------------------------------------------
 __global__ void collect_repairs(Dev d) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t == 0) {
-    d.ctr[C_REFINE_BEGIN] = d.ctr[C_REFINE_CURSOR] = d.ctr[C_NREFINE];
-  }
+  if (t == 0) restart_refine_list(d);
   if (t >= d.n_traces) return;
   const unsigned fl = d.tflags[t];
   if (fl & INTERNAL_REPAIR) {
@@ -1554,25 +1565,83 @@ __global__ void assemble(Dev d, const int *list = nullptr, int count_id = 0) {
 
 // ---------------------------------------------------------------------------
 // continuity_screen: one thread per trace of an FP32-scan run, after assembly.
-// A trace is suspect when, with both neighbouring periods of its model within
-// a log step of 0.25 (the nearest shorter and longer period, in value order),
-// some mode has roots at both neighbours but is missing here or lies outside
-// [0.95 min, 1.05 max] of them -- the bilateral envelope of the reference's
-// continuity screen (cpp/cpu/continuity_screen.hpp:8-67).  Suspects are queued
-// for an FP64 re-scan (the repair list); their old roots are taken out of the
-// root count, their group-velocity entries re-queued.
+// The rules of the reference's screen (cpp/cpu/continuity_screen.hpp:8-67) on
+// the phase velocities as float32 values (the precision of the reference's
+// FP32 results, which its screen sees as float32):
+//   ENVELOPE (16)   with the neighbouring periods of the model (in period order)
+//                   within a log step of 0.25, a mode with roots at both that is
+//                   missing here or outside [0.95 min, 1.05 max] of them;
+//   CLOSE_FP32 (32) adjacent modes within 16 float32 ULPs;
+//   PREDICTION (64) a continuation prediction marked for review;
+//   NO_BILATERAL (8) until some mode has roots at both neighbours.
+// Suspects (16 | 32 | 64) are REVIEWED (1) and queued for an FP64 re-scan (the
+// repair list) unless FP64 already re-solved them in this run; their roots and
+// count are kept in d.cold / d.ccount for continuity_finish, their old roots are
+// taken out of the root count and their group-velocity entries re-queued.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ double log_step(double target, double anchor) {
+  // cpp/common/continuation.hpp:12-15
+  return fabs(target - anchor) < .5 * anchor ? log1p((target - anchor) / anchor) : log(target) - log(anchor);
+}
+__device__ __forceinline__ double as_float(double x) { return static_cast<double>(static_cast<float>(x)); }
+
+// The screen's flags of one trace: its nm roots at vel[o + k s], those of its
+// neighbouring periods at vel[ol + k sl] and vel[orr + k sr] (read only when
+// `interior`), its prediction word.  `single`: the roots are compared as
+// float32 values and the CLOSE_FP32 rule applies (the reference's screen of
+// float32 results); `bilateral`: the envelope rule is on.
+__device__ __forceinline__ unsigned screen_flag(const double *vel, size_t o, int s, size_t ol, int sl, size_t orr,
+                                                int sr, bool interior, int nm, unsigned pred, bool single,
+                                                bool bilateral) {
+  unsigned flag = bilateral ? CONT_NO_BILATERAL : 0u;
+  interior = interior && bilateral;
+  if (interior || (bilateral && single && nm > 1)) {
+    double prev = NAN;
+    for (int k = 0; k < nm; ++k) {
+      double c = vel[o + static_cast<size_t>(k) * s];
+      if (single) c = as_float(c);
+      if (interior) {
+        double cl = vel[ol + static_cast<size_t>(k) * sl], cr = vel[orr + static_cast<size_t>(k) * sr];
+        if (single) cl = as_float(cl), cr = as_float(cr);
+        if (isfinite(cl) && isfinite(cr)) {
+          flag &= ~CONT_NO_BILATERAL;
+          if (!isfinite(c) || c < .95 * fmin(cl, cr) || c > 1.05 * fmax(cl, cr)) flag |= CONT_ENVELOPE;
+        }
+      }
+      if (single && k && isfinite(c) && isfinite(prev)) {
+        const unsigned x = __float_as_uint(static_cast<float>(c)), y = __float_as_uint(static_cast<float>(prev));
+        if ((x > y ? x - y : y - x) <= 16u) flag |= CONT_CLOSE_FP32;
+      }
+      prev = c;
+    }
+  }
+  if (pred & PRED_REVIEW) flag |= CONT_PREDICTION;
+  return flag;
+}
+
+// The screen alone on a [B][K][T] result (the reference's module function,
+// cpp/cpu/continuity_screen.hpp:8-67): one thread per (model, period rank);
+// `order` is the period order the host chose (identity for ascending periods).
+__global__ void continuity_screen_plain(const double *periods, const int *order, int T, const double *vel, int B,
+                                        int K, const unsigned *pred, int single, int bilateral,
+                                        unsigned char *out, int *suspect) {
+  const long long q = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (q >= static_cast<long long>(B) * T) return;
+  const int b = static_cast<int>(q / T), j = static_cast<int>(q - static_cast<long long>(b) * T);
+  const int f = order[j], l = order[j > 0 ? j - 1 : j], r = order[j + 1 < T ? j + 1 : j];
+  const bool interior = j > 0 && j + 1 < T && log_step(periods[r], periods[l]) <= .25;
+  const size_t base = static_cast<size_t>(b) * K * T;
+  const unsigned flag = screen_flag(vel, base + f, T, base + l, T, base + r, T, interior, K,
+                                    pred ? pred[static_cast<size_t>(b) * T + f] : 0u, single != 0, bilateral != 0);
+  out[static_cast<size_t>(b) * T + f] = static_cast<unsigned char>(flag);
+  if (flag & (CONT_ENVELOPE | CONT_CLOSE_FP32 | CONT_PREDICTION)) *suspect = 1;
+}
+
 __global__ void continuity_screen(Dev d) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t == 0) {
-    d.ctr[C_REFINE_BEGIN] = d.ctr[C_REFINE_CURSOR] = d.ctr[C_NREFINE];
-    d.ctr[C_GROUP_BEGIN] = d.ctr[C_NGROUP];
-  }
+  if (t == 0) restart_lists(d);
   if (t >= d.n_traces) return;
   const int b = d.tr_model[t];
-  if (d.mstate[b] != 0) return;
-  const unsigned fl = d.tflags[t];
-  if (fl & (TRACE_FP64_REPAIR | TRACE_SEARCH_UNCONVERGED)) return;
   // the model's traces
   int first, count;
   if (d.ragged) {
@@ -1582,38 +1651,72 @@ __global__ void continuity_screen(Dev d) {
     first = b * d.T;
     count = d.T;
   }
+  // neighbours in period order: the nearest shorter and longer periods
   const double p = d.tr_period[t];
   int l = -1, r = -1;
-  double pl = 0., pr = INFINITY;
+  double pl = -INFINITY, pr = INFINITY;
   for (int j = 0; j < count; ++j) {
     const double q = d.tr_period[first + j];
     if (q < p && q > pl) { pl = q; l = first + j; }
     if (q > p && q < pr) { pr = q; r = first + j; }
   }
-  if (l < 0 || r < 0 || !(log(pr / pl) <= .25)) return;
+  const bool interior = l >= 0 && r >= 0 && log_step(pr, pl) <= .25;
   const int nm = d.tr_modes[t];
-  const size_t o = static_cast<size_t>(d.tr_out[t]), ol = static_cast<size_t>(d.tr_out[l]),
-               orr = static_cast<size_t>(d.tr_out[r]);
-  const int s = d.tr_stride[t], sl = d.tr_stride[l], sr = d.tr_stride[r];
-  bool suspect = false;
-  for (int k = 0; k < nm && !suspect; ++k) {
-    const double cl = d.vel[ol + static_cast<size_t>(k) * sl], cr = d.vel[orr + static_cast<size_t>(k) * sr];
-    if (!(isfinite(cl) && isfinite(cr))) continue;
-    const double c = d.vel[o + static_cast<size_t>(k) * s];
-    suspect = !isfinite(c) || c < .95 * fmin(cl, cr) || c > 1.05 * fmax(cl, cr);
+  const size_t o = static_cast<size_t>(d.tr_out[t]);
+  const int s = d.tr_stride[t];
+  unsigned flag = screen_flag(d.vel, o, s, interior ? static_cast<size_t>(d.tr_out[l]) : 0, interior ? d.tr_stride[l] : 0,
+                              interior ? static_cast<size_t>(d.tr_out[r]) : 0, interior ? d.tr_stride[r] : 0, interior,
+                              nm, d.pred ? d.pred[t] : 0u, true, true);
+  const bool suspect = (flag & (CONT_ENVELOPE | CONT_CLOSE_FP32 | CONT_PREDICTION)) != 0;
+  if (suspect) flag |= CONT_REVIEWED;
+  if (d.cflags) d.cflags[t] = static_cast<unsigned char>(flag);
+  const unsigned fl = d.tflags[t];
+  if (!suspect || d.mstate[b] != 0 || (fl & TRACE_FP64_REPAIR)) return;  // FP64 already solved it
+  if (d.cold) {  // (by trace: tr_modes[t] <= nmodes)
+    double *keep = d.cold + static_cast<size_t>(t) * d.nmodes;
+    for (int k = 0; k < nm; ++k) keep[k] = d.vel[o + static_cast<size_t>(k) * s];
+    d.ccount[t] = d.ocounts[t];
   }
-  if (!suspect) return;
   const int pos = atomicAdd(&d.ctr[C_NREPAIR], 1);
   d.repair_list[pos] = t;
-  d.tflags[t] = fl | TRACE_FP64_REPAIR;
+  d.tflags[t] = TRACE_FP64_REPAIR;  // the FP64 scan sets its own search flags afresh
   d.nbr[t] = 0;
   atomicAdd(&d.ctr[C_NSUSPECT], 1);
   if (d.stats) {
     int finite = 0;
     for (int k = 0; k < nm; ++k) finite += isfinite(d.vel[o + static_cast<size_t>(k) * s]);
     if (finite) atomicAdd(&d.stats[10], static_cast<unsigned long long>(-finite));
+    if (fl & TRACE_SEARCH_UNCONVERGED) atomicAdd(&d.stats[8], static_cast<unsigned long long>(-1LL));
     atomicAdd(&d.stats[15], 1ULL);
   }
+}
+
+// continuity_finish: one thread per re-scanned suspect, after its FP64 re-solve.
+// REPAIRED (2) when the root count or a root moved by more than the refinement
+// tolerance (the reference adopts a review result under that test,
+// python/modisp/_continuity.py:96-100); UNRESOLVED (4) when the FP64 search
+// failed.
+__global__ void continuity_finish(Dev d) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= *(volatile int *)&d.ctr[C_NREPAIR]) return;
+  const int t = d.repair_list[i];
+  const int nm = d.tr_modes[t];
+  const size_t o = static_cast<size_t>(d.tr_out[t]);
+  const int s = d.tr_stride[t];
+  unsigned flag = d.cflags[t];
+  if ((d.oflags[t] & TRACE_SEARCH_UNCONVERGED) || d.ocounts[t] < 0) {
+    flag |= CONT_UNRESOLVED;
+  } else {
+    const double *kept = d.cold + static_cast<size_t>(t) * d.nmodes;
+    bool changed = d.ocounts[t] != d.ccount[t];
+    for (int k = 0; k < nm && !changed; ++k) {
+      const double x = d.vel[o + static_cast<size_t>(k) * s], y = kept[k];
+      if (isfinite(x) != isfinite(y)) changed = true;
+      else if (isfinite(x) && fabs(x - y) > d.tol * fabs(x)) changed = true;
+    }
+    if (changed) flag |= CONT_REPAIRED;
+  }
+  d.cflags[t] = static_cast<unsigned char>(flag);
 }
 
 // ---------------------------------------------------------------------------

@@ -114,15 +114,15 @@ class QeSolver:
     accuracy {0 high, 1 balanced, 2 fast, 3 uniform, 4 auto}, period_threshold,
     close_root_rtol, shape, sampling_rtol, secular {0, 1}, refinement {0, 1, 2},
     love_phase, single_precision, group_velocity, group_rtol, continuation,
-    anchor_stride.  Engine tuning keywords (scan_density, log_points,
-    warps_per_block, blocks_per_sm, device) may follow.
+    anchor_stride.  Engine keywords (scan_density, log_points, warps_per_block,
+    blocks_per_sm, continuity_check, device) may follow.
     """
 
     def __init__(self, B, L, nf, nmodes, accuracy=0, period_threshold=0., close_root_rtol=.005,
                  shape=False, sampling_rtol=.001, secular=0, refinement=1, love_phase=1,
                  single_precision=False, group_velocity=False, group_rtol=.001, continuation=False,
                  anchor_stride=4, *, scan_density=0., log_points=0, warps_per_block=0, blocks_per_sm=0,
-                 device=None):
+                 continuity_check=True, device=None):
         if int(B) < 1 or not 1 <= int(L) <= 256 or int(nf) < 1 or not 1 <= int(nmodes) <= 256:
             raise ValueError("invalid QE geometry")
         if int(refinement) not in (0, 1, 2) or int(secular) not in (0, 1):
@@ -147,6 +147,7 @@ class QeSolver:
         o.log_points = int(log_points)
         o.warps_per_block = int(warps_per_block)
         o.blocks_per_sm = int(blocks_per_sm)
+        o.continuity_check = int(bool(continuity_check))
         if device is None:
             device = _current_device
         self.capacity, self.layers, self.nf, self.nmodes = int(B), int(L), int(nf), int(nmodes)
