@@ -97,9 +97,13 @@ def reference_wrapper():
     global _WRAPPER
     if _WRAPPER is None:
         root = HERE / "_ref"
-        if not (root / "modisp" / "__init__.py").is_file():
+        engine = reference()
+        if engine is None or not (root / "modisp" / "__init__.py").is_file():
             return None
         import sys
+        # one loaded copy of the engine serves both the wrapper (its `from . import
+        # _cpu`) and reference(): a pybind11 module cannot be loaded twice
+        sys.modules.setdefault("modisp._cpu", engine)
         if str(root) not in sys.path:
             sys.path.insert(0, str(root))
         import modisp
