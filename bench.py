@@ -531,7 +531,7 @@ def main():
             "flags": [torch.empty((B, T), dtype=torch.int32, device=dev) for _ in range(2)],
             "levels": [torch.empty((B, T), dtype=torch.int32, device=dev) for _ in range(2)],
             "counts": [torch.empty((B, T), dtype=torch.int32, device=dev) for _ in range(2)],
-            "stats": [torch.zeros(16, dtype=torch.int64, device=dev) for _ in range(2)]}
+            "stats": [torch.zeros(_native.STAT_COUNT, dtype=torch.int64, device=dev) for _ in range(2)]}
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # 256 MiB > 126 MB L2
 
     # launch shape of the scan, chosen by the autotuner on a 1,000-model sample

@@ -41,7 +41,11 @@ enum md200_stat {
   MD200_STAT_CONT_ACCEPTED = 13,   /* continuation targets accepted */
   MD200_STAT_CONT_FALLBACK = 14,   /* continuation targets searched globally */
   MD200_STAT_CONTINUITY = 15,      /* FP32-scan traces re-scanned by the continuity recheck */
-  MD200_STAT_COUNT = 16
+  MD200_STAT_FALLBACK = 16,        /* traces re-scanned by the FP64 fallback (first search unfinished) */
+  MD200_STAT_CONT_ANCHORS = 17,    /* continuation anchor traces */
+  MD200_STAT_CONT_EVALUATIONS = 18,/* secular evaluations of continuation targets (prediction + audit) */
+  MD200_STAT_RESERVED = 19,
+  MD200_STAT_COUNT = 20
 };
 
 typedef struct md200_engine md200_engine;
@@ -70,6 +74,9 @@ typedef struct md200_options {
   int continuity_check;    /* FP32 scan: the reference's continuity screen on the results
                               (cpp/cpu/continuity_screen.hpp:8-67) and an FP64 re-scan of
                               its suspects (default 1) */
+  long long scan_points;   /* scan points per trace before TRACE_WORKSPACE_LIMIT in the first
+                              search (<= 0: 2^22); an unfinished trace is re-scanned in FP64
+                              with a limit of 2^26 (TRACE_ADAPTIVE_FALLBACK, level 24) */
 } md200_options;
 
 /* Fill *options with the defaults of a high-accuracy FP64 engine. */

@@ -17,8 +17,9 @@ ABI_VERSION = 2
 STAT_NAMES = ("evaluations", "evaluations_fp32", "layer_steps", "layer_steps_fp32", "brackets",
               "trough_probes", "probe_pairs", "fp64_repair_traces", "unconverged", "group_roots",
               "roots", "traces", "dual_layer_steps", "continuation_accepted",
-              "continuation_fallbacks", "continuity_rescans")
-STAT_COUNT = 16
+              "continuation_fallbacks", "continuity_rescans", "fallback_rescans", "continuation_anchors",
+              "continuation_evaluations", "reserved")
+STAT_COUNT = 20
 
 
 class BackendUnavailableError(RuntimeError):
@@ -45,6 +46,7 @@ class Options(ctypes.Structure):
         ("warps_per_block", ctypes.c_int),
         ("blocks_per_sm", ctypes.c_int),
         ("continuity_check", ctypes.c_int),
+        ("scan_points", ctypes.c_longlong),
     ]
 
 

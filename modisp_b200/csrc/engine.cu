@@ -189,6 +189,7 @@ int setup(md200_engine *e) {
   d.nkmax = d.nlog + 1 + 2 * L;
   d.nsmax = 6 * L + 32;
   d.close_rtol = e->o.close_root_rtol > 0. ? e->o.close_root_rtol : .005;
+  d.jmax = e->o.scan_points > 0 ? std::min<long long>(e->o.scan_points, JMAX_FALLBACK) : JMAX;
   d.fp32 = e->o.single_precision ? 1 : 0;
   d.group = e->o.group_velocity ? 1 : 0;
   const size_t nt = static_cast<size_t>(B) * T;
@@ -395,6 +396,34 @@ int enqueue(md200_engine *e, const double *h, const double *vp, const double *vs
     group_velocity<<<e->list_blocks, 128, 0, s>>>(d);
     ++nl;
     MD200_CK(cudaGetLastError());
+  }
+  {
+    // fallback: traces the first search could not finish, re-scanned in FP64 with
+    // the larger point limit, refined, assembled and given group velocities again
+    // (the lists are empty -- and the launches nearly free -- when there are none)
+    MD200_CK(cudaMemsetAsync(d.ctr + C_REPAIR_CURSOR, 0, 2 * sizeof(int), s));
+    collect_fallback<<<(nt + 255) / 256, 256, 0, s>>>(d);
+    ++nl;
+    Dev df = d;
+    df.jmax = JMAX_FALLBACK;
+    if (wave == 0)
+      scan<double, 0><<<e->scan_blocks64, 32 * e->scan_warps, e->scan_smem64, s>>>(df, d.repair_list,
+                                                                                 C_REPAIR_CURSOR, C_NREPAIR);
+    else
+      scan<double, 1><<<e->scan_blocks64, 32 * e->scan_warps, e->scan_smem64, s>>>(df, d.repair_list,
+                                                                                 C_REPAIR_CURSOR, C_NREPAIR);
+    ++nl;
+    MD200_CK(cudaGetLastError());
+    refine<<<e->list_blocks, 128, 0, s>>>(d);
+    ++nl;
+    assemble<<<(nt + 255) / 256, 256, 0, s>>>(d, d.repair_list, C_NREPAIR);
+    ++nl;
+    MD200_CK(cudaGetLastError());
+    if (d.group) {
+      group_velocity<<<e->list_blocks, 128, 0, s>>>(d);
+      ++nl;
+      MD200_CK(cudaGetLastError());
+    }
   }
   MD200_CK(mark(9));
   if (screen) {
@@ -950,7 +979,8 @@ int md200_kernel_launches(md200_engine *e) {
   if (e->last_launches >= 0) return e->last_launches;  // counted by the last run
   // before any run: the launches of a run without continuity flags requested
   const int check = e->d.fp32 && e->o.continuity_check ? 4 + (e->d.group ? 1 : 0) : 0;
-  return 6 + (e->d.fp32 ? 4 : 0) - (e->d.group ? 0 : 1) + check;
+  const int fallback = 4 + (e->d.group ? 1 : 0);
+  return 6 + (e->d.fp32 ? 4 : 0) - (e->d.group ? 0 : 1) + fallback + check;
 }
 
 void md200_destroy(md200_engine *e) {

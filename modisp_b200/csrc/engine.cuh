@@ -10,7 +10,8 @@ constexpr unsigned FULL = 0xffffffffu;
 constexpr int ROWS = 9;        // per-layer rows of the prepared table (7 used by the recurrence)
 constexpr int EVAL_ROWS = 7;   // rows staged into shared memory for the recurrence
 constexpr int SLOT = 5;        // doubles per bracket slot: lo, hi, flo, fhi, root
-constexpr long long JMAX = 1LL << 22;  // scan points per trace before the workspace flag
+constexpr long long JMAX = 1LL << 22;  // scan points per trace before the workspace flag (default)
+constexpr long long JMAX_FALLBACK = 1LL << 26;  // the fallback re-scan's limit
 
 // Trace flag bits reported to the caller (values of python/modisp/__init__.py:15-32).
 constexpr unsigned TRACE_SEARCH_UNCONVERGED = 4;
@@ -20,6 +21,7 @@ constexpr unsigned TRACE_NONFINITE = 32;
 constexpr unsigned TRACE_REFINEMENT_FAILED = 64;
 constexpr unsigned TRACE_F_REJECTED = 128;
 constexpr unsigned TRACE_CLOSE_ROOT_RISK = 4096;
+constexpr unsigned TRACE_ADAPTIVE_FALLBACK = 8192;
 constexpr unsigned TRACE_FP64_REPAIR = 32768;
 constexpr unsigned TRACE_CONTINUATION_APPROXIMATE = 65536;
 // Engine-internal bits, cleared before the flags are written out.
@@ -35,8 +37,9 @@ constexpr unsigned GROUP_NONFINITE = 32;
 
 // Search levels reported by this engine (the reference's ladder levels do not
 // apply): 20 FP64 scan, 21 FP32 scan with FP64 refinement, 22 FP32 scan repaired
-// by an FP64 re-scan, 23 continuation-predicted; -3 no SH guide, -4 empty window.
-constexpr int LEVEL_FP64 = 20, LEVEL_FP32 = 21, LEVEL_REPAIRED = 22, LEVEL_CONTINUATION = 23;
+// by an FP64 re-scan, 23 continuation-predicted, 24 the FP64 fallback re-scan of
+// a trace the first search could not finish; -3 no SH guide, -4 empty window.
+constexpr int LEVEL_FP64 = 20, LEVEL_FP32 = 21, LEVEL_REPAIRED = 22, LEVEL_CONTINUATION = 23, LEVEL_FALLBACK = 24;
 
 // Device counters (int) used by the work lists.
 enum Counter {
@@ -48,6 +51,7 @@ struct Dev {
   // geometry of this run
   int B, Lmax, Ls, T, nmodes, K, KB, wave, fp32, nlog, nkmax, nsmax;
   int n_traces, group;
+  long long jmax;   // scan points per trace before the workspace flag
   double tol, accept, close_rtol, density;
   // inputs (device)
   const double *h, *vp, *vs, *rho, *periods, *bounds_in;

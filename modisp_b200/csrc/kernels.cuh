@@ -863,8 +863,8 @@ __device__ __forceinline__ ScanState scan_start(const Dev &d, const TraceCtx &x)
   long long J = static_cast<long long>(ceil((u_hi - x.u_lo) * d.density)) - 1;
   st.tfl = 0;
   if (J < 0) J = 0;
-  if (J > JMAX) {
-    J = JMAX;
+  if (J > d.jmax) {
+    J = d.jmax;
     st.tfl |= TRACE_WORKSPACE_LIMIT;
   }
   st.J = J;
@@ -1445,6 +1445,41 @@ __global__ void collect_repairs(Dev d) {
 }
 
 // ---------------------------------------------------------------------------
+// collect_fallback: traces the first search could not finish -- a non-finite
+// value (the FP32 range, say), or the scan-point limit reached before the trace
+// held all its brackets -- re-scanned in FP64 with the larger limit
+// JMAX_FALLBACK (the reference escalates such traces to its adaptive ladder and
+// dense grid, cpp/cpu/solver.cpp:254-370,517-584).  Their earlier roots are
+// taken out of the counters; assemble() reports them at LEVEL_FALLBACK with
+// TRACE_ADAPTIVE_FALLBACK.
+// ---------------------------------------------------------------------------
+__global__ void collect_fallback(Dev d) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t == 0) restart_lists(d);
+  if (t >= d.n_traces) return;
+  const int b = d.tr_model[t];
+  if (d.mstate[b] != 0) return;
+  const unsigned fl = d.tflags[t];
+  const bool capped = (fl & TRACE_WORKSPACE_LIMIT) && d.nbr[t] < d.tr_modes[t] + 2;
+  if (!(fl & TRACE_SEARCH_UNCONVERGED) && !capped) return;
+  const int pos = atomicAdd(&d.ctr[C_NREPAIR], 1);
+  d.repair_list[pos] = t;
+  // (an FP64 re-solve: in an FP32-scan engine also an FP64 repair, which the
+  // continuity recheck does not re-scan)
+  d.tflags[t] = TRACE_ADAPTIVE_FALLBACK | (d.fp32 ? TRACE_FP64_REPAIR : 0u);
+  d.nbr[t] = 0;
+  if (d.stats) {
+    const int nm = d.tr_modes[t], s = d.tr_stride[t];
+    const size_t o = static_cast<size_t>(d.tr_out[t]);
+    int finite = 0;
+    for (int k = 0; k < nm; ++k) finite += isfinite(d.vel[o + static_cast<size_t>(k) * s]);
+    if (finite) atomicAdd(&d.stats[10], static_cast<unsigned long long>(-finite));
+    if (fl & TRACE_SEARCH_UNCONVERGED) atomicAdd(&d.stats[8], static_cast<unsigned long long>(-1LL));
+    atomicAdd(&d.stats[16], 1ULL);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // assemble: one thread per trace.
 // ---------------------------------------------------------------------------
 // With `list`, only the traces list[0 .. ctr[count_id]) (re-solved traces)
@@ -1506,6 +1541,7 @@ __global__ void assemble(Dev d, const int *list = nullptr, int count_id = 0) {
   const double vs_hs = layer_table<double>(d, b)[8 * d.Ls + m.L - 1];
   const double w = TWO_PI / d.tr_period[t];
   int level = d.fp32 ? ((fl & TRACE_FP64_REPAIR) ? LEVEL_REPAIRED : LEVEL_FP32) : LEVEL_FP64;
+  if (fl & TRACE_ADAPTIVE_FALLBACK) level = LEVEL_FALLBACK;
   int count = n;
   if (failed) {
     fl |= TRACE_SEARCH_UNCONVERGED;

@@ -35,7 +35,7 @@ def test_options_struct_matches_header():
     from modisp_b200 import _native
     text = (ROOT / "include" / "modisp_b200.h").read_text()
     body = text[text.index("typedef struct md200_options"):text.index("} md200_options;")]
-    fields = re.findall(r"^\s*(?:int|double)\s+(\w+);", body, flags=re.M)
+    fields = re.findall(r"^\s*(?:int|double|long long)\s+(\w+);", body, flags=re.M)
     assert fields == [f for f, _ in _native.Options._fields_]
     o = _native.default_options()
     assert o.close_root_rtol == .005 and o.refinement == 1 and o.anchor_stride == 4

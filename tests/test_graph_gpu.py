@@ -113,7 +113,7 @@ def test_chunked_host_run_equals_device_run():
         grp = torch.empty_like(vel)
         gfl = torch.empty((B, 3, periods.size), dtype=torch.int32, device=dev)
         fl, lv, ct = (torch.empty((B, periods.size), dtype=torch.int32, device=dev) for _ in range(3))
-        st = torch.zeros(16, dtype=torch.int64, device=dev)
+        st = torch.zeros(_native.STAT_COUNT, dtype=torch.int64, device=dev)
         eng.run_device(x["thickness"].data_ptr(), x["vp"].data_ptr(), x["vs"].data_ptr(), x["rho"].data_ptr(), B,
                        per.data_ptr(), 0, 1e-10, 1., 0, vel.data_ptr(), fl.data_ptr(), lv.data_ptr(), ct.data_ptr(),
                        grp.data_ptr(), gfl.data_ptr(), stats=st.data_ptr(),
