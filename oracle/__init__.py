@@ -277,20 +277,22 @@ def group_windows(roots, lower, upper, close_rtol=0.005):
 
 
 def reference_solve(h, vp, vs, rho, periods, nmodes, wave=0, tol=1e-12, threads=None,
-                    group_velocity=False, group_rtol=1e-3, accuracy=0):
+                    group_velocity=False, group_rtol=1e-3, accuracy=0, bounds=None):
     """Run the reference CPU engine on a [B, L] batch the way its Python wrapper does
     for ``Solver(backend="cpu", accuracy="high", search_strategy="shape_adaptive",
     secular="dunkin", refinement="brent", love_strategy="phase")``
-    (python/modisp/__init__.py:343,414-424)."""
+    (python/modisp/__init__.py:343,414-424).  ``bounds`` [B, 2]: a given search
+    window, run as the wrapper runs one from cmin/cmax (not automatic)."""
     ref = reference()
     if ref is None:
         raise RuntimeError("reference CPU engine not built (make -C oracle ref)")
     h, vp, vs, rho = (np.atleast_2d(np.ascontiguousarray(x, dtype=np.float64)) for x in (h, vp, vs, rho))
     periods = np.ascontiguousarray(periods, dtype=np.float64)
     threads = threads or min(256, len(os.sched_getaffinity(0)))
-    bnd = ref.bounds(h, vp, vs, rho, int(wave), None, None)
+    automatic = bounds is None
+    bnd = ref.bounds(h, vp, vs, rho, int(wave), None, None) if automatic else np.ascontiguousarray(bounds, np.float64)
     solver = ref.CpuSolver(int(threads), int(accuracy), 0., .005, True, .001, 0, 1, 1)
-    out = solver.run(h, vp, vs, rho, periods, bnd, int(nmodes), int(wave), True, float(tol), 1.,
+    out = solver.run(h, vp, vs, rho, periods, bnd, int(nmodes), int(wave), automatic, float(tol), 1.,
                      False, bool(group_velocity), float(group_rtol), True)
     velocity, flags, stats, levels, counts, extras = out
     counts = counts.copy()

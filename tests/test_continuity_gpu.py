@@ -24,7 +24,7 @@ SCREEN_BITS = 8 | 16 | 32 | 64
 
 def synthetic_result(seed, B=64, K=6, T=30, unsorted=False, duplicates=False):
     rng = np.random.default_rng(seed)
-    periods = np.geomspace(0.5, 40., T)
+    periods = np.geomspace(0.5, 10., T)  # two-period log steps of 0.21: every inner period bilateral
     if duplicates:
         periods[rng.choice(T - 1, 4, replace=False)] = periods[rng.choice(T - 1, 4, replace=False)]
     if unsorted:
