@@ -335,10 +335,10 @@ class Solver:
             limit = max(1, int(0.4 * free) // per_model)
         return max(1, min(B, limit, self.chunk_size or B))
 
-    def _engine_for(self, capacity, L, T, nmodes):
+    def _engine_for(self, capacity, L, T, nmodes, continuation=False):
         from . import plugin
         key = (self.device, L, T, int(nmodes), self.accuracy, self.close_root_rtol, self.precision,
-               self.group_velocity, self.frequency_strategy, self.anchor_stride, self.continuity_check,
+               self.group_velocity, bool(continuation), self.anchor_stride, self.continuity_check,
                tuple(sorted(self.tuning.items())))
         if self._engine is not None and self._engine_key[0] == key and self._engine_key[1] >= capacity:
             return self._engine, False
@@ -349,7 +349,7 @@ class Solver:
             self.sampling_rtol, 1 if self.secular == "fast" else 0,
             {"legacy": 0, "brent": 1, "chandrupatla": 2}[self.refinement], int(self.love_strategy == "phase"),
             self.precision != "float64", self.group_velocity, self.group_rtol,
-            self.frequency_strategy == "anchor_continuation", self.anchor_stride,
+            bool(continuation), self.anchor_stride,
             scan_density=float(t["scan_density"]), log_points=int(t["log_points"]),
             warps_per_block=int(t["warps_per_block"]), blocks_per_sm=int(t["blocks_per_sm"]),
             continuity_check=self.continuity_check, device=self.device)
@@ -389,13 +389,29 @@ class Solver:
         backend, reason = self._select()
         input_periods = per
         inverse = None
-        if per.size > 1 and not np.all(per[1:] > per[:-1]) and not np.all(per[1:] < per[:-1]):
+        # frequency strategy (python/modisp/__init__.py:318-340): continuation runs on
+        # sorted unique periods for the approximate presets
+        continuation = False
+        frequency_reason = "independent frequency search requested"
+        if self.frequency_strategy == "anchor_continuation":
+            unique = np.unique(per)
+            if self.accuracy == "high":
+                frequency_reason = "high accuracy retains independent search"
+            elif unique.size < 8:
+                frequency_reason = "fewer than 8 unique periods; using independent search"
+            elif not np.any(np.log(unique[2:]) - np.log(unique[:-2]) <= .25):
+                frequency_reason = ("period grid has no interior target within the anchor log-gap limit; "
+                                    "using independent search")
+            else:
+                continuation = True
+                frequency_reason = "CUDA anchor continuation on sorted unique periods"
+        if continuation or (per.size > 1 and not np.all(per[1:] > per[:-1]) and not np.all(per[1:] < per[:-1])):
             per, inverse = np.unique(per, return_inverse=True)  # python/modisp/__init__.py:314-341
         bounds_in = np.zeros((B, 2))
         bounds_in[:, 0] = self.cmin if self.cmin is not None else 0.
         bounds_in[:, 1] = self.cmax if self.cmax is not None else np.inf
         capacity = self._capacity(B, L, per.size, nmodes)
-        engine, allocated = self._engine_for(capacity, L, per.size, nmodes)
+        engine, allocated = self._engine_for(capacity, L, per.size, nmodes, continuation)
         dtype = np.float32 if self.precision == "float32" else np.float64
         velocity = np.empty((B, nmodes, per.size), dtype=dtype)
         flags = np.empty((B, per.size), np.uint32)
@@ -407,6 +423,9 @@ class Solver:
         # the continuity screen runs in the FP32-scan engine (continuity_check)
         screened = self.precision != "float64" and self.continuity_check
         cflags = np.empty((B, per.size), np.uint8) if screened else None
+        # PredictionFlag words: BYPASSED (8) unless continuation assigns them
+        pflags = (np.full((B, per.size), 8, np.uint32) if self.frequency_strategy == "anchor_continuation"
+                  else None)
         stats = {}
         chunks = 0
         wave_code = int(wave == "love")
@@ -414,7 +433,7 @@ class Solver:
             end = min(B, start + capacity)
             out = engine._engine.run(h[start:end], a[start:end], b[start:end], r[start:end], per,
                                      bounds_in[start:end], self.c_tol_rel, self.f_accept, wave_code,
-                                     group=self.group_velocity, continuity=screened)
+                                     group=self.group_velocity, continuity=screened, prediction=continuation)
             velocity[start:end] = out["velocity"]
             flags[start:end] = out["flags"]
             levels[start:end] = out["levels"]
@@ -425,6 +444,8 @@ class Solver:
                 gflags[start:end] = out["group_velocity_flags"]
             if screened:
                 cflags[start:end] = out["continuity_flags"]
+            if continuation:
+                pflags[start:end] = out["prediction_flags"]
             for k, v in out["stats"].items():
                 stats[k] = stats.get(k, 0) + int(v)
             chunks += 1
@@ -434,6 +455,8 @@ class Solver:
             velocity, flags, levels, counts = (x.take(inverse, axis=-1) for x in (velocity, flags, levels, counts))
             if cflags is not None:
                 cflags = cflags.take(inverse, axis=-1)
+            if pflags is not None:
+                pflags = pflags.take(inverse, axis=-1)
             if group is not None:
                 group, gflags = group.take(inverse, axis=-1), gflags.take(inverse, axis=-1)
         if self.cmin is not None or self.cmax is not None:
@@ -447,7 +470,9 @@ class Solver:
                      close_root_rtol=self.close_root_rtol, refinement_tolerance=self.c_tol_rel, chunks=chunks,
                      capacity_models=int(capacity), engine_allocations=int(allocated),
                      group_velocity=self.group_velocity, group_rtol=self.group_rtol,
-                     frequency_strategy=self.frequency_strategy, frequency_strategy_used="independent",
+                     frequency_strategy=self.frequency_strategy,
+                     frequency_strategy_used="anchor_continuation" if continuation else "independent",
+                     frequency_strategy_reason=frequency_reason,
                      periods_requested=int(input_periods.size), periods_computed=int(per.size),
                      close_root_risk_traces=int(np.count_nonzero(flags & TRACE_CLOSE_ROOT_RISK)),
                      threads=0)
@@ -460,9 +485,11 @@ class Solver:
             accuracy=self.accuracy, close_root_rtol=self.close_root_rtol, search_strategy=self.search_strategy,
             sampling_rtol=self.sampling_rtol, secular=secular, refinement=self.refinement,
             love_strategy=self.love_strategy if wave == "love" else None, group_velocity=group,
-            group_velocity_flags=gflags, prediction_flags=None,
+            group_velocity_flags=gflags, prediction_flags=pflags,
             group_rtol=self.group_rtol if self.group_velocity else None,
-            frequency_strategy=self.frequency_strategy, anchor_stride=self.anchor_stride, continuity_flags=cflags)
+            frequency_strategy=self.frequency_strategy,
+            frequency_strategy_used="anchor_continuation" if continuation else "independent",
+            frequency_strategy_reason=frequency_reason, anchor_stride=self.anchor_stride, continuity_flags=cflags)
         self.last_result = result
         return result
 

@@ -20,6 +20,7 @@
 #include "kernels.cuh"
 #include "adjoint.cuh"
 #include "reliability.cuh"
+#include "continuation.cuh"
 
 using namespace md200;
 
@@ -225,6 +226,12 @@ int setup(md200_engine *e) {
   if (d.fp32 && e->o.continuity_check &&
       (own_alloc(e, &d.cold, nt * nm) || own_alloc(e, &d.ccount, nt)))
     return 1;
+  // anchor continuation: plan, anchor slopes and safety, target and root lists
+  if (e->o.continuation &&
+      (own_alloc(e, &d.crole, nt) || own_alloc(e, &d.cleft, nt) || own_alloc(e, &d.cright, nt) ||
+       own_alloc(e, &d.cslope, nt * d.KB) || own_alloc(e, &d.csafe, nt) || own_alloc(e, &d.cont_list, nt) ||
+       own_alloc(e, &d.croot_list, nt * d.KB) || own_alloc(e, &d.ccode, nt * d.KB)))
+    return 1;
   e->pinned_bytes = sizeof(double) * (4 * static_cast<size_t>(B) * L + T + 2 * static_cast<size_t>(B)) +
                     nt * nm * (2 * sizeof(double) + sizeof(unsigned)) + nt * 4 * sizeof(int) + nt +
                     md200_engine::MAX_CHUNKS * MD200_STAT_COUNT * sizeof(unsigned long long) +
@@ -326,6 +333,7 @@ int enqueue(md200_engine *e, const double *h, const double *vp, const double *vs
   d.stats = stats;
   d.pred = pred;
   const bool screen = d.fp32 && e->o.continuity_check;
+  const bool cont = d.crole != nullptr;  // anchor continuation, each model over its own periods
   d.cflags = screen ? cflags : nullptr;
   if (!d.cflags) d.cold = nullptr, d.ccount = nullptr;
   d.bounds_out = bounds_out;
@@ -343,6 +351,11 @@ int enqueue(md200_engine *e, const double *h, const double *vp, const double *vs
   prep_models<<<(B + pw - 1) / pw, 32 * pw, e->prep_smem, s>>>(d, e->sortcap, 0);
   ++nl;
   MD200_CK(cudaGetLastError());
+  if (cont) {
+    continuation_plan<<<(B + 127) / 128, 128, 0, s>>>(d, std::max(2, e->o.anchor_stride));
+    ++nl;
+    MD200_CK(cudaGetLastError());
+  }
   MD200_CK(mark(1));
   init_traces<<<(nt + 255) / 256, 256, 0, s>>>(d);
   ++nl;
@@ -417,6 +430,38 @@ int enqueue(md200_engine *e, const double *h, const double *vp, const double *vs
     refine<<<e->list_blocks, 128, 0, s>>>(d);
     ++nl;
     assemble<<<(nt + 255) / 256, 256, 0, s>>>(d, d.repair_list, C_NREPAIR);
+    ++nl;
+    MD200_CK(cudaGetLastError());
+    if (d.group) {
+      group_velocity<<<e->list_blocks, 128, 0, s>>>(d);
+      ++nl;
+      MD200_CK(cudaGetLastError());
+    }
+  }
+  if (cont) {
+    // anchor continuation: the anchors are solved; predict, refine and audit the
+    // targets, and send every doubtful one to the FP64 full search
+    const size_t items = static_cast<size_t>(nt) * d.KB;
+    MD200_CK(cudaMemsetAsync(d.ctr + C_REPAIR_CURSOR, 0, 2 * sizeof(int), s));
+    anchor_slopes<<<static_cast<unsigned>((items + 255) / 256), 256, 0, s>>>(d);
+    ++nl;
+    continuation_predict<<<(nt + 255) / 256, 256, 0, s>>>(d);
+    ++nl;
+    continuation_root<<<static_cast<unsigned>((items + 127) / 128), 128, 0, s>>>(d);
+    ++nl;
+    continuation_audit<<<e->list_blocks, 128, 0, s>>>(d);
+    ++nl;
+    MD200_CK(cudaGetLastError());
+    if (wave == 0)
+      scan<double, 0><<<e->scan_blocks64, 32 * e->scan_warps, e->scan_smem64, s>>>(d, d.repair_list,
+                                                                                 C_REPAIR_CURSOR, C_NREPAIR);
+    else
+      scan<double, 1><<<e->scan_blocks64, 32 * e->scan_warps, e->scan_smem64, s>>>(d, d.repair_list,
+                                                                                 C_REPAIR_CURSOR, C_NREPAIR);
+    ++nl;
+    refine<<<e->list_blocks, 128, 0, s>>>(d);
+    ++nl;
+    assemble<<<(nt + 255) / 256, 256, 0, s>>>(d, d.cont_list, C_NTARGET);
     ++nl;
     MD200_CK(cudaGetLastError());
     if (d.group) {

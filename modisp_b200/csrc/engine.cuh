@@ -44,7 +44,7 @@ constexpr int LEVEL_FP64 = 20, LEVEL_FP32 = 21, LEVEL_REPAIRED = 22, LEVEL_CONTI
 // Device counters (int) used by the work lists.
 enum Counter {
   C_SCAN_CURSOR = 0, C_NTRACE, C_NREFINE, C_REFINE_BEGIN, C_NGROUP, C_REPAIR_CURSOR, C_NREPAIR,
-  C_JFAIL, C_GROUP_BEGIN, C_NSUSPECT, C_REFINE_CURSOR, C_COUNT
+  C_JFAIL, C_GROUP_BEGIN, C_NSUSPECT, C_REFINE_CURSOR, C_NTARGET, C_NCROOT, C_COUNT
 };
 
 struct Dev {
@@ -96,6 +96,14 @@ struct Dev {
   unsigned char *cflags;  // [B][T] continuity-screen flags (optional; FP32-scan runs)
   double *cold;        // [n_traces][nmodes] roots of the screen's suspects before their FP64 re-scan
   int *ccount;         // [n_traces] root counts of those suspects before the re-scan
+  // anchor continuation (engines created with it)
+  signed char *crole;   // [n_traces]: 1 anchor, 2 target, 0 searched independently
+  int *cleft, *cright;  // [n_traces]: a target's left and right anchor traces
+  double *cslope;       // [n_traces][KB] dc/dln T at anchor roots
+  unsigned char *csafe; // [n_traces] anchor roots usable as a source
+  int *cont_list;       // target traces
+  int *croot_list;      // predicted roots (trace * KB + rank)
+  unsigned *ccode;      // [n_traces][KB] verdict of each predicted root
   unsigned long long *stats;
 };
 

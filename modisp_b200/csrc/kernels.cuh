@@ -430,12 +430,13 @@ __global__ void prep_models(Dev d, int sortcap, int automatic) {
 }
 
 // ---------------------------------------------------------------------------
-// init_traces: the round-0 trace list (period-major) and per-trace resets.
+// init_traces: the round-0 trace list (period-major) and per-trace resets;
+// with anchor continuation, targets go to their own list.
 // ---------------------------------------------------------------------------
 __global__ void init_traces(Dev d) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= d.n_traces) return;
-  int b, t;
+  int b, t, role = 0;  // role: 1 continuation anchor, 2 continuation target
   if (d.ragged) {
     // CSR order; the owning model by binary search of the offsets
     t = q;
@@ -463,12 +464,20 @@ __global__ void init_traces(Dev d) {
     d.tr_stride[t] = d.T;
     d.tr_modes[t] = d.nmodes;
   }
+  if (d.crole) role = d.crole[t];
   d.nbr[t] = 0;
   d.tflags[t] = 0;
-  if (d.pred) d.pred[t] = 8u;  // searched independently (PredictionFlag.BYPASSED)
+  // PredictionFlag: ANCHOR (1), a target's verdict later, else searched
+  // independently (BYPASSED, 8)
+  if (d.pred) d.pred[t] = role == 1 ? 1u : (role == 2 && d.mstate[b] == 0 ? 0u : 8u);
   if (d.mstate[b] == 0) {
-    const int pos = atomicAdd(&d.ctr[C_NTRACE], 1);
-    d.trace_list[pos] = t;
+    if (role == 2) {
+      const int pos = atomicAdd(&d.ctr[C_NTARGET], 1);
+      d.cont_list[pos] = t;
+    } else {
+      const int pos = atomicAdd(&d.ctr[C_NTRACE], 1);
+      d.trace_list[pos] = t;
+    }
   }
 }
 
@@ -1542,6 +1551,7 @@ __global__ void assemble(Dev d, const int *list = nullptr, int count_id = 0) {
   const double w = TWO_PI / d.tr_period[t];
   int level = d.fp32 ? ((fl & TRACE_FP64_REPAIR) ? LEVEL_REPAIRED : LEVEL_FP32) : LEVEL_FP64;
   if (fl & TRACE_ADAPTIVE_FALLBACK) level = LEVEL_FALLBACK;
+  if (fl & TRACE_CONTINUATION_APPROXIMATE) level = LEVEL_CONTINUATION;
   int count = n;
   if (failed) {
     fl |= TRACE_SEARCH_UNCONVERGED;

@@ -98,14 +98,18 @@ def _csr(periods, B):
 
 
 def dispersion_ragged(thickness, vp, vs, rho, periods, nmodes=5, wave="rayleigh", precision="mixed",
-                      group_velocity=True, c_tol_rel=1e-10, f_accept=1., device=0, chunk_models=65536):
+                      group_velocity=True, c_tol_rel=1e-10, f_accept=1., device=0, chunk_models=65536,
+                      frequency_strategy="independent", anchor_stride=4):
     """Solve a ragged batch.
 
     ``periods``: a list of per-model period arrays, or a CSR pair (offsets [B+1],
     flat periods).  ``nmodes``: one count for all models or one per model.
     ``precision``: "mixed" (FP32 scan, FP64 refinement) or "float64".  Models are
     padded [B, L] arrays as in ``dispersion_batch``; chunks of ``chunk_models``
-    models share one engine.
+    models share one engine.  ``frequency_strategy="anchor_continuation"`` solves
+    every ``anchor_stride``-th period of a model (its periods ascending, at least
+    8) by the full search and predicts, refines and audits the periods between
+    them, falling back to the full FP64 search on any doubt.
     """
     if wave not in WAVES:
         raise ValueError("wave must be 'rayleigh' or 'love'")
@@ -113,6 +117,10 @@ def dispersion_ragged(thickness, vp, vs, rho, periods, nmodes=5, wave="rayleigh"
         raise ValueError("precision must be 'mixed' or 'float64'")
     if not (0. < c_tol_rel < 1.):
         raise ValueError("c_tol_rel must lie in (0, 1)")
+    if frequency_strategy not in ("independent", "anchor_continuation"):
+        raise ValueError("frequency_strategy must be independent or anchor_continuation")
+    if not isinstance(anchor_stride, (int, np.integer)) or anchor_stride < 2:
+        raise ValueError("anchor_stride must be an integer of at least 2")
     h, a, b, r = _models(thickness, vp, vs, rho)
     B, L = h.shape
     offsets, flat = _csr(periods, B)
@@ -136,6 +144,8 @@ def dispersion_ragged(thickness, vp, vs, rho, periods, nmodes=5, wave="rayleigh"
     o = _native.default_options()
     o.single_precision = 1 if precision == "mixed" else 0
     o.group_velocity = int(bool(group_velocity))
+    o.continuation = int(frequency_strategy == "anchor_continuation")
+    o.anchor_stride = int(anchor_stride)
     cap = int(min(B, chunk_models))
     engine = _native.Engine(device, cap, L, T_max, nm_max, o)
     try:
