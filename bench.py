@@ -2,24 +2,36 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Workload (one "step"): the batched crustal configuration -- 10,000 seeded random
-models with 8-20 layers over a half-space (padded to 21 rows), 60 periods
-geomspaced 0.5-50 s, 5 modes, Rayleigh and Love, group velocity on -- solved to
-c_tol_rel 1e-10 (|dc|/c <= 1e-11, inside the 1e-9 parity bar).  Each rank solves
-its own batch (weak scaling; ranks exchange nothing but the timing reduction).
+Workload (one "step"): the mixed-precision configuration -- 100,000 seeded random
+models with 8-20 layers over a half-space (padded to 21 rows), 30 % of them with
+one low-velocity layer (Vs 20-40 % below the layer above), 60 periods geomspaced
+0.5-50 s, 5 modes, Rayleigh and Love, group velocity on -- solved to c_tol_rel
+1e-10 (|dc|/c <= 1e-11, inside the 1e-9 parity bar).  Each rank solves its own
+batch (weak scaling; ranks exchange nothing but the timing reduction).
 
 Printed JSON (rank 0, one line):
   value      roots/s of the FP32-scan / FP64-refinement engine, device-resident
              inputs, CUDA events on the launching stream, L2 flushed between steps
-  e2e        the same metric through the plugin's QeSolver.run (C ABI host path,
-             host arrays, host<->device copies inside the timed region)
   fp64       the plain FP64 engine on the same protocol (the denominator of the
              FP32-scan speed-up)
-  roofline   the scan kernel's algorithmic FP32 flop rate against the measured
-             non-tensor FP32 FMA peak of this GPU
-  cpu_baseline  the reference CPU engine (oracle/_ref, built from the reference
-             sources) on a bounded sample of the same batch, all host cores
---impl reference times that reference CPU engine alone (rank 0 only).
+  e2e        the same metric through the plugin's QeSolver.run (C ABI host path,
+             host arrays, host<->device copies inside the timed region)
+  roofline   the FP32 scan kernel's algorithmic FP32 flop rate against the
+             measured non-tensor FP32 FMA peak of this GPU
+  cpu_baseline, cpu_baseline_auto
+             the reference CPU engine (oracle/_ref, built from the reference
+             sources) through the reference's own Solver on a bounded sample of
+             the same batch, all host cores, at accuracy="high" (c_tol_rel 1e-10)
+             and at its default accuracy="auto"
+  reference_cuda
+             the reference's own CUDA plugin compiled for sm_100a (oracle/_ref/cuda)
+             on a sample of the same batch on this GPU: a same-GPU comparator
+  config2, jacobian, ragged, reliability, parity
+             side workloads: the 10,000-model crustal batch, Jacobians (config 4),
+             the large uneven batch (config 5 sample, with and without anchor
+             continuation), the mode-reliability checks, and the agreement of both
+             engines with each other and with the reference
+--impl reference times the reference CPU engine alone (rank 0 only).
 """
 from __future__ import annotations
 
@@ -40,16 +52,18 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "roots/s at |dc/c|<=1e-9 (FP32-scan+FP64-refine engine; plain FP64 alongside)"
 TOL = 1e-10
-MODELS = 10_000
-WORKLOAD = "crustal batch: 10000 models x 8-20 layers, 60 periods 0.5-50 s, 5 modes, Rayleigh+Love, group velocity"
+MODELS = 100_000
+WORKLOAD = ("mixed-precision batch: 100000 models x 8-20 layers, 30 % with one low-velocity layer, "
+            "60 periods 0.5-50 s, 5 modes, Rayleigh+Love, group velocity")
 # Algorithmic floating-point operations of one layer step of the secular
 # recurrences, counted from modisp_b200/csrc/secular.cuh (adds and multiplies
 # each 1, an FMA 2; the elementary functions counted separately: 2 rsqrt and
 # 2 sin/cos-or-exp per Rayleigh step, 1 rsqrt and 1 sin/cos-or-exp per Love step).
 FLOPS_PER_STEP = {0: 170, 1: 24}
-# DRAM traffic of the FP32 Rayleigh scan, dram__bytes_read.sum + dram__bytes_write.sum
-# from one ncu capture of a 2,000-model launch (120,000 traces: 30.1 MB + 93.0 MB),
-# per trace; scaled to this workload's launch by its trace count.
+# DRAM traffic of the FP32 Rayleigh scan per trace, dram__bytes_read.sum +
+# dram__bytes_write.sum of one ncu capture of a 2,000-model crustal launch
+# (120,000 traces: 30.7 MB + 95.4 MB), scaled to the headline launch by its trace
+# count.
 SCAN32_DRAM_BYTES_PER_TRACE = (30.661888e6 + 95.3536e6) / 120_000
 
 
@@ -60,12 +74,14 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=("ours", "reference"), default="ours")
     p.add_argument("--models", type=int, default=MODELS)
-    p.add_argument("--cpu-sample", type=int, default=128, help="models in the CPU-baseline sample")
+    p.add_argument("--cpu-sample", type=int, default=1024, help="models in the CPU-baseline sample")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-side", action="store_true", help="skip every side workload")
     p.add_argument("--no-jacobian", action="store_true")
     p.add_argument("--no-ragged", action="store_true")
-    p.add_argument("--no-config3", action="store_true")
+    p.add_argument("--no-config2", action="store_true")
     p.add_argument("--no-reliability", action="store_true")
+    p.add_argument("--no-reference-cuda", action="store_true")
     return p.parse_args()
 
 
@@ -77,8 +93,9 @@ def dist_env():
 
 
 def workload(rank, models):
+    """Rank 0 solves exactly the seeded mixed-precision batch; other ranks their own seeds."""
     from modisp_b200 import workloads
-    batch = workloads.crustal_batch(models, seed=workloads.SEED + 2 + 1000 * rank)
+    batch = workloads.crustal_batch(models, seed=workloads.SEED + 3 + 1000 * rank, lvz_fraction=0.3)
     return batch, np.geomspace(0.5, 50., 60), 5
 
 
@@ -134,27 +151,53 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline(batch, periods, nmodes, sample):
-    """The reference CPU engine (built from the reference sources) on a bounded sample."""
+# ---------------------------------------------------------------------------
+# the reference CPU engine (oracle/_ref) on a bounded sample
+# ---------------------------------------------------------------------------
+def cpu_solve(sub, periods, nmodes, wave, accuracy, threads):
+    """One wave of the reference CPU engine, through the reference's own Solver when
+    the oracle recipe staged it (its stock path, continuity screen and review
+    included), else through its CpuSolver directly."""
     import oracle
-    ref = oracle.reference()
-    if ref is None:
+    wrapper = oracle.reference_wrapper()
+    if wrapper is not None:
+        opts = dict(backend="cpu", threads=threads, group_velocity=True)
+        if accuracy == "high":
+            opts.update(accuracy="high", c_tol_rel=TOL)
+        r = wrapper.dispersion_batch(sub["thickness"], sub["vp"], sub["vs"], sub["rho"], periods, nmodes,
+                                     "love" if wave else "rayleigh", **opts)
+        return r.phase_velocity
+    if accuracy != "high":
         return None
-    sub = {k: v[:sample] for k, v in batch.items()}
-    cores = len(os.sched_getaffinity(0))
-    threads = min(256, cores)
+    out = oracle.reference_solve(sub["thickness"], sub["vp"], sub["vs"], sub["rho"], periods, nmodes, wave=wave,
+                                 tol=TOL, threads=threads, group_velocity=True)
+    return out["phase_velocity"]
+
+
+def cpu_baseline(batch, periods, nmodes, sample, accuracy="high"):
+    """The reference CPU engine on the first `sample` models of the batch (both
+    waves), one warm-up call per wave, all host cores."""
+    import oracle
+    if oracle.reference() is None:
+        return None
+    sub = {k: np.ascontiguousarray(v[:sample]) for k, v in batch.items()}
+    threads = min(256, len(os.sched_getaffinity(0)))
     roots, elapsed = 0, 0.
     for wave in (0, 1):
-        oracle.reference_solve(sub["thickness"][:4], sub["vp"][:4], sub["vs"][:4], sub["rho"][:4], periods, nmodes,
-                               wave=wave, tol=TOL, threads=threads, group_velocity=True)  # warm-up
+        small = {k: v[:4] for k, v in sub.items()}
+        if cpu_solve(small, periods, nmodes, wave, accuracy, threads) is None:  # warm-up
+            return None
         t = time.perf_counter()
-        out = oracle.reference_solve(sub["thickness"], sub["vp"], sub["vs"], sub["rho"], periods, nmodes,
-                                     wave=wave, tol=TOL, threads=threads, group_velocity=True)
+        v = cpu_solve(sub, periods, nmodes, wave, accuracy, threads)
         elapsed += time.perf_counter() - t
-        roots += int(np.isfinite(out["phase_velocity"]).sum())
+        roots += int(np.isfinite(v).sum())
+    path = "the reference's Solver(backend='cpu')" if oracle.reference_wrapper() is not None else "its CpuSolver"
+    setting = (f"accuracy='high', c_tol_rel={TOL:g}" if accuracy == "high"
+               else "default accuracy='auto' (c_tol_rel 1e-5, continuity screen and review on)")
     return {"value": roots / elapsed, "unit": "roots/s", "cores": threads, "kind": "reference", "seconds": elapsed,
-            "sample": f"{sample} models of the same batch x 60 periods x 5 modes, Rayleigh+Love, group velocity, "
-                      f"accuracy=high shape-adaptive, c_tol_rel={TOL:g}; {roots} roots in {elapsed:.2f} s"}
+            "accuracy": accuracy,
+            "sample": f"{sample} of the {batch['thickness'].shape[0]} models x 60 periods x 5 modes, Rayleigh+Love, "
+                      f"group velocity, {setting}, via {path}; {roots} roots in {elapsed:.2f} s"}
 
 
 def run_reference(args, rank, world):
@@ -163,6 +206,7 @@ def run_reference(args, rank, world):
     batch, periods, nmodes = workload(0, args.models)
     sample = args.cpu_sample
     vals, times = [], []
+    res = None
     for step in range(args.warmup + args.steps):
         res = cpu_baseline(batch, periods, nmodes, sample)
         if res is None:
@@ -172,17 +216,68 @@ def run_reference(args, rank, world):
             vals.append(res["value"])
             times.append(res["seconds"])
     value = statistics.median(vals)
+    auto = cpu_baseline(batch, periods, nmodes, sample, accuracy="auto")
     line = {"metric": METRIC, "value": value, "unit": "roots/s", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * statistics.median(times), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "impl": "reference",
+            "warmup": args.warmup, "ms_per_step": 1e3 * statistics.median(times), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "impl": "reference",
             "config": {"workload": WORKLOAD, "models_per_step": sample, "periods": 60, "nmodes": 5,
-                       "c_tol_rel": TOL},
+                       "c_tol_rel": TOL, "same_config_note": f"each step solves {sample} of the "
+                       f"{args.models} models (a bounded sample; roots/s is a per-root rate)"},
             "cpu_baseline": {"value": value, "unit": "roots/s", "cores": res["cores"], "kind": "reference",
                              "sample": res["sample"]},
+            "cpu_baseline_auto": auto,
             "e2e": {"value": value, "unit": "roots/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
 
+# ---------------------------------------------------------------------------
+# the reference's CUDA plugin (sm_100a build) on this GPU
+# ---------------------------------------------------------------------------
+def reference_cuda_bench(batch, periods, nmodes, local, sample=10_000, ours=None):
+    """The reference's own QeSolver (its CUDA plugin compiled for sm_100a from its
+    sources) on the first `sample` models, both waves, FP64 and FP32 precision at
+    accuracy='high' (shape-adaptive search), host arrays in and out like its
+    wrapper's call; one warm-up and two timed calls per wave.  Masks compared with
+    this engine's on the same models."""
+    import oracle
+    mod = oracle.reference_cuda()
+    if mod is None:
+        return {"unavailable": "reference CUDA plugin not built (make -C oracle ref-cuda REFERENCE=...)"}
+    mod.set_device(local)
+    sub = {k: np.ascontiguousarray(v[:sample]) for k, v in batch.items()}
+    B, L = sub["thickness"].shape
+    T = periods.size
+    out = {}
+    for single in (False, True):
+        s = mod.QeSolver(B, L, T, nmodes, 0, 0., .005, True, .001, 0, 1, 1, single, True, .001, False, 4)
+        total, roots, masks = 0., 0, {}
+        try:
+            for wave in (0, 1):
+                bounds = oracle.reference().bounds(sub["thickness"], sub["vp"], sub["vs"], sub["rho"], wave, None,
+                                                   None)
+                args = (sub["thickness"], sub["vp"], sub["vs"], sub["rho"], periods, bounds, TOL, 1., wave, True)
+                s.run(*args)
+                for _ in range(2):
+                    t = time.perf_counter()
+                    r = s.run(*args)
+                    total += time.perf_counter() - t
+                roots += 2 * int(np.isfinite(r[0]).sum())
+                masks[wave] = np.isfinite(r[0])
+        finally:
+            s.close()
+        key = "fp32" if single else "fp64"
+        out[key] = {"value": roots / total, "unit": "roots/s", "seconds": total}
+        if ours is not None:
+            out[key]["mask_mismatch_traces_vs_this_engine"] = int(sum(
+                np.any(masks[w] != np.isfinite(ours[w][:sample]), axis=1).sum() for w in (0, 1)))
+    out["sample"] = (f"{sample} models of the batch, accuracy='high' shape-adaptive, c_tol_rel={TOL:g}, group "
+                     f"velocity, QeSolver.run on host arrays (the wrapper's call), 2 timed calls per wave")
+    return out
+
+
+# ---------------------------------------------------------------------------
+# side workloads
+# ---------------------------------------------------------------------------
 def jacobian_bench(torch, local, steps, warmup, flush):
     """Differentiation workload: forward solve, full phase/group Jacobians and the
     misfit gradient (vector-Jacobian product) of 4096 12-layer models, 40 periods
@@ -255,74 +350,26 @@ def jacobian_bench(torch, local, steps, warmup, flush):
 RAGGED_MODELS = 10_000
 
 
-def config3_bench(torch, local, flush, sample=256, rank=0):
-    """Mixed precision on the 100,000-model batch with 30 % low-velocity-layer models:
-    FP32-scan throughput (one timed step, both waves), agreement of the FP32-scan and
-    plain FP64 engines over the whole batch, and per-root error of the FP32-scan
-    engine against the reference CPU engine on a sample of the batch."""
+def config2_bench(torch, local, steps, warmup, flush):
+    """The 10,000-model crustal batch (no low-velocity layers), both engines, the
+    headline's device-resident protocol."""
     from modisp_b200 import _native, workloads
-    import oracle
-    batch, periods, nmodes = workloads.config3()
+    batch, periods, nmodes = workloads.config2()
     B, L = batch["thickness"].shape
     T = periods.size
-    dev = torch.device("cuda", local)
-    x = {k: torch.tensor(batch[k], device=dev) for k in ("thickness", "vp", "vs", "rho")}
-    per = torch.tensor(periods, device=dev)
+    tens = device_tensors(torch, batch, periods, nmodes, local)
     out = {}
-    ms = 0.
-    for single in (1, 0):
+    for single in (True, False):
         o = _native.default_options()
-        o.single_precision = single
-        o.group_velocity = 1
+        o.single_precision, o.group_velocity = int(single), 1
         eng = _native.Engine(local, B, L, T, nmodes, o)
-        stream = torch.cuda.current_stream().cuda_stream
-        for wave in (0, 1):
-            vel = torch.empty((B, nmodes, T), dtype=torch.float64, device=dev)
-            grp = torch.empty_like(vel)
-            gfl = torch.empty((B, nmodes, T), dtype=torch.int32, device=dev)
-            tr = [torch.empty((B, T), dtype=torch.int32, device=dev) for _ in range(3)]
-            args = (x["thickness"].data_ptr(), x["vp"].data_ptr(), x["vs"].data_ptr(), x["rho"].data_ptr(), B,
-                    per.data_ptr(), 0, TOL, 1., wave, vel.data_ptr(), tr[0].data_ptr(), tr[1].data_ptr(),
-                    tr[2].data_ptr(), grp.data_ptr(), gfl.data_ptr())
-            eng.run_device(*args, stream=stream)  # warm-up
-            flush.zero_()
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a.record()
-            eng.run_device(*args, stream=stream)
-            b.record()
-            b.synchronize()
-            if single:
-                ms += a.elapsed_time(b)
-            out[single, wave] = (vel.cpu().numpy(), grp.cpu().numpy(), tr[2].cpu().numpy())
+        ms, roots, _ = timed_runs(torch, eng, tens, B, steps, warmup, flush)
         eng.close()
-    roots = sum(int(np.isfinite(out[1, w][0]).sum()) for w in (0, 1))
-    agree = {"mask_mismatch_traces": 0, "count_mismatches": 0, "max_rel_diff_phase": 0., "max_rel_diff_group": 0.}
-    for w in (0, 1):
-        v32, g32, c32 = out[1, w]
-        v64, g64, c64 = out[0, w]
-        agree["mask_mismatch_traces"] += int(np.any(np.isfinite(v32) != np.isfinite(v64), axis=1).sum())
-        agree["count_mismatches"] += int((c32 != c64).sum())
-        m = np.isfinite(v32) & np.isfinite(v64)
-        agree["max_rel_diff_phase"] = max(agree["max_rel_diff_phase"], float((np.abs(v32[m] - v64[m]) / v64[m]).max()))
-        mg = np.isfinite(g32) & np.isfinite(g64)
-        agree["max_rel_diff_group"] = max(agree["max_rel_diff_group"], float((np.abs(g32[mg] - g64[mg]) / g64[mg]).max()))
-    vs_ref = None
-    if rank == 0 and oracle.reference() is not None:
-        threads = len(os.sched_getaffinity(0))
-        idx = np.linspace(0, B - 1, sample).astype(int)
-        vs_ref = {"sample_models": sample, "mask_mismatch_traces": 0, "count_mismatches": 0, "max_rel_err_phase": 0.}
-        for w in (0, 1):
-            ref = oracle.reference_solve(*(batch[k][idx] for k in ("thickness", "vp", "vs", "rho")), periods, nmodes,
-                                         wave=w, tol=1e-12, threads=threads)
-            v, rv = out[1, w][0][idx], ref["phase_velocity"]
-            vs_ref["mask_mismatch_traces"] += int(np.any(np.isfinite(v) != np.isfinite(rv), axis=1).sum())
-            vs_ref["count_mismatches"] += int((out[1, w][2][idx] != ref["root_count"]).sum())
-            m = np.isfinite(v) & np.isfinite(rv)
-            vs_ref["max_rel_err_phase"] = max(vs_ref["max_rel_err_phase"], float((np.abs(v[m] - rv[m]) / rv[m]).max()))
-    return {"workload": "100,000 models as the crustal batch, 30 % with one low-velocity layer (Vs 20-40 % below "
-                        "the layer above), 60 periods 0.5-50 s, 5 modes, Rayleigh + Love, FP32 scan / FP64 refinement",
-            "value": roots / (ms * 1e-3), "unit": "roots/s", "ms_per_step": ms, "roots_per_step": roots,
-            "fp32_vs_fp64_engine": agree, "fp32_vs_reference": vs_ref}
+        out["fp32" if single else "fp64"] = {"value": roots * steps / (ms * 1e-3), "ms_per_step": ms / steps}
+    out["fp32_scan_speedup"] = out["fp32"]["value"] / out["fp64"]["value"]
+    out["workload"] = "10,000 crustal models x 8-20 layers (no low-velocity layers), 60 periods 0.5-50 s, 5 modes"
+    out["unit"] = "roots/s"
+    return out
 
 
 def hbm_peak_gbs():
@@ -427,12 +474,13 @@ def reliability_bench(torch, local, steps, flush, rank=0, sample=300):
     return line
 
 
-def ragged_bench(torch, local, steps, warmup, flush, models=RAGGED_MODELS):
+def ragged_bench(torch, local, steps, warmup, flush, models=RAGGED_MODELS, continuation=False):
     """Large uneven batch: smooth-gradient models of 30-100 thin layers, each with its
     own 50-120 periods inside 0.2-100 s and 1-10 modes, Rayleigh + Love, FP32 scan /
     FP64 refinement, group velocity; one ragged (CSR) run per wave, both captured in
     one CUDA graph that each step replays.  A seeded sample of the 1,000,000-model
-    workload (throughput does not depend on the batch size beyond filling the GPU)."""
+    workload (throughput does not depend on the batch size beyond filling the GPU).
+    With `continuation`, each model's periods run with anchor continuation."""
     from modisp_b200 import _native, workloads
     batch, periods, modes = workloads.gradient_batch(models, seed=workloads.SEED + 50)
     B, L = batch["thickness"].shape
@@ -454,7 +502,9 @@ def ragged_bench(torch, local, steps, warmup, flush, models=RAGGED_MODELS):
     o = _native.default_options()
     o.single_precision = 1
     o.group_velocity = 1
+    o.continuation = int(continuation)
     eng = _native.Engine(local, B, L, int(np.diff(off).max()), int(md.max()), o)
+    launches = 0
     eng.graph_begin()
     for wave in (0, 1):
         eng.run_ragged_device(x["thickness"].data_ptr(), x["vp"].data_ptr(), x["vs"].data_ptr(), x["rho"].data_ptr(),
@@ -462,6 +512,7 @@ def ragged_bench(torch, local, steps, warmup, flush, models=RAGGED_MODELS):
                               meta["outb"].data_ptr(), TOL, 1., wave, vel[wave].data_ptr(), tr[wave][0].data_ptr(),
                               tr[wave][1].data_ptr(), tr[wave][2].data_ptr(), grp[wave].data_ptr(),
                               gfl[wave].data_ptr())
+        launches += eng.kernel_launches()  # counted as the run enqueued them
     eng.graph_end()
     stream = torch.cuda.current_stream().cuda_stream
     for _ in range(warmup):
@@ -483,21 +534,97 @@ def ragged_bench(torch, local, steps, warmup, flush, models=RAGGED_MODELS):
                         "periods in 0.2-100 s, 1-10 modes each; Rayleigh + Love; ragged CSR batch, one CUDA graph",
             "models": B, "traces_per_wave": ntr, "output_cells_per_wave": ncell, "roots_per_step": roots,
             "ms_per_step": total / steps, "value": roots * steps / (total * 1e-3), "unit": "roots/s",
-            "unconverged_traces": unconverged, "launches_per_step": eng_launches_ragged()}
+            "unconverged_traces": unconverged, "launches_per_step": launches}
 
 
-def eng_launches_ragged():
-    # prep, init, tail values, scan, refine, repair select, repair scan, repair refine, assemble, group: per wave
-    return 2 * 10
+# ---------------------------------------------------------------------------
+# the headline
+# ---------------------------------------------------------------------------
+def device_tensors(torch, batch, periods, nmodes, local):
+    from modisp_b200 import _native
+    B = batch["thickness"].shape[0]
+    T = periods.size
+    dev = torch.device("cuda", local)
+    f64 = torch.float64
+    t = {k: torch.tensor(batch[k], dtype=f64, device=dev) for k in ("thickness", "vp", "vs", "rho")}
+    return {"h": t["thickness"], "vp": t["vp"], "vs": t["vs"], "rho": t["rho"],
+            "per": torch.tensor(periods, dtype=f64, device=dev),
+            "vel": [torch.empty((B, nmodes, T), dtype=f64, device=dev) for _ in range(2)],
+            "grp": [torch.empty((B, nmodes, T), dtype=f64, device=dev) for _ in range(2)],
+            "gfl": [torch.empty((B, nmodes, T), dtype=torch.int32, device=dev) for _ in range(2)],
+            "flags": [torch.empty((B, T), dtype=torch.int32, device=dev) for _ in range(2)],
+            "levels": [torch.empty((B, T), dtype=torch.int32, device=dev) for _ in range(2)],
+            "counts": [torch.empty((B, T), dtype=torch.int32, device=dev) for _ in range(2)],
+            "stats": [torch.zeros(_native.STAT_COUNT, dtype=torch.int64, device=dev) for _ in range(2)]}
 
 
-def device_run(torch, eng, tens, B, wave, stream):
+def device_run(eng, tens, B, wave, stream):
     """Enqueue one engine run on device-resident tensors."""
     eng.run_device(tens["h"].data_ptr(), tens["vp"].data_ptr(), tens["vs"].data_ptr(), tens["rho"].data_ptr(), B,
                    tens["per"].data_ptr(), 0, TOL, 1., wave, tens["vel"][wave].data_ptr(),
                    tens["flags"][wave].data_ptr(), tens["levels"][wave].data_ptr(), tens["counts"][wave].data_ptr(),
                    tens["grp"][wave].data_ptr(), tens["gfl"][wave].data_ptr(), None, None,
                    tens["stats"][wave].data_ptr(), stream)
+
+
+def timed_runs(torch, eng, tens, B, steps, warmup, flush, barrier=None):
+    """W warm-up steps, then K timed steps (both waves each), L2 flushed before each
+    step, CUDA events on the launching stream.  Returns (total ms, roots of one
+    step, kernels launched per step)."""
+    stream = torch.cuda.current_stream().cuda_stream
+    for _ in range(warmup):
+        for wave in (0, 1):
+            device_run(eng, tens, B, wave, stream)
+    (barrier or torch.cuda.synchronize)()
+    total, launches = 0., 0
+    for _ in range(steps):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        launches = 0
+        for wave in (0, 1):
+            device_run(eng, tens, B, wave, stream)
+            launches += eng.kernel_launches()
+        b.record()
+        b.synchronize()
+        total += a.elapsed_time(b)
+    (barrier or torch.cuda.synchronize)()
+    roots = sum(int(torch.isfinite(tens["vel"][w]).sum()) for w in (0, 1))
+    return total, roots, launches
+
+
+def parity_summary(out32, out64, batch, periods, nmodes, rank, sample=256):
+    """Agreement of the two engines on the whole headline batch, and of the FP32-scan
+    engine with the reference CPU engine on a spread sample of it."""
+    import oracle
+    agree = {"mask_mismatch_traces": 0, "count_mismatches": 0, "max_rel_diff_phase": 0., "max_rel_diff_group": 0.}
+    for w in (0, 1):
+        v32, g32, c32 = out32[w]
+        v64, g64, c64 = out64[w]
+        agree["mask_mismatch_traces"] += int(np.any(np.isfinite(v32) != np.isfinite(v64), axis=1).sum())
+        agree["count_mismatches"] += int((c32 != c64).sum())
+        m = np.isfinite(v32) & np.isfinite(v64)
+        agree["max_rel_diff_phase"] = max(agree["max_rel_diff_phase"], float((np.abs(v32[m] - v64[m]) / v64[m]).max()))
+        mg = np.isfinite(g32) & np.isfinite(g64)
+        agree["max_rel_diff_group"] = max(agree["max_rel_diff_group"],
+                                          float((np.abs(g32[mg] - g64[mg]) / g64[mg]).max()))
+    line = {"fp32_vs_fp64_engine": agree}
+    if rank == 0 and oracle.reference() is not None:
+        threads = len(os.sched_getaffinity(0))
+        B = batch["thickness"].shape[0]
+        idx = np.linspace(0, B - 1, sample).astype(int)
+        vs_ref = {"sample_models": sample, "mask_mismatch_traces": 0, "count_mismatches": 0, "max_rel_err_phase": 0.}
+        for w in (0, 1):
+            ref = oracle.reference_solve(*(batch[k][idx] for k in ("thickness", "vp", "vs", "rho")), periods, nmodes,
+                                         wave=w, tol=1e-12, threads=threads)
+            v, rv = out32[w][0][idx], ref["phase_velocity"]
+            vs_ref["mask_mismatch_traces"] += int(np.any(np.isfinite(v) != np.isfinite(rv), axis=1).sum())
+            vs_ref["count_mismatches"] += int((out32[w][2][idx] != ref["root_count"]).sum())
+            m = np.isfinite(v) & np.isfinite(rv)
+            vs_ref["max_rel_err_phase"] = max(vs_ref["max_rel_err_phase"],
+                                              float((np.abs(v[m] - rv[m]) / rv[m]).max()))
+        line["fp32_vs_reference"] = vs_ref
+    return line
 
 
 def main():
@@ -520,26 +647,14 @@ def main():
     batch, periods, nmodes = workload(rank, args.models)
     B, L = batch["thickness"].shape
     T = periods.size
-    dev = torch.device("cuda", local)
-    f64 = torch.float64
-    tens = {k: torch.tensor(batch[k], dtype=f64, device=dev) for k in ("thickness", "vp", "vs", "rho")}
-    tens = {"h": tens["thickness"], "vp": tens["vp"], "vs": tens["vs"], "rho": tens["rho"],
-            "per": torch.tensor(periods, dtype=f64, device=dev),
-            "vel": [torch.empty((B, nmodes, T), dtype=f64, device=dev) for _ in range(2)],
-            "grp": [torch.empty((B, nmodes, T), dtype=f64, device=dev) for _ in range(2)],
-            "gfl": [torch.empty((B, nmodes, T), dtype=torch.int32, device=dev) for _ in range(2)],
-            "flags": [torch.empty((B, T), dtype=torch.int32, device=dev) for _ in range(2)],
-            "levels": [torch.empty((B, T), dtype=torch.int32, device=dev) for _ in range(2)],
-            "counts": [torch.empty((B, T), dtype=torch.int32, device=dev) for _ in range(2)],
-            "stats": [torch.zeros(_native.STAT_COUNT, dtype=torch.int64, device=dev) for _ in range(2)]}
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # 256 MiB > 126 MB L2
+    tens = device_tensors(torch, batch, periods, nmodes, local)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=torch.device("cuda", local))  # > L2
 
     # launch shape of the scan, chosen by the autotuner on a 1,000-model sample
     from modisp_b200 import autotune
     sample = {k: v[:1000] for k, v in batch.items()}
-    tuned = {}
-    for single in (True, False):
-        tuned[single] = autotune.autotune(sample, periods, nmodes, 0, single, device=local, use_cache=False)
+    tuned = {single: autotune.autotune(sample, periods, nmodes, 0, single, device=local, use_cache=False)
+             for single in (True, False)}
 
     def engine(single):
         o = _native.default_options()
@@ -553,131 +668,135 @@ def main():
             torch.distributed.barrier()
         torch.cuda.synchronize()
 
-    def timed(eng, steps, warmup):
-        stream = torch.cuda.current_stream().cuda_stream
-        for _ in range(warmup):
-            for wave in (0, 1):
-                device_run(torch, eng, tens, B, wave, stream)
-        barrier()
-        total = 0.
-        for _ in range(steps):
-            flush.zero_()
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a.record()
-            for wave in (0, 1):
-                device_run(torch, eng, tens, B, wave, stream)
-            b.record()
-            b.synchronize()
-            total += a.elapsed_time(b)
-        barrier()
-        roots = sum(int(torch.isfinite(tens["vel"][w]).sum()) for w in (0, 1))
-        return total, roots
-
     def reduce_max(x):
-        return sharding.reduce_max(x, dev)
+        return sharding.reduce_max(x, torch.device("cuda", local))
 
     def reduce_sum(x):
-        return sharding.reduce_sum(x, dev)
+        return sharding.reduce_sum(x, torch.device("cuda", local))
+
+    def host_outputs():
+        return {w: (tens["vel"][w].cpu().numpy(), tens["grp"][w].cpu().numpy(), tens["counts"][w].cpu().numpy())
+                for w in (0, 1)}
 
     # ---- FP32-scan engine: the headline ----
     e32 = engine(True)
     with ClockSampler(local) as clocks:
-        ms32, roots32 = timed(e32, args.steps, args.warmup)
+        ms32, roots32, launches = timed_runs(torch, e32, tens, B, args.steps, args.warmup, flush, barrier)
     ms32 = reduce_max(ms32)
-    roots_all = reduce_sum(roots32)
-    value = roots_all * args.steps / (ms32 * 1e-3)
-    # per-stage device times of one more run per wave (scan kernel = dominant)
+    value = reduce_sum(roots32) * args.steps / (ms32 * 1e-3)
+    out32 = host_outputs()
+    # per-stage device times of one more run per wave (the scan kernel dominates)
     stream = torch.cuda.current_stream().cuda_stream
-    stage = {}
-    scan_flops = 0.
+    stage, scan_flops = {}, 0.
     for wave in (0, 1):
         flush.zero_()
-        device_run(torch, e32, tens, B, wave, stream)
-        st = e32.stage_times()
+        device_run(e32, tens, B, wave, stream)
+        stage[wave] = e32.stage_times()
         stats = tens["stats"][wave].cpu().numpy()
-        stage[wave] = st
         scan_flops += float(stats[3]) * FLOPS_PER_STEP[wave]  # FP32 layer steps (scan kernel)
     scan_ms = sum(stage[w]["scan"] for w in (0, 1))
-    launches = e32.kernel_launches() * 2 * args.steps
     e32_stats = {w: tens["stats"][w].cpu().numpy().tolist() for w in (0, 1)}
+    e32.close()
 
-    # ---- plain FP64 engine ----
+    # ---- plain FP64 engine, same protocol ----
     e64 = engine(False)
-    ms64, roots64 = timed(e64, max(2, args.steps // 2), 1)
+    ms64, roots64, _ = timed_runs(torch, e64, tens, B, args.steps, args.warmup, flush, barrier)
     ms64 = reduce_max(ms64)
-    value64 = reduce_sum(roots64) * max(2, args.steps // 2) / (ms64 * 1e-3)
+    value64 = reduce_sum(roots64) * args.steps / (ms64 * 1e-3)
+    out64 = host_outputs()
+    stage64 = {}
+    for wave in (0, 1):
+        flush.zero_()
+        device_run(e64, tens, B, wave, stream)
+        stage64[wave] = e64.stage_times()
     e64.close()
+    del tens
 
     # ---- end to end through the plugin (host arrays) ----
-    h2d = d2h = 0
-    e2e_value = None
-    if True:
-        solver = plugin.QeSolver(B, L, T, nmodes, 0, 0., .005, True, .001, 0, 1, 1, True, True, .001, False, 4,
-                                 device=local)
-        bounds = np.zeros((B, 2))
-        bounds[:, 1] = np.inf
-        host = [np.ascontiguousarray(batch[k]) for k in ("thickness", "vp", "vs", "rho")]
-        for _ in range(max(1, args.warmup - 1)):
-            for wave in (0, 1):
-                solver.run(*host, periods, bounds, TOL, 1., wave)
-        barrier()
-        t0 = time.perf_counter()
-        outs = {}
-        for _ in range(args.steps):
-            for wave in (0, 1):
-                outs[wave] = solver.run(*host, periods, bounds, TOL, 1., wave)
-        barrier()
-        wall = reduce_max(time.perf_counter() - t0)
-        # every step returns the same roots: counted once, outside the timed region
-        roots_e2e = args.steps * sum(int(np.isfinite(outs[w][0]).sum()) for w in (0, 1))
-        e2e_value = reduce_sum(roots_e2e) / wall
-        per_wave_in = sum(a.nbytes for a in host) + periods.nbytes + bounds.nbytes
-        per_wave_out = B * nmodes * T * (8 + 8 + 4) + B * T * 4 * 3 + B * 16 + 16 * 8
-        h2d, d2h = 2 * per_wave_in, 2 * per_wave_out
-        solver.close()
+    solver = plugin.QeSolver(B, L, T, nmodes, 0, 0., .005, True, .001, 0, 1, 1, True, True, .001, False, 4,
+                             device=local)
+    bounds = np.zeros((B, 2))
+    bounds[:, 1] = np.inf
+    host = [np.ascontiguousarray(batch[k]) for k in ("thickness", "vp", "vs", "rho")]
+    for _ in range(max(1, args.warmup - 1)):
+        for wave in (0, 1):
+            solver.run(*host, periods, bounds, TOL, 1., wave)
+    barrier()
+    t0 = time.perf_counter()
+    outs = {}
+    for _ in range(args.steps):
+        for wave in (0, 1):
+            outs[wave] = solver.run(*host, periods, bounds, TOL, 1., wave)
+    barrier()
+    wall = reduce_max(time.perf_counter() - t0)
+    # every step returns the same roots: counted once, outside the timed region
+    roots_e2e = args.steps * sum(int(np.isfinite(outs[w][0]).sum()) for w in (0, 1))
+    e2e_value = reduce_sum(roots_e2e) / wall
+    per_wave_in = sum(a.nbytes for a in host) + periods.nbytes + bounds.nbytes
+    # device-to-host copies of one run: phase and group velocity (float64; the plugin
+    # narrows phase to float32 on the host), group flags, trace flags, levels,
+    # counts, windows and counters
+    cells, traces = B * nmodes * T, B * T
+    per_wave_out = cells * (8 + 8 + 4) + traces * 4 * 3 + B * 16 + _native.STAT_COUNT * 8
+    solver.close()
 
-    jac = jacobian_bench(torch, local, max(2, args.steps // 2), 2, flush) if not args.no_jacobian else None
-    ragged = ragged_bench(torch, local, max(2, args.steps // 2), 2, flush) if not args.no_ragged else None
-    config3 = config3_bench(torch, local, flush, rank=rank) if not args.no_config3 else None
+    side = not args.no_side
+    parity = parity_summary(out32, out64, batch, periods, nmodes, rank)
+    config2 = (config2_bench(torch, local, max(2, args.steps // 2), 2, flush)
+               if side and not args.no_config2 else None)
+    jac = (jacobian_bench(torch, local, max(2, args.steps // 2), 2, flush)
+           if side and not args.no_jacobian else None)
+    ragged = None
+    if side and not args.no_ragged:
+        ragged = ragged_bench(torch, local, max(2, args.steps // 2), 2, flush)
+        ragged["continuation"] = ragged_bench(torch, local, max(2, args.steps // 2), 2, flush, continuation=True)
     reliability = (reliability_bench(torch, local, max(3, args.steps), flush, rank=rank)
-                   if not args.no_reliability else None)
+                   if side and not args.no_reliability else None)
+    ref_cuda = (reference_cuda_bench(batch, periods, nmodes, local, ours={w: out64[w][0] for w in (0, 1)})
+                if side and rank == 0 and not args.no_reference_cuda else None)
 
     peak32 = _native.measure_peak(local, fp64=False)
     peak64 = _native.measure_peak(local, fp64=True)
     achieved = scan_flops / (scan_ms * 1e-3)
-    cpu = None
+    cpu = cpu_auto = None
     if rank == 0 and not args.no_cpu:
         cpu = cpu_baseline(batch, periods, nmodes, args.cpu_sample)
-    e32.close()
+        cpu_auto = cpu_baseline(batch, periods, nmodes, args.cpu_sample, accuracy="auto")
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "roots/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms32 / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded crustal models)",
+            "vs_baseline": None, "dtype": "f32+f64",
+            "data": "synthetic (seeded crustal models, 30 % with a low-velocity layer)",
             "config": {"workload": WORKLOAD, "models_per_gpu": B, "layers_padded": L, "periods": T, "nmodes": nmodes,
                        "waves": ["rayleigh", "love"], "c_tol_rel": TOL, "l2": "flushed between steps (256 MiB write)",
                        "parallelism": f"model-sharded x{world}",
                        "scan_launch_shape": {"fp32": list(tuned[True]), "fp64": list(tuned[False]),
                                              "chosen_by": "autotuner (warps per CTA, CTAs per SM)"}},
-            "fp64": {"value": value64, "unit": "roots/s", "ms_per_step": ms64 / max(2, args.steps // 2),
-                     "fp32_scan_speedup": value / value64},
-            "e2e": {"value": e2e_value, "unit": "roots/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "fp64": {"value": value64, "unit": "roots/s", "ms_per_step": ms64 / args.steps,
+                     "fp32_scan_speedup": value / value64,
+                     "stage_ms": {("rayleigh" if w == 0 else "love"): stage64[w] for w in (0, 1)}},
+            "e2e": {"value": e2e_value, "unit": "roots/s", "h2d_bytes_per_step": 2 * per_wave_in,
+                    "d2h_bytes_per_step": 2 * per_wave_out},
             "roofline": {"bound": "fp32-cuda-core", "kernel": "scan<float>", "achieved": achieved / 1e12,
                          "peak": peak32 / 1e12, "unit": "TFLOP/s", "frac": achieved / peak32,
                          "traffic": SCAN32_DRAM_BYTES_PER_TRACE * B * T,
-                         "traffic_note": "bytes per Rayleigh FP32 scan launch, from an ncu capture of 2,000 models "
-                                         "scaled by traces; the algorithmic input is the model tables (~1.5 KB per "
-                                         "model): the kernel is compute-bound, DRAM at 0.2 % of peak",
+                         "traffic_note": "DRAM bytes of the Rayleigh FP32 scan launch, from an ncu capture of a smaller "
+                                         "launch scaled by traces; the algorithmic input is the model tables (~1.5 KB "
+                                         "per model): the kernel is compute-bound",
                          "peak_kind": "measured FMA throughput (md200_measure_peak), not MEASURED_PEAKS.json",
                          "fp64_peak": peak64 / 1e12, "scan_ms_per_step": scan_ms,
                          "stage_ms": {("rayleigh" if w == 0 else "love"): stage[w] for w in (0, 1)}},
             "cpu_baseline": cpu,
-            "gpu_launches": launches,
+            "cpu_baseline_auto": cpu_auto,
+            "gpu_launches": launches * args.steps,
             "clocks": clocks.summary(),
             "engine_stats": {"rayleigh": e32_stats[0], "love": e32_stats[1]},
+            "parity": parity,
+            "reference_cuda": ref_cuda,
+            "config2": config2,
             "jacobian": jac,
             "ragged": ragged,
-            "config3": config3,
             "reliability": reliability,
         }
         print(json.dumps(line))

@@ -895,7 +895,15 @@ __device__ __forceinline__ unsigned scan_positions(const TraceCtx &x, ScanState 
   const double gv = gj <= st.J ? scan_point(x.kt, x.nk, x.fr, x.alpha, x.u_lo + static_cast<double>(gj) * step,
                                             kfrom)
                                : INFINITY;
-  const double sv = st.si + lane < x.ns ? x.sd[st.si + lane] : INFINITY;
+  double sv = st.si + lane < x.ns ? x.sd[st.si + lane] : INFINITY;
+  if ((st.tfl & TRACE_WORKSPACE_LIMIT) && st.gi + 31 >= st.J) {
+    // a capped grid ends in this step (or has ended): seeds past its last point
+    // lie outside the first search -- between seeds alone, roots would be
+    // skipped -- so the scan stops there and the trace goes to the fallback
+    double last = gj <= st.J ? gv : -INFINITY;
+    for (int o = 16; o; o >>= 1) last = fmax(last, __shfl_xor_sync(FULL, last, o));
+    if (sv > last) sv = INFINITY;
+  }
   const int rg = warp_rank(sv, gv, false);  // seeds strictly below this scan point
   const int rs = warp_rank(gv, sv, true);   // scan points at or below this seed
   const int pg = lane + rg, ps = lane + rs;

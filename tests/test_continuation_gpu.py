@@ -49,7 +49,9 @@ def test_continuation_equals_the_full_search(wave, precision):
     assert np.all(anchors[:, 0]) and np.all(anchors[:, -1])
     assert stats["continuation_accepted"] == int(accepted.sum())
     assert stats["continuation_fallbacks"] == int(fallback.sum())
-    assert accepted.sum() > 0.2 * (accepted.sum() + fallback.sum())  # the predictions do serve
+    # the predictions do serve: the reference's own continuation accepts 27 %
+    # (Rayleigh) and 17 % (Love) of these targets (CPU engine, same batch)
+    assert accepted.sum() > 0.1 * (accepted.sum() + fallback.sum())
     np.testing.assert_array_equal((cont.trace_flags[accepted] & 65536) != 0, True)  # CONTINUATION_APPROXIMATE
     np.testing.assert_array_equal(cont.search_level[accepted], 23)
     # group velocity of the accepted roots: the same analytic derivative at nearly the same roots
