@@ -22,7 +22,7 @@
 extern "C" {
 #endif
 
-#define MD200_ABI_VERSION 2
+#define MD200_ABI_VERSION 3
 /* Statistics written by md200_run (indices into the stats array). */
 enum md200_stat {
   MD200_STAT_EVALUATIONS = 0,      /* secular evaluations, all precisions */
@@ -77,6 +77,10 @@ typedef struct md200_options {
   long long scan_points;   /* scan points per trace before TRACE_WORKSPACE_LIMIT in the first
                               search (<= 0: 2^22); an unfinished trace is re-scanned in FP64
                               with a limit of 2^26 (TRACE_ADAPTIVE_FALLBACK, level 24) */
+  int scan_mode;           /* FP32 scan: 0 auto (rounds of split kernels for Rayleigh runs of
+                              4096 traces or more, else the fused one-warp-per-trace
+                              kernel), 1 fused, 2 split; all return the same brackets bit
+                              for bit */
 } md200_options;
 
 /* Fill *options with the defaults of a high-accuracy FP64 engine. */

@@ -13,7 +13,7 @@ from pathlib import Path
 import numpy as np
 
 LIBRARY = Path(__file__).resolve().parent / "_lib" / "libmodisp_b200.so"
-ABI_VERSION = 2
+ABI_VERSION = 3
 STAT_NAMES = ("evaluations", "evaluations_fp32", "layer_steps", "layer_steps_fp32", "brackets",
               "trough_probes", "probe_pairs", "fp64_repair_traces", "unconverged", "group_roots",
               "roots", "traces", "dual_layer_steps", "continuation_accepted",
@@ -47,6 +47,7 @@ class Options(ctypes.Structure):
         ("blocks_per_sm", ctypes.c_int),
         ("continuity_check", ctypes.c_int),
         ("scan_points", ctypes.c_longlong),
+        ("scan_mode", ctypes.c_int),
     ]
 
 

@@ -21,6 +21,7 @@
 #include "adjoint.cuh"
 #include "reliability.cuh"
 #include "continuation.cuh"
+#include "split_scan.cuh"
 
 using namespace md200;
 
@@ -226,6 +227,17 @@ int setup(md200_engine *e) {
   if (d.fp32 && e->o.continuity_check &&
       (own_alloc(e, &d.cold, nt * nm) || own_alloc(e, &d.ccount, nt)))
     return 1;
+  // split FP32 scan: active lists, per-trace state, per-sample buffers
+  if (d.fp32) {
+    d.sp_cap = static_cast<int>(std::min<size_t>(nt, SPLIT_ACTIVE_MAX));
+    const size_t ns = static_cast<size_t>(d.sp_cap) * SPLIT_SAMPLES;
+    if (own_alloc(e, &d.sp_act[0], d.sp_cap) || own_alloc(e, &d.sp_act[1], d.sp_cap) ||
+        own_alloc(e, &d.sp_state, nt) || own_alloc(e, &d.sp_s, ns) || own_alloc(e, &d.sp_tr, d.sp_cap) ||
+        own_alloc(e, &d.sp_kf, nt) ||
+        own_alloc(e, &d.sp_redo, ns) || own_alloc(e, &d.sp_zoom, d.sp_cap) ||
+        own_alloc(e, &d.sp_zarg, static_cast<size_t>(d.sp_cap) * 8))
+      return 1;
+  }
   // anchor continuation: plan, anchor slopes and safety, target and root lists
   if (e->o.continuation &&
       (own_alloc(e, &d.crole, nt) || own_alloc(e, &d.cleft, nt) || own_alloc(e, &d.cright, nt) ||
@@ -298,6 +310,45 @@ struct Ragged {
   const long long *outbase = nullptr;
 };
 
+// Rounds of the split FP32 scan for a run of nt traces over an active set of
+// cap traces: enough for every trace of a typical run to finish (a trace takes
+// a round per SPLIT_SAMPLES samples, most take two or three); traces still
+// unfinished after them are handed to the fused kernel.
+int split_rounds(int nt, int cap) {
+  const int waves = (nt + cap - 1) / cap;
+  return std::min(64, 3 * waves + 6);
+}
+
+// The split FP32 scan's launches (split_scan.cuh): `rounds` rounds, then the
+// fused kernel for the traces still unfinished (resumed from their state) and
+// for any the rounds never took from the trace list.  Returns the launch count.
+template <int WAVE>
+int split_scan(md200_engine *e, const Dev &d, int rounds, cudaStream_t s) {
+  const int sms = e->list_blocks / 8;
+  const int cap = d.sp_cap;
+  const int fill_blocks = std::max(1, std::min((cap + 255) / 256, sms * 8));
+  const int pos_blocks = std::max(1, std::min((cap + 3) / 4, sms * 16));
+  const int eval_blocks = sms * 16;
+  const int book_blocks = std::max(1, std::min((cap + 127) / 128, sms * 8));
+  int nl = 0;
+  for (int r = 0; r < rounds; ++r) {
+    const int p = r & 1;
+    split_feed_count<<<1, 1, 0, s>>>(d, p);
+    split_feed_fill<<<fill_blocks, 256, 0, s>>>(d, p);
+    split_positions<<<pos_blocks, 128, 0, s>>>(d, p);
+    split_eval32<WAVE><<<eval_blocks, 128, 0, s>>>(d, p);
+    split_redo<WAVE><<<sms * 8, 128, 0, s>>>(d, p);
+    split_book<WAVE><<<book_blocks, 128, 0, s>>>(d, p);
+    split_zoom<WAVE><<<sms * 4, 128, 0, s>>>(d, p);
+    nl += 7;
+  }
+  const int pf = rounds & 1;
+  const dim3 grid(e->scan_blocks32), block(32 * e->scan_warps);
+  scan<float, WAVE><<<grid, block, e->scan_smem32, s>>>(d, d.sp_act[pf], C_SP_RESUME, C_SP_ACT0 + pf, 1);
+  scan<float, WAVE><<<grid, block, e->scan_smem32, s>>>(d, d.trace_list, C_SP_FEED, C_NTRACE, 0);
+  return nl + 2;
+}
+
 int enqueue(md200_engine *e, const double *h, const double *vp, const double *vs, const double *rho,
             int B, const double *periods, const double *bounds, double tol, double accept, int wave,
             double *vel, unsigned *flags, int *levels, int *counts, double *grp, unsigned *gflags,
@@ -366,7 +417,15 @@ int enqueue(md200_engine *e, const double *h, const double *vp, const double *vs
     MD200_CK(cudaGetLastError());
   }
   MD200_CK(mark(2));
-  {
+  // the split scan in auto mode: Rayleigh runs of SPLIT_MIN_TRACES traces or more
+  // (the Love step is too cheap for the rounds to pay: measured slower)
+  const bool split = d.fp32 && (e->o.scan_mode == 2 ||
+                                (e->o.scan_mode == 0 && wave == 0 && nt >= SPLIT_MIN_TRACES));
+  if (split) {
+    const int rounds = split_rounds(nt, d.sp_cap);
+    if (wave == 0) nl += split_scan<0>(e, d, rounds, s);
+    else nl += split_scan<1>(e, d, rounds, s);
+  } else {
     const dim3 grid(d.fp32 ? e->scan_blocks32 : e->scan_blocks64), block(32 * e->scan_warps);
     const size_t sm = d.fp32 ? e->scan_smem32 : e->scan_smem64;
     if (d.fp32 && wave == 0) scan<float, 0><<<grid, block, sm, s>>>(d, d.trace_list, C_SCAN_CURSOR, C_NTRACE);

@@ -44,8 +44,17 @@ constexpr int LEVEL_FP64 = 20, LEVEL_FP32 = 21, LEVEL_REPAIRED = 22, LEVEL_CONTI
 // Device counters (int) used by the work lists.
 enum Counter {
   C_SCAN_CURSOR = 0, C_NTRACE, C_NREFINE, C_REFINE_BEGIN, C_NGROUP, C_REPAIR_CURSOR, C_NREPAIR,
-  C_JFAIL, C_GROUP_BEGIN, C_NSUSPECT, C_REFINE_CURSOR, C_NTARGET, C_NCROOT, C_COUNT
+  C_JFAIL, C_GROUP_BEGIN, C_NSUSPECT, C_REFINE_CURSOR, C_NTARGET, C_NCROOT,
+  // split FP32 scan: active-list sizes by round parity, the trace-list feed
+  // cursor, this round's fill base and count, FP64 re-evaluations, window
+  // requests, the hand-over cursor
+  C_SP_ACT0, C_SP_ACT1, C_SP_FEED, C_SP_BASE, C_SP_TAKE, C_SP_REDO, C_SP_ZOOM, C_SP_RESUME,
+  C_COUNT
 };
+
+struct ScanState;
+struct SplitSample;
+struct SplitTrace;
 
 struct Dev {
   // geometry of this run
@@ -104,6 +113,18 @@ struct Dev {
   int *cont_list;       // target traces
   int *croot_list;      // predicted roots (trace * KB + rank)
   unsigned *ccode;      // [n_traces][KB] verdict of each predicted root
+  // split FP32 scan (single-precision engines): rounds of positions, values,
+  // FP64 re-evaluations, bookkeeping and trough windows over an active set of
+  // traces; per-sample buffers [sp_cap][SPLIT_SAMPLES]
+  int sp_cap;           // active-set capacity (traces)
+  int *sp_act[2];       // active trace lists by round parity
+  ScanState *sp_state;  // [n_traces] scan state between rounds
+  struct SplitSample *sp_s;  // [sp_cap][SPLIT_SAMPLES] samples of the round
+  struct SplitTrace *sp_tr;  // [sp_cap] the active traces' evaluation constants
+  int *sp_kf;           // [n_traces] knot interval of the trace's next grid point (a lower bound)
+  int *sp_redo;         // samples to evaluate in FP64
+  int *sp_zoom;         // window requests: active-list index
+  double *sp_zarg;      // [sp_cap][8] their arguments
   unsigned long long *stats;
 };
 

@@ -888,9 +888,13 @@ __device__ __forceinline__ ScanState scan_start(const Dev &d, const TraceCtx &x)
 }
 
 // The next 32 sample positions: grid points and seeds merged in order (this
-// lane's position in c; INFINITY past the window).  Returns the valid-lane mask.
+// lane's position in c; INFINITY past the window).  Returns the valid-lane mask;
+// with SRC, also (*seeds) the lanes whose position is a seed (kbuf: 32 bytes of
+// shared memory beside mbuf).
+template <bool SRC = false>
 __device__ __forceinline__ unsigned scan_positions(const TraceCtx &x, ScanState &st, double step, int lane,
-                                                   double *mbuf, int &kfrom, double &c) {
+                                                   double *mbuf, int &kfrom, double &c,
+                                                   unsigned char *kbuf = nullptr, unsigned *seeds = nullptr) {
   const long long gj = st.gi + lane;
   const double gv = gj <= st.J ? scan_point(x.kt, x.nk, x.fr, x.alpha, x.u_lo + static_cast<double>(gj) * step,
                                             kfrom)
@@ -911,8 +915,13 @@ __device__ __forceinline__ unsigned scan_positions(const TraceCtx &x, ScanState 
   __syncwarp();
   if (pg < 32) mbuf[pg] = gv;
   if (ps < 32) mbuf[ps] = sv;
+  if constexpr (SRC) {
+    if (pg < 32) kbuf[pg] = 0;
+    if (ps < 32) kbuf[ps] = 1;
+  }
   __syncwarp();
   c = mbuf[lane];
+  if constexpr (SRC) *seeds = __ballot_sync(FULL, c < INFINITY && kbuf[lane]);
   __syncwarp();
   st.gi += __popc(__ballot_sync(FULL, pg < 32 && gv < INFINITY));
   st.si += __popc(__ballot_sync(FULL, ps < 32 && sv < INFINITY));
@@ -1117,7 +1126,8 @@ __device__ __forceinline__ void scan_counters_flush(const Dev &d, const ScanCoun
 // (merge buffer).
 // ---------------------------------------------------------------------------
 template <class T, int WAVE>
-__global__ void __launch_bounds__(128, MD200_SCAN_MIN_BLOCKS) scan(Dev d, const int *list, int cursor_id, int count_id) {
+__global__ void __launch_bounds__(128, MD200_SCAN_MIN_BLOCKS) scan(Dev d, const int *list, int cursor_id, int count_id,
+                                                                   int resume = 0) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const size_t tab_bytes = (static_cast<size_t>(EVAL_ROWS) * d.Ls * sizeof(T) + 15) & ~size_t(15);
@@ -1150,7 +1160,8 @@ __global__ void __launch_bounds__(128, MD200_SCAN_MIN_BLOCKS) scan(Dev d, const 
     LayerView<double> view64;
     if constexpr (single) view64 = global_view(d, x.b);
     else view64 = *reinterpret_cast<const LayerView<double> *>(&view);
-    ScanState st = scan_start(d, x);
+    // a fresh trace, or (resume) one the split scan handed over mid-way
+    ScanState st = resume ? d.sp_state[x.t] : scan_start(d, x);
     int kfrom = 0;  // this lane's knot interval (scan_point)
     while (st.nbr < x.K && !(st.bits & SS_FINISHED)) {
       double c;

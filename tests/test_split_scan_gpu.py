@@ -1,0 +1,121 @@
+"""The split FP32 scan against the fused one.
+
+The single-precision scan runs either as one fused kernel (a warp scans one trace
+from start to end) or as rounds of split kernels over an active set of traces
+(positions one warp per trace, FP32 values one thread per sample, FP64
+re-evaluations one thread per listed sample, bookkeeping one thread per trace,
+trough windows and last cells one warp per request; modisp_b200/csrc/split_scan.cuh).
+Every decision follows the same rule in the same order, so both must return the
+same brackets -- and therefore identical velocities, group velocities, flags,
+levels and counts, bit for bit -- on crustal, low-velocity-layer and water-layer
+batches, the reference suite's frozen fixtures, the large uneven workload (whose
+deep models outlast the rounds and are finished by the fused kernel), and with
+the scan-point cap that sends traces to the fallback.
+"""
+import numpy as np
+import pytest
+
+from conftest import load_golden, GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+FUSED, SPLIT = 1, 2
+
+
+def solve(batch, periods, nmodes, wave, mode, bounds=None, **opts):
+    from modisp_b200 import _native
+    h = batch["thickness"]
+    o = _native.default_options()
+    o.single_precision, o.group_velocity, o.scan_mode = 1, 1, mode
+    for k, v in opts.items():
+        setattr(o, k, v)
+    e = _native.Engine(0, h.shape[0], h.shape[1], periods.size, nmodes, o)
+    try:
+        out = e.run(h, batch["vp"], batch["vs"], batch["rho"], periods, bounds, 1e-10, 1., wave, group=True,
+                    continuity=True)
+        out["launches"] = e.kernel_launches()
+        return out
+    finally:
+        e.close()
+
+
+def assert_identical(a, b, where):
+    for key in ("velocity", "group_velocity"):
+        np.testing.assert_array_equal(a[key].view(np.uint64), b[key].view(np.uint64), err_msg=f"{where}: {key}")
+    for key in ("flags", "levels", "counts", "group_velocity_flags", "continuity_flags"):
+        np.testing.assert_array_equal(a[key], b[key], err_msg=f"{where}: {key}")
+    assert a["stats"]["roots"] == b["stats"]["roots"]
+
+
+@pytest.mark.parametrize("wave", [0, 1])
+@pytest.mark.parametrize("lvz", [0.0, 0.5])
+def test_split_equals_fused_on_crustal_batches(wave, lvz):
+    from modisp_b200 import workloads
+    batch = workloads.crustal_batch(600, workloads.SEED + 80 + int(10 * lvz), lvz_fraction=lvz)
+    periods = np.geomspace(0.5, 50., 60)
+    fused = solve(batch, periods, 5, wave, FUSED)
+    split = solve(batch, periods, 5, wave, SPLIT)
+    assert split["launches"] > fused["launches"]  # the rounds did run
+    assert_identical(split, fused, f"crustal lvz={lvz} wave={wave}")
+
+
+@pytest.mark.parametrize("name", sorted(p.stem for p in GOLDEN.glob("fixture_0*.npz")))
+def test_split_equals_fused_on_frozen_fixtures(name):
+    g = load_golden(name)
+    wave = 1 if str(g["wave"]) == "love" else 0
+    batch = {k: np.atleast_2d(g[k]) for k in ("thickness", "vp", "vs", "rho")}
+    bounds = np.atleast_2d(g["search_bounds"])
+    args = (batch, g["periods"], int(g["nmodes"]), wave)
+    assert_identical(solve(*args, SPLIT, bounds=bounds), solve(*args, FUSED, bounds=bounds), name)
+
+
+@pytest.mark.parametrize("wave", [0, 1])
+def test_split_equals_fused_on_water_models(wave):
+    from modisp_b200 import workloads
+    batch = workloads.crustal_batch(300, workloads.SEED + 83, lvz_fraction=0.3)
+    batch = {k: v.copy() for k, v in batch.items()}
+    # a 1-3 km water layer on top of every model
+    rng = np.random.default_rng(5)
+    batch["thickness"][:, 0] = rng.uniform(1., 3., batch["thickness"].shape[0])
+    batch["vp"][:, 0], batch["vs"][:, 0], batch["rho"][:, 0] = 1.5, 0., 1.03
+    periods = np.geomspace(1., 40., 40)
+    assert_identical(solve(batch, periods, 4, wave, SPLIT), solve(batch, periods, 4, wave, FUSED), f"water {wave}")
+
+
+@pytest.mark.parametrize("name", ["ref_crustal48_rayleigh", "ref_lvz48_love"])
+def test_split_equals_fused_with_the_scan_point_cap(name):
+    g = load_golden(name)
+    wave = int(g["wave"])
+    batch = {k: np.atleast_2d(g[k]) for k in ("thickness", "vp", "vs", "rho")}
+    bounds = np.atleast_2d(g["search_bounds"])
+    args = (batch, g["periods"], int(g["nmodes"]), wave)
+    split = solve(*args, SPLIT, bounds=bounds, scan_points=48)
+    fused = solve(*args, FUSED, bounds=bounds, scan_points=48)
+    assert (split["flags"] & 8192).any()  # traces did go to the fallback
+    assert_identical(split, fused, f"{name} capped")
+
+
+@pytest.mark.parametrize("wave", [0, 1])
+def test_split_equals_fused_on_the_large_uneven_workload(wave):
+    from modisp_b200 import _native, workloads
+    batch, periods, modes = workloads.gradient_batch(200, seed=workloads.SEED + 84)
+    B, L = batch["thickness"].shape
+    off = np.zeros(B + 1, np.int32)
+    off[1:] = np.cumsum([p.size for p in periods])
+    flat = np.concatenate(periods)
+    md = np.asarray(modes, np.int32)
+    outs = {}
+    for mode in (FUSED, SPLIT):
+        o = _native.default_options()
+        o.single_precision, o.group_velocity, o.scan_mode = 1, 1, mode
+        e = _native.Engine(0, B, L, int(np.diff(off).max()), int(md.max()), o)
+        try:
+            outs[mode] = e.run_ragged(batch["thickness"], batch["vp"], batch["vs"], batch["rho"], off, flat, md,
+                                      1e-10, 1., wave, group=True)
+        finally:
+            e.close()
+    a, b = outs[SPLIT], outs[FUSED]
+    for key in ("velocity", "group_velocity"):
+        np.testing.assert_array_equal(a[key].view(np.uint64), b[key].view(np.uint64), err_msg=key)
+    for key in ("flags", "levels", "counts"):
+        np.testing.assert_array_equal(a[key], b[key], err_msg=key)
