@@ -811,12 +811,10 @@ __device__ __noinline__ int last_cell(const LayerView<T> view, const LayerView<d
 // ---------------------------------------------------------------------------
 // The scan of one trace as a sequence of 32-sample steps: positions, values,
 // bookkeeping.  One warp runs a trace from start to end (persistent kernel
-// `scan`, the model table in shared memory).  Splitting the steps into rounds
-// of a one-thread-per-sample evaluation kernel and a one-warp-per-trace
-// bookkeeping kernel, with the state in global memory between them, gave the
-// same brackets bit for bit but was slower (45 vs 39 ms for the Rayleigh
-// FP32 scan of 10,000 crustal models): the bookkeeping costs more on its own
-// than interleaved with the evaluations of other warps.
+// `scan`, the model table in shared memory).  The same steps also run as rounds
+// of separate kernels over an active set of traces (split_scan.cuh), with the
+// state below carried in global memory between rounds; the fused kernel then
+// finishes, in resume mode, the traces the rounds left unfinished.
 // ---------------------------------------------------------------------------
 
 // Per-trace scan state carried between steps.

@@ -35,7 +35,7 @@
 namespace md200 {
 
 #ifndef MD200_SPLIT_STEPS
-#define MD200_SPLIT_STEPS 4
+#define MD200_SPLIT_STEPS 2
 #endif
 #ifndef MD200_SPLIT_EVAL_BLOCKS
 #define MD200_SPLIT_EVAL_BLOCKS 1
@@ -44,7 +44,7 @@ constexpr int SPLIT_STEPS = MD200_SPLIT_STEPS;    // 32-sample steps per trace p
 constexpr int SPLIT_SAMPLES = 32 * SPLIT_STEPS;  // sample slots per active trace
 constexpr int SPLIT_ACTIVE_MAX = 1 << 20;         // active-set capacity (traces)
 constexpr int SPLIT_MIN_TRACES = 4096;            // runs with fewer traces use the fused kernel
-constexpr unsigned SK_SEED = 1, SK_NEAR = 2, SK_EXACT = 4;
+constexpr unsigned SK_SEED = 1, SK_NEAR = 2, SK_EXACT = 4, SK_REDO = 8;
 constexpr int ZOOM_TROUGH = 0, ZOOM_LAST = 1;
 
 }  // namespace md200
@@ -189,7 +189,6 @@ __global__ void __launch_bounds__(128, MD200_SPLIT_EVAL_BLOCKS) split_eval32(Dev
   const int lane = threadIdx.x & 31;
   const long long n = static_cast<long long>(d.ctr[C_SP_ACT0 + p]) * SPLIT_SAMPLES;
   const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
-  unsigned long long ev = 0, ev32 = 0, st = 0, st32 = 0;
   // the loop runs whole warps (n is a multiple of 32), so appends are warp-wide
   for (long long q = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; q < n; q += stride) {
     const int i = static_cast<int>(q / SPLIT_SAMPLES);
@@ -216,11 +215,6 @@ __global__ void __launch_bounds__(128, MD200_SPLIT_EVAL_BLOCKS) split_eval32(Dev
         const float c32 = static_cast<float>(c);
         float F32, g32, M32;
         scan_eval<float, WAVE, 1>(view, static_cast<float>(tr.w), &c32, &F32, &g32, &M32);
-        const unsigned long long ns = layer_steps(tr.L, tr.water);
-        ++ev;
-        ++ev32;
-        st += ns;
-        st32 += ns;
         const double g = g32;
         smp.F = F32;
         smp.g = g32;
@@ -232,16 +226,13 @@ __global__ void __launch_bounds__(128, MD200_SPLIT_EVAL_BLOCKS) split_eval32(Dev
     const int at = warp_append(&d.ctr[C_SP_REDO], redo ? 1 : 0, lane);
     if (redo) d.sp_redo[at] = static_cast<int>(q);
   }
-  split_count(d, ev, ev32, st, st32, lane);
 }
 
 // One thread per listed sample: its FP64 value (eval64_outline, as in the fused
 // scan).
 template <int WAVE>
 __global__ void __launch_bounds__(128) split_redo(Dev d, int p) {
-  const int lane = threadIdx.x & 31;
   const int n = d.ctr[C_SP_REDO];
-  unsigned long long ev = 0, st = 0;
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
     const int q = d.sp_redo[r];
     const SplitTrace tr = d.sp_tr[q / SPLIT_SAMPLES];
@@ -252,20 +243,7 @@ __global__ void __launch_bounds__(128) split_redo(Dev d, int p) {
     smp.F = F;
     smp.g = static_cast<float>(g);
     smp.M = static_cast<float>(M);
-    smp.k |= SK_EXACT;
-    ++ev;
-    st += layer_steps(tr.L, tr.water);
-  }
-  if (d.stats) {
-    const unsigned m = __activemask();
-    for (int o = 16; o; o >>= 1) {
-      ev += __shfl_xor_sync(m, ev, o);
-      st += __shfl_xor_sync(m, st, o);
-    }
-    if (lane == __ffs(m) - 1 && ev) {
-      atomicAdd(&d.stats[0], ev);
-      atomicAdd(&d.stats[2], st);
-    }
+    smp.k |= SK_EXACT | SK_REDO;
   }
 }
 
@@ -310,6 +288,9 @@ __global__ void __launch_bounds__(128) split_book(Dev d, int p) {
   const int n = d.ctr[C_SP_ACT0 + p];
   const int stride = gridDim.x * blockDim.x;
   const int n_pad = (n + 31) & ~31;
+  // counters of the samples the bookkeeping consumes, as the fused scan counts
+  // its steps' samples: each an FP32 evaluation, the re-evaluated ones also FP64
+  unsigned long long ev = 0, ev32 = 0, sts = 0, sts32 = 0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_pad; i += stride) {
     const bool active = i < n;
     int t = 0;
@@ -323,6 +304,8 @@ __global__ void __launch_bounds__(128) split_book(Dev d, int p) {
       K = d.tr_modes[t] + 2;
       double *slot = d.slot + static_cast<size_t>(t) * d.KB * SLOT;
       const size_t base = static_cast<size_t>(i) * SPLIT_SAMPLES;
+      const SplitTrace tr = d.sp_tr[i];
+      const unsigned long long nsteps = layer_steps(tr.L, tr.water);
       bool stop = false;  // the K-th bracket, the window end or a non-finite value
       int j = 0;
       for (; j < SPLIT_SAMPLES; ++j) {
@@ -338,6 +321,10 @@ __global__ void __launch_bounds__(128) split_book(Dev d, int p) {
         const double g = gf;
         const unsigned k = smp.k;
         const bool exact = (k & SK_EXACT) != 0;
+        ++ev32;
+        sts32 += nsteps;
+        ev += (k & SK_REDO) ? 2 : 1;
+        sts += (k & SK_REDO) ? 2 * nsteps : nsteps;
         if (!(isfinite(F) && isfinite(g))) {
           st.tfl |= TRACE_NONFINITE | TRACE_SEARCH_UNCONVERGED;
           st.bits |= SS_FINISHED;
@@ -432,6 +419,7 @@ __global__ void __launch_bounds__(128) split_book(Dev d, int p) {
     const int ga = warp_append(&d.ctr[C_SP_ACT0 + 1 - p], go_on ? 1 : 0, lane);
     if (go_on) d.sp_act[1 - p][ga] = t;
   }
+  split_count(d, ev, ev32, sts, sts32, lane);
 }
 
 // One warp per window request: a trough window (screened in FP32, zoomed in
