@@ -16,8 +16,9 @@ Printed JSON (rank 0, one line):
              FP32-scan speed-up)
   e2e        the same metric through the plugin's QeSolver.run (C ABI host path,
              host arrays, host<->device copies inside the timed region)
-  roofline   the FP32 scan kernel's algorithmic FP32 flop rate against the
-             measured non-tensor FP32 FMA peak of this GPU
+  roofline   the dominant kernel's (the split scan's FP32 Rayleigh evaluation
+             kernel) algorithmic FP32 flop rate against the measured non-tensor
+             FP32 FMA peak of this GPU; the whole scan stage's rate alongside
   cpu_baseline, cpu_baseline_auto
              the reference CPU engine (oracle/_ref, built from the reference
              sources) through the reference's own Solver on a bounded sample of
@@ -60,11 +61,19 @@ WORKLOAD = ("mixed-precision batch: 100000 models x 8-20 layers, 30 % with one l
 # each 1, an FMA 2; the elementary functions counted separately: 2 rsqrt and
 # 2 sin/cos-or-exp per Rayleigh step, 1 rsqrt and 1 sin/cos-or-exp per Love step).
 FLOPS_PER_STEP = {0: 170, 1: 24}
-# DRAM traffic of the FP32 Rayleigh scan per trace, dram__bytes_read.sum +
-# dram__bytes_write.sum of one ncu capture of a 2,000-model crustal launch
-# (120,000 traces: 30.7 MB + 95.4 MB), scaled to the headline launch by its trace
-# count.
-SCAN32_DRAM_BYTES_PER_TRACE = (30.661888e6 + 95.3536e6) / 120_000
+# DRAM traffic of the split scan's Rayleigh evaluation kernel (split_eval32<0>) per
+# FP32 layer step it evaluates: dram__bytes_read.sum + dram__bytes_write.sum over
+# the 9 launches of one run (1,090.3 MB + 717.8 MB), from an ncu capture of 2,000
+# mixed-precision models, divided by that run's evaluated layer steps
+# (MD200_STAT_SPLIT_EVAL_STEPS, 437,543,083).
+EVAL_DRAM_BYTES_PER_STEP = (1090339328 + 717784832) / 437543083
+
+
+def split_rounds(n_traces):
+    """Launches of the split scan's evaluation kernel in one run (the engine's
+    split_rounds: an active set of up to 2^20 traces, 3 rounds per set + 6)."""
+    cap = min(n_traces, 1 << 20)
+    return min(64, 3 * (-(-n_traces // cap)) + 6)
 
 
 def parse():
@@ -693,8 +702,13 @@ def main():
         device_run(e32, tens, B, wave, stream)
         stage[wave] = e32.stage_times()
         stats = tens["stats"][wave].cpu().numpy()
-        scan_flops += float(stats[3]) * FLOPS_PER_STEP[wave]  # FP32 layer steps (scan kernel)
+        scan_flops += float(stats[3]) * FLOPS_PER_STEP[wave]  # FP32 layer steps the scans consumed
+        if wave == 0:  # the dominant kernel: the split scan's FP32 evaluations (Rayleigh)
+            eval_flops = float(stats[19]) * FLOPS_PER_STEP[0]
+            eval_steps = float(stats[19])
     scan_ms = sum(stage[w]["scan"] for w in (0, 1))
+    eval_ms = stage[0]["scan_eval"]
+    eval_launches = split_rounds(B * T)
     e32_stats = {w: tens["stats"][w].cpu().numpy().tolist() for w in (0, 1)}
     e32.close()
 
@@ -757,7 +771,8 @@ def main():
 
     peak32 = _native.measure_peak(local, fp64=False)
     peak64 = _native.measure_peak(local, fp64=True)
-    achieved = scan_flops / (scan_ms * 1e-3)
+    achieved = eval_flops / (eval_ms * 1e-3) if eval_ms > 0 else 0.
+    scan_achieved = scan_flops / (scan_ms * 1e-3)
     cpu = cpu_auto = None
     if rank == 0 and not args.no_cpu:
         cpu = cpu_baseline(batch, periods, nmodes, args.cpu_sample)
@@ -778,14 +793,28 @@ def main():
                      "stage_ms": {("rayleigh" if w == 0 else "love"): stage64[w] for w in (0, 1)}},
             "e2e": {"value": e2e_value, "unit": "roots/s", "h2d_bytes_per_step": 2 * per_wave_in,
                     "d2h_bytes_per_step": 2 * per_wave_out},
-            "roofline": {"bound": "fp32-cuda-core", "kernel": "scan<float>", "achieved": achieved / 1e12,
-                         "peak": peak32 / 1e12, "unit": "TFLOP/s", "frac": achieved / peak32,
-                         "traffic": SCAN32_DRAM_BYTES_PER_TRACE * B * T,
-                         "traffic_note": "DRAM bytes of the Rayleigh FP32 scan launch, from an ncu capture of a smaller "
-                                         "launch scaled by traces; the algorithmic input is the model tables (~1.5 KB "
-                                         "per model): the kernel is compute-bound",
+            "roofline": {"bound": "fp32-cuda-core",
+                         "kernel": "split_eval32<0>: the FP32 Rayleigh evaluations of the split scan",
+                         "achieved": achieved / 1e12, "peak": peak32 / 1e12, "unit": "TFLOP/s",
+                         "frac": achieved / peak32,
+                         "traffic": (EVAL_DRAM_BYTES_PER_STEP * eval_steps / eval_launches
+                                     if EVAL_DRAM_BYTES_PER_STEP else None),
+                         "launches": eval_launches, "ms_per_launch": eval_ms / eval_launches,
+                         "flop_per_launch": eval_flops / eval_launches,
+                         "algorithmic_flops": "170 per Rayleigh layer step (secular.cuh, FMA = 2) x FP32 layer "
+                                              "steps the kernel evaluated (MD200_STAT_SPLIT_EVAL_STEPS), special "
+                                              "functions not counted",
+                         "traffic_note": "DRAM bytes per evaluated layer step from an ncu capture of every "
+                                         "evaluation launch of a 2,000-model run, times this launch's steps; the "
+                                         "kernel reads 32-byte sample records and the model tables and is "
+                                         "compute-bound",
                          "peak_kind": "measured FMA throughput (md200_measure_peak), not MEASURED_PEAKS.json",
-                         "fp64_peak": peak64 / 1e12, "scan_ms_per_step": scan_ms,
+                         "fp64_peak": peak64 / 1e12,
+                         "scan_stage": {"achieved": scan_achieved / 1e12, "frac": scan_achieved / peak32,
+                                        "ms_per_step": scan_ms,
+                                        "note": "the whole FP32 scan stage of both waves (split rounds for "
+                                                "Rayleigh, fused kernel for Love), algorithmic flops of the "
+                                                "samples the scans consumed"},
                          "stage_ms": {("rayleigh" if w == 0 else "love"): stage[w] for w in (0, 1)}},
             "cpu_baseline": cpu,
             "cpu_baseline_auto": cpu_auto,

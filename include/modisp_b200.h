@@ -44,7 +44,8 @@ enum md200_stat {
   MD200_STAT_FALLBACK = 16,        /* traces re-scanned by the FP64 fallback (first search unfinished) */
   MD200_STAT_CONT_ANCHORS = 17,    /* continuation anchor traces */
   MD200_STAT_CONT_EVALUATIONS = 18,/* secular evaluations of continuation targets (prediction + audit) */
-  MD200_STAT_RESERVED = 19,
+  MD200_STAT_SPLIT_EVAL_STEPS = 19,/* FP32 layer steps of the split scan's evaluation kernel (every
+                                      sample it evaluated, those past a trace's last bracket too) */
   MD200_STAT_COUNT = 20
 };
 
@@ -237,8 +238,9 @@ int md200_vjp(md200_engine *engine, const double *thickness, const double *vp, c
  * cpp/cuda/qe.cu:853-864): [0] model preparation, [1] trace list, [2] scan,
  * [3] refinement, [4] repair selection, [5] FP64 re-scan, [6] re-scan
  * refinement, [7] assembly, [8] group velocity, [9] FP64 continuity recheck
- * (screen, re-scan, refinement, assembly and group velocity of the suspects).
- * Waits for the run to finish. */
+ * (screen, re-scan, refinement, assembly and group velocity of the suspects),
+ * [10] the split scan's evaluation kernel alone (its launches summed; 0 when the
+ * run used the fused scan).  Waits for the run to finish. */
 int md200_stage_times(md200_engine *engine, double *ms, int n);
 
 /* Number of kernel launches the engine's last run enqueued (counted as it

@@ -18,7 +18,7 @@ STAT_NAMES = ("evaluations", "evaluations_fp32", "layer_steps", "layer_steps_fp3
               "trough_probes", "probe_pairs", "fp64_repair_traces", "unconverged", "group_roots",
               "roots", "traces", "dual_layer_steps", "continuation_accepted",
               "continuation_fallbacks", "continuity_rescans", "fallback_rescans", "continuation_anchors",
-              "continuation_evaluations", "reserved")
+              "continuation_evaluations", "split_eval_layer_steps")
 STAT_COUNT = 20
 
 
@@ -98,7 +98,7 @@ PERIOD_PLAN = np.dtype([("prev", np.int32), ("older", np.int32), ("kind", np.int
                         ("dup_end", np.int32), ("reserved", np.int32), ("ratio", np.float64)])
 PLAN_FIRST, PLAN_DUPLICATE, PLAN_GAP, PLAN_PREDICT = 1, 2, 4, 8
 STAGES = ("prep", "trace_list", "scan", "refine", "repair_select", "repair_scan", "repair_refine",
-          "assemble", "group_velocity", "continuity")
+          "assemble", "group_velocity", "continuity", "scan_eval")
 
 
 def lib():

@@ -134,6 +134,10 @@ struct md200_engine {
   // per-stage timing (cudaEvent pairs on the run's stream)
   static constexpr int NSTAGE = 10;
   cudaEvent_t ev[NSTAGE + 1] = {};
+  // the split scan's evaluation launches, one event pair per round
+  static constexpr int MAX_SPLIT_ROUNDS = 64;
+  cudaEvent_t sp_ev[2 * MAX_SPLIT_ROUNDS] = {};
+  int sp_timed = 0;  // rounds timed by the last run
   bool profiling = false;
   int last_launches = -1;  // kernels launched by the last run (enqueue)
   // CUDA graph of the calls captured between md200_graph_begin and md200_graph_end
@@ -163,6 +167,8 @@ void release(md200_engine *e) {
   for (auto &x : e->ev)
     if (x) cudaEventDestroy(x);
   for (auto &x : e->chunk_ev)
+    if (x) cudaEventDestroy(x);
+  for (auto &x : e->sp_ev)
     if (x) cudaEventDestroy(x);
   if (e->graph_exec) cudaGraphExecDestroy(e->graph_exec);
   if (e->graph) cudaGraphDestroy(e->graph);
@@ -282,6 +288,8 @@ int setup(md200_engine *e) {
   e->prep_smem = static_cast<size_t>(e->prep_warps) * cap2 * (sizeof(double) + sizeof(int));
   for (auto &x : e->ev) MD200_CK(cudaEventCreate(&x));
   for (auto &x : e->chunk_ev) MD200_CK(cudaEventCreateWithFlags(&x, cudaEventDisableTiming));
+  if (d.fp32)
+    for (auto &x : e->sp_ev) MD200_CK(cudaEventCreate(&x));
   MD200_CK(cudaFuncSetAttribute(prep_models, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(std::max<size_t>(e->prep_smem, 1024))));
   return 0;
@@ -316,12 +324,13 @@ struct Ragged {
 // unfinished after them are handed to the fused kernel.
 int split_rounds(int nt, int cap) {
   const int waves = (nt + cap - 1) / cap;
-  return std::min(64, 3 * waves + 6);
+  return std::min(md200_engine::MAX_SPLIT_ROUNDS, 3 * waves + 6);
 }
 
 // The split FP32 scan's launches (split_scan.cuh): `rounds` rounds, then the
 // fused kernel for the traces still unfinished (resumed from their state) and
-// for any the rounds never took from the trace list.  Returns the launch count.
+// for any the rounds never took from the trace list.  Returns the launch count,
+// or -1 when an event could not be recorded.
 template <int WAVE>
 int split_scan(md200_engine *e, const Dev &d, int rounds, cudaStream_t s) {
   const int sms = e->list_blocks / 8;
@@ -336,12 +345,15 @@ int split_scan(md200_engine *e, const Dev &d, int rounds, cudaStream_t s) {
     split_feed_count<<<1, 1, 0, s>>>(d, p);
     split_feed_fill<<<fill_blocks, 256, 0, s>>>(d, p);
     split_positions<<<pos_blocks, 128, 0, s>>>(d, p);
+    if (!e->capturing && cudaEventRecord(e->sp_ev[2 * r], s) != cudaSuccess) return -1;
     split_eval32<WAVE><<<eval_blocks, 128, 0, s>>>(d, p);
+    if (!e->capturing && cudaEventRecord(e->sp_ev[2 * r + 1], s) != cudaSuccess) return -1;
     split_redo<WAVE><<<sms * 8, 128, 0, s>>>(d, p);
     split_book<WAVE><<<book_blocks, 128, 0, s>>>(d, p);
     split_zoom<WAVE><<<sms * 4, 128, 0, s>>>(d, p);
     nl += 7;
   }
+  e->sp_timed = e->capturing ? 0 : rounds;
   const int pf = rounds & 1;
   const dim3 grid(e->scan_blocks32), block(32 * e->scan_warps);
   scan<float, WAVE><<<grid, block, e->scan_smem32, s>>>(d, d.sp_act[pf], C_SP_RESUME, C_SP_ACT0 + pf, 1);
@@ -423,9 +435,11 @@ int enqueue(md200_engine *e, const double *h, const double *vp, const double *vs
                                 (e->o.scan_mode == 0 && wave == 0 && nt >= SPLIT_MIN_TRACES));
   if (split) {
     const int rounds = split_rounds(nt, d.sp_cap);
-    if (wave == 0) nl += split_scan<0>(e, d, rounds, s);
-    else nl += split_scan<1>(e, d, rounds, s);
+    const int launched = wave == 0 ? split_scan<0>(e, d, rounds, s) : split_scan<1>(e, d, rounds, s);
+    if (launched < 0) return fail("modisp_b200 CUDA: event record failed in the split scan");
+    nl += launched;
   } else {
+    e->sp_timed = 0;
     const dim3 grid(d.fp32 ? e->scan_blocks32 : e->scan_blocks64), block(32 * e->scan_warps);
     const size_t sm = d.fp32 ? e->scan_smem32 : e->scan_smem64;
     if (d.fp32 && wave == 0) scan<float, 0><<<grid, block, sm, s>>>(d, d.trace_list, C_SCAN_CURSOR, C_NTRACE);
@@ -1074,6 +1088,15 @@ int md200_stage_times(md200_engine *e, double *ms, int n) {
     float t = 0.f;
     MD200_CK(cudaEventElapsedTime(&t, e->ev[i], e->ev[i + 1]));
     ms[i] = t;
+  }
+  if (n > md200_engine::NSTAGE) {  // the split scan's evaluation launches
+    double sum = 0.;
+    for (int r = 0; r < e->sp_timed; ++r) {
+      float t = 0.f;
+      MD200_CK(cudaEventElapsedTime(&t, e->sp_ev[2 * r], e->sp_ev[2 * r + 1]));
+      sum += t;
+    }
+    ms[md200_engine::NSTAGE] = sum;
   }
   return 0;
 }

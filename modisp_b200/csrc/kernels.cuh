@@ -906,6 +906,15 @@ __device__ __forceinline__ unsigned scan_positions(const TraceCtx &x, ScanState 
     for (int o = 16; o; o >>= 1) last = fmax(last, __shfl_xor_sync(FULL, last, o));
     if (sv > last) sv = INFINITY;
   }
+  // a step of grid points only: 32 finite grid points and the next seed at or
+  // above the last of them, so the merge would keep the grid points in place
+  const double g31 = __shfl_sync(FULL, gv, 31), s0 = __shfl_sync(FULL, sv, 0);
+  if (g31 < INFINITY && s0 >= g31) {
+    c = gv;
+    if constexpr (SRC) *seeds = 0u;
+    st.gi += 32;
+    return FULL;
+  }
   const int rg = warp_rank(sv, gv, false);  // seeds strictly below this scan point
   const int rs = warp_rank(gv, sv, true);   // scan points at or below this seed
   const int pg = lane + rg, ps = lane + rs;

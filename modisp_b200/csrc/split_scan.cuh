@@ -189,6 +189,7 @@ __global__ void __launch_bounds__(128, MD200_SPLIT_EVAL_BLOCKS) split_eval32(Dev
   const int lane = threadIdx.x & 31;
   const long long n = static_cast<long long>(d.ctr[C_SP_ACT0 + p]) * SPLIT_SAMPLES;
   const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
+  unsigned long long steps = 0;  // FP32 layer steps evaluated here (MD200_STAT_SPLIT_EVAL_STEPS)
   // the loop runs whole warps (n is a multiple of 32), so appends are warp-wide
   for (long long q = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; q < n; q += stride) {
     const int i = static_cast<int>(q / SPLIT_SAMPLES);
@@ -215,6 +216,7 @@ __global__ void __launch_bounds__(128, MD200_SPLIT_EVAL_BLOCKS) split_eval32(Dev
         const float c32 = static_cast<float>(c);
         float F32, g32, M32;
         scan_eval<float, WAVE, 1>(view, static_cast<float>(tr.w), &c32, &F32, &g32, &M32);
+        steps += layer_steps(tr.L, tr.water);
         const double g = g32;
         smp.F = F32;
         smp.g = g32;
@@ -225,6 +227,10 @@ __global__ void __launch_bounds__(128, MD200_SPLIT_EVAL_BLOCKS) split_eval32(Dev
     }
     const int at = warp_append(&d.ctr[C_SP_REDO], redo ? 1 : 0, lane);
     if (redo) d.sp_redo[at] = static_cast<int>(q);
+  }
+  if (d.stats) {
+    for (int o = 16; o; o >>= 1) steps += __shfl_xor_sync(FULL, steps, o);
+    if (lane == 0 && steps) atomicAdd(&d.stats[19], steps);
   }
 }
 

@@ -34,6 +34,7 @@ def solve(batch, periods, nmodes, wave, mode, bounds=None, **opts):
         out = e.run(h, batch["vp"], batch["vs"], batch["rho"], periods, bounds, 1e-10, 1., wave, group=True,
                     continuity=True)
         out["launches"] = e.kernel_launches()
+        out["stage_ms"] = e.stage_times()
         return out
     finally:
         e.close()
@@ -56,6 +57,8 @@ def test_split_equals_fused_on_crustal_batches(wave, lvz):
     fused = solve(batch, periods, 5, wave, FUSED)
     split = solve(batch, periods, 5, wave, SPLIT)
     assert split["launches"] > fused["launches"]  # the rounds did run
+    assert split["stats"]["split_eval_layer_steps"] > 0 and fused["stats"]["split_eval_layer_steps"] == 0
+    assert split["stage_ms"]["scan_eval"] > 0. and fused["stage_ms"]["scan_eval"] == 0.
     assert_identical(split, fused, f"crustal lvz={lvz} wave={wave}")
 
 
