@@ -659,10 +659,10 @@ def main():
     tens = device_tensors(torch, batch, periods, nmodes, local)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=torch.device("cuda", local))  # > L2
 
-    # launch shape of the scan, chosen by the autotuner on a 1,000-model sample
+    # launch shape and FP32 scan form, chosen by the autotuner on a 1,000-model sample
     from modisp_b200 import autotune
     sample = {k: v[:1000] for k, v in batch.items()}
-    tuned = {single: autotune.autotune(sample, periods, nmodes, 0, single, device=local, use_cache=False)
+    tuned = {single: autotune.autotune(sample, periods, nmodes, None, single, device=local, use_cache=False)
              for single in (True, False)}
 
     def engine(single):
@@ -787,7 +787,10 @@ def main():
                        "waves": ["rayleigh", "love"], "c_tol_rel": TOL, "l2": "flushed between steps (256 MiB write)",
                        "parallelism": f"model-sharded x{world}",
                        "scan_launch_shape": {"fp32": list(tuned[True]), "fp64": list(tuned[False]),
-                                             "chosen_by": "autotuner (warps per CTA, CTAs per SM)"}},
+                                             "chosen_by": "autotuner on 1,000 of the models, both waves: fused-scan warps "
+                                                           "per CTA, CTAs per SM, FP32 scan form (0 automatic: "
+                                                           "split rounds for Rayleigh, fused for Love; 1 fused; "
+                                                           "2 split)"}},
             "fp64": {"value": value64, "unit": "roots/s", "ms_per_step": ms64 / args.steps,
                      "fp32_scan_speedup": value / value64,
                      "stage_ms": {("rayleigh" if w == 0 else "love"): stage64[w] for w in (0, 1)}},

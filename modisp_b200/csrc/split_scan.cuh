@@ -313,9 +313,12 @@ __global__ void __launch_bounds__(128) split_book(Dev d, int p) {
       const SplitTrace tr = d.sp_tr[i];
       const unsigned long long nsteps = layer_steps(tr.L, tr.water);
       bool stop = false;  // the K-th bracket, the window end or a non-finite value
-      int j = 0;
-      for (; j < SPLIT_SAMPLES; ++j) {
-        const SplitSample smp = d.sp_s[base + j];
+      // the next record is loaded while this one is worked on (the loop is a
+      // chain of dependent decisions; its loads need not be)
+      SplitSample ahead = d.sp_s[base];
+      for (int j = 0; j < SPLIT_SAMPLES; ++j) {
+        const SplitSample smp = ahead;
+        if (j + 1 < SPLIT_SAMPLES) ahead = d.sp_s[base + j + 1];
         const double c = smp.c;
         if (!(c < INFINITY)) {  // the window is exhausted
           st.bits |= SS_FINISHED;

@@ -140,14 +140,20 @@ def test_autotuner_picks_the_fastest_shape_and_caches_it(tmp_path, monkeypatch):
 
     def timer(shape, *args):
         calls.append(shape)
-        return {(2, 0): 1.0}.get(tuple(shape), 2.0), same
+        return {(2, 0, 2): 1.0}.get(tuple(shape), 2.0), same
 
     best = autotune.autotune(sample, [1., 2.], 3, 0, True, timer=timer)
-    assert best == (2, 0) and len(calls) == len(autotune.CANDIDATES)
+    assert best == (2, 0, 2) and len(calls) == len(autotune.CANDIDATES)
+    assert {c[2] for c in autotune.CANDIDATES} == {0, 1, 2}  # both scan forms and the automatic choice
+    assert {c[2] for c in autotune.candidates(False)} == {0}  # the FP64 engine has one scan form
     table = json.loads(autotune.cache_path().read_text())
-    assert list(table.values())[0]["shape"] == [2, 0]
+    assert list(table.values())[0]["shape"] == [2, 0, 2]
     calls.clear()
-    assert autotune.autotune(sample, [1., 2.], 3, 0, True, timer=timer) == (2, 0) and not calls  # cached
+    assert autotune.autotune(sample, [1., 2.], 3, 0, True, timer=timer) == (2, 0, 2) and not calls  # cached
+    from modisp_b200 import _native
+    o = _native.Options()
+    autotune.apply(o, (2, 3, 1))
+    assert (o.warps_per_block, o.blocks_per_sm, o.scan_mode) == (2, 3, 1)
 
     def bad_timer(shape, *args):
         out = dict(same, velocity=same["velocity"] + (shape[0] == 1))
