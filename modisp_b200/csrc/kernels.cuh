@@ -807,6 +807,11 @@ __device__ __noinline__ int last_cell(const LayerView<T> view, const LayerView<d
 #ifndef MD200_SCAN_MIN_BLOCKS
 #define MD200_SCAN_MIN_BLOCKS 4
 #endif
+// resident CTAs per SM the single-precision Love scan is compiled for (its
+// recurrence is a 2-vector: fewer live registers than the Rayleigh scan's)
+#ifndef MD200_SCAN_MIN_BLOCKS_LOVE32
+#define MD200_SCAN_MIN_BLOCKS_LOVE32 MD200_SCAN_MIN_BLOCKS
+#endif
 
 // ---------------------------------------------------------------------------
 // The scan of one trace as a sequence of 32-sample steps: positions, values,
@@ -1133,7 +1138,9 @@ __device__ __forceinline__ void scan_counters_flush(const Dev &d, const ScanCoun
 // (merge buffer).
 // ---------------------------------------------------------------------------
 template <class T, int WAVE>
-__global__ void __launch_bounds__(128, MD200_SCAN_MIN_BLOCKS) scan(Dev d, const int *list, int cursor_id, int count_id,
+__global__ void __launch_bounds__(128, (sizeof(T) == 4 && WAVE == 1) ? MD200_SCAN_MIN_BLOCKS_LOVE32
+                                                                      : MD200_SCAN_MIN_BLOCKS)
+    scan(Dev d, const int *list, int cursor_id, int count_id,
                                                                    int resume = 0) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -1419,7 +1426,10 @@ __device__ __forceinline__ void refine_fetch(Dev &d, RefineLane &L, int end, int
   brent_init(L.st, L.sl[0], L.sl[1], L.sl[2], L.sl[3]);
 }
 
-__global__ void __launch_bounds__(128, 4) refine(Dev d) {
+#ifndef MD200_REFINE_MIN_BLOCKS
+#define MD200_REFINE_MIN_BLOCKS 4
+#endif
+__global__ void __launch_bounds__(128, MD200_REFINE_MIN_BLOCKS) refine(Dev d) {
   const int lane = threadIdx.x & 31;
   const int end = d.ctr[C_NREFINE];
   unsigned long long evals = 0, steps = 0, count = 0;
@@ -1795,7 +1805,10 @@ __global__ void continuity_finish(Dev d) {
 // group: one thread per root.  U = -F_k / F_omega from one forward-mode
 // evaluation (value + two directional derivatives) at the refined root.
 // ---------------------------------------------------------------------------
-__global__ void group_velocity(Dev d) {
+#ifndef MD200_GROUP_MIN_BLOCKS
+#define MD200_GROUP_MIN_BLOCKS 1
+#endif
+__global__ void __launch_bounds__(128, MD200_GROUP_MIN_BLOCKS) group_velocity(Dev d) {
   const int n = d.ctr[C_NGROUP];
   unsigned long long steps = 0, count = 0;
   for (int i = d.ctr[C_GROUP_BEGIN] + blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {

@@ -34,6 +34,10 @@
 
 namespace md200 {
 
+// Compile-time tuning: 32-sample steps per trace per round (two measured best:
+// fewer samples evaluated past a trace's last bracket than four, half the
+// rounds of one) and the evaluation kernel's minimum resident CTAs per SM (1:
+// no register cap; capping it measured no faster).
 #ifndef MD200_SPLIT_STEPS
 #define MD200_SPLIT_STEPS 2
 #endif

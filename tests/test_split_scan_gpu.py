@@ -122,3 +122,15 @@ def test_split_equals_fused_on_the_large_uneven_workload(wave):
         np.testing.assert_array_equal(a[key].view(np.uint64), b[key].view(np.uint64), err_msg=key)
     for key in ("flags", "levels", "counts"):
         np.testing.assert_array_equal(a[key], b[key], err_msg=key)
+
+
+def test_split_equals_fused_beyond_one_active_set():
+    """More traces than the active set holds (2^20): the set is refilled from the
+    trace list round after round, and the fused kernel finishes whatever the rounds
+    leave -- still the fused scan's results bit for bit."""
+    from modisp_b200 import workloads
+    batch = workloads.crustal_batch(18_000, workloads.SEED + 85, lvz_fraction=0.3)
+    periods = np.geomspace(0.5, 50., 60)  # 1,080,000 traces
+    split = solve(batch, periods, 5, 0, SPLIT)
+    fused = solve(batch, periods, 5, 0, FUSED)
+    assert_identical(split, fused, "beyond one active set")
