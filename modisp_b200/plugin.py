@@ -89,21 +89,35 @@ _cast_pool = None
 _cast_lock = threading.Lock()
 
 
+def _pool():
+    global _cast_pool
+    with _cast_lock:
+        if _cast_pool is None:
+            _cast_pool = ThreadPoolExecutor(8, thread_name_prefix="md200-cast")
+    return _cast_pool
+
+
+def _count_nonzero(a):
+    """np.count_nonzero of a large array, counted in slices on 8 threads (numpy
+    releases the GIL while counting)."""
+    if a.size < 1 << 20:
+        return int(np.count_nonzero(a))
+    flat = a.reshape(-1)
+    step = -(-flat.size // 8)
+    return int(sum(_pool().map(lambda i: np.count_nonzero(flat[i * step:(i + 1) * step]), range(8))))
+
+
 def _to_float32(a):
     """float32 copy of a float64 array (the reference's FP32-mode output type),
     converted in slices on 8 threads for large arrays: numpy releases the GIL
     while casting, and the rounding is the same as astype's."""
-    global _cast_pool
     if a.size < 1 << 20:
         return a.astype(np.float32)
-    with _cast_lock:
-        if _cast_pool is None:
-            _cast_pool = ThreadPoolExecutor(8, thread_name_prefix="md200-cast")
     out = np.empty(a.shape, np.float32)
     src, dst = a.reshape(-1), out.reshape(-1)
     step = -(-src.size // 8)
-    list(_cast_pool.map(lambda i: np.copyto(dst[i * step:(i + 1) * step], src[i * step:(i + 1) * step],
-                                            casting="same_kind"), range(8)))
+    list(_pool().map(lambda i: np.copyto(dst[i * step:(i + 1) * step], src[i * step:(i + 1) * step],
+                                         casting="same_kind"), range(8)))
     return out
 
 
@@ -200,7 +214,7 @@ class QeSolver:
             # the counters the reference's continuity review adds to
             # (python/modisp/_continuity.py:112-119, :136-137; cpp/cpu/solver.cpp:748-749)
             stats["group_evaluations"] = int(stats.get("group_roots", 0))
-            stats["group_invalid"] = int(np.count_nonzero(out["group_velocity_flags"]))
+            stats["group_invalid"] = _count_nonzero(out["group_velocity_flags"])
         extras = dict(group_velocity=out.get("group_velocity"),
                       group_velocity_flags=out.get("group_velocity_flags"),
                       prediction_flags=out.get("prediction_flags"))
