@@ -45,7 +45,7 @@ using Q2 = Dual<D2, 2>;      // d/d(h, 1/v) of one wave block
 using P4 = Dual<D2, 4>;      // d/d(h, vp, vs, rho) of one row (start vector, fluid top)
 
 constexpr int JAC_SEG = 12;     // layer steps per recomputed segment
-constexpr int JAC_MAXSEG = 12;  // checkpoints: up to 144 layer steps (145 rows)
+constexpr int JAC_MAXSEG = 22;  // checkpoints: up to 264 layer steps (the API's 256 rows fit)
 constexpr int JAC_MAX_STEPS = JAC_SEG * JAC_MAXSEG;
 
 MD200_FN P4 lift4(const D2 &x) {
@@ -317,7 +317,7 @@ MD200_HD bool root_adjoint(const LayerView<double> &m, const double *tab, double
   const K1 iwx = K1(1) / ww, iw2x = iwx * iwx, k2x = kk * kk;
 
   D2 ck[JAC_MAXSEG][NV];
-  int ex[JAC_MAX_STEPS];
+  short ex[JAC_MAX_STEPS];  // per-step binade exponents of a double, |e| < 1100
   int ex0 = 0, pex = 0;
 
   // ---- 1. forward sweep, exponents and checkpoints ----
@@ -337,7 +337,7 @@ MD200_HD bool root_adjoint(const LayerView<double> &m, const double *tab, double
     if (s % JAC_SEG == 0)
       for (int i = 0; i < NV; ++i) ck[s / JAC_SEG][i] = e[i].v;
     if constexpr (WAVE == 0) {
-      ex[s] = rayleigh_step_k1(e, kk, k2x, ww, iw2x, m.h(l), m.ivp(l), m.vs2(l), m.ivs(l), m.rho(l), m.irho(l));
+      ex[s] = (short)rayleigh_step_k1(e, kk, k2x, ww, iw2x, m.h(l), m.ivp(l), m.vs2(l), m.ivs(l), m.rho(l), m.irho(l));
     } else {
       const K1 kj = ww * m.ivs(l);
       K1 cq, y, z;
@@ -347,7 +347,7 @@ MD200_HD bool root_adjoint(const LayerView<double> &m, const double *tab, double
       const K1 v = e[0] * y * m.imu(l) + e[1] * cq;
       e[0] = u;
       e[1] = v;
-      ex[s] = scale_vector(e, NV, tiny);
+      ex[s] = (short)scale_vector(e, NV, tiny);
     }
   }
   K1 F;

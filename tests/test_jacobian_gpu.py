@@ -190,3 +190,35 @@ def test_autograd_misfit_gradient():
         assert checked == 5
     finally:
         solver.close()
+
+
+@pytest.mark.parametrize("wave", [0, 1])
+@pytest.mark.parametrize("single", [False, True])
+def test_jacobians_at_the_largest_layer_count(wave, single, oracle_lib):
+    """256 rows (255 thin layers over a half-space), the most the API accepts
+    (python/modisp/__init__.py:152): the adjoint's checkpoints cover all 255
+    layer steps, and the rows match the oracle's complex-step Jacobian."""
+    L = 256
+    z = np.arange(L - 1)
+    vs = np.concatenate([2.0 + 2.5 * z / (L - 2), [4.7]])
+    model = [np.full(L, 0.2), 1.75 * vs, vs, 1.6 + 0.3 * vs]
+    model[0][-1] = 0.
+    model = [np.ascontiguousarray(np.stack([x, x * (1. + 0.02 * (wave + 1))]), dtype=np.float64)
+             for x in model]
+    periods = np.array([4., 15., 40.])
+    eng = _engine(2, L, periods.size, 2, single)
+    try:
+        out = eng.run(*model, periods, None, 1e-12, 1., wave, group=True)
+        v = out["velocity"]
+        jc, ju, failed = eng.jacobian(*model, periods, wave, v, out["group_velocity"])
+    finally:
+        eng.close()
+    assert failed == 0
+    cells = list(zip(*np.nonzero(np.isfinite(v))))
+    assert len(cells) >= 8
+    worst = 0.
+    for b, m, f in cells:
+        row = [x[b] for x in model]
+        worst = max(worst, _row_err(jc[b, m, f], oracle_lib.phase_jacobian(*row, periods[f], v[b, m, f], wave)))
+        assert np.isfinite(ju[b, m, f]).all()
+    assert worst < PHASE_TOL_ORACLE, worst
