@@ -91,6 +91,7 @@ def parse():
     p.add_argument("--no-config2", action="store_true")
     p.add_argument("--no-reliability", action="store_true")
     p.add_argument("--no-reference-cuda", action="store_true")
+    p.add_argument("--no-uniform", action="store_true")
     return p.parse_args()
 
 
@@ -281,6 +282,61 @@ def reference_cuda_bench(batch, periods, nmodes, local, sample=10_000, ours=None
                 np.any(masks[w] != np.isfinite(ours[w][:sample]), axis=1).sum() for w in (0, 1)))
     out["sample"] = (f"{sample} models of the batch, accuracy='high' shape-adaptive, c_tol_rel={TOL:g}, group "
                      f"velocity, QeSolver.run on host arrays (the wrapper's call), 2 timed calls per wave")
+    return out
+
+
+def uniform_bench(local, models=10_000, nc=512, cmin=0.2, calls=2):
+    """The legacy uniform-grid path (search_strategy="uniform") on the 10,000-model
+    crustal batch, Rayleigh, 60 periods, 5 modes, nc 512 over [0.2, the largest
+    half-space vs]: this engine's CoarseScan/Refine and, beside it, the reference's
+    own CUDA stages (compiled for sm_100a) through the same calls as the legacy
+    solver makes them (python/modisp/_legacy.py:300-340: upload, scan, refine,
+    download of roots and flags); one warm-up and `calls` timed calls each."""
+    import oracle
+    from modisp_b200 import plugin, workloads
+    batch, periods, nmodes = workloads.config2(models)
+    h, vp, vs, rho = (np.ascontiguousarray(batch[k]) for k in ("thickness", "vp", "vs", "rho"))
+    B, L = h.shape
+    cmax = float(vs[:, -1].max())
+
+    def arm(mod):
+        scan, refine = mod.CoarseScan(B, L), mod.Refine(B, L)
+        for stage in (scan, refine):
+            stage.upload_periods(periods)
+        scan.allocate(nc)
+        refine.allocate(nc, nmodes)
+
+        def call():
+            for stage in (scan, refine):
+                stage.upload_models(h, vp, vs, rho)
+            scan.run(cmin, cmax, 256)
+            refine.run(scan, cmin, cmax, 1e-6, 1., nmodes, 256)
+            return refine.download(), refine.flags()
+
+        call()
+        t = time.perf_counter()
+        for _ in range(calls):
+            v, f = call()
+        return (time.perf_counter() - t) / calls, v, f
+
+    out = {"workload": f"{B} crustal models (8-20 layers), Rayleigh, 60 periods 0.5-50 s, {nmodes} modes, nc {nc}, "
+                       f"cmin {cmin}, cmax {cmax:.4g}, c_tol_rel 1e-6; host arrays in and out, {calls} timed calls",
+           "unit": "roots/s"}
+    sec, v, f = arm(plugin)
+    out["ours"] = {"value": int(np.isfinite(v).sum()) / sec, "seconds_per_call": sec}
+    ref = oracle.reference_cuda()
+    if ref is None:
+        out["reference"] = {"unavailable": "reference CUDA plugin not built (make -C oracle ref-cuda REFERENCE=...)"}
+        return out
+    ref.set_device(local)
+    rsec, rv, rf = arm(ref)
+    out["reference"] = {"value": int(np.isfinite(rv).sum()) / rsec, "seconds_per_call": rsec}
+    out["speedup"] = rsec / sec
+    both = np.isfinite(v) & np.isfinite(rv)
+    out["agreement"] = {"mask_mismatch_traces": int(np.any(np.isfinite(v) != np.isfinite(rv), axis=1).sum()),
+                        "flag_mismatch_traces": int((f != rf).sum()),
+                        "max_abs_root_difference": float(np.abs(v[both] - rv[both]).max(initial=0.)),
+                        "roots": int(np.isfinite(rv).sum())}
     return out
 
 
@@ -768,6 +824,7 @@ def main():
                    if side and not args.no_reliability else None)
     ref_cuda = (reference_cuda_bench(batch, periods, nmodes, local, ours={w: out64[w][0] for w in (0, 1)})
                 if side and rank == 0 and not args.no_reference_cuda else None)
+    uniform = uniform_bench(local) if side and rank == 0 and not args.no_uniform else None
 
     peak32 = _native.measure_peak(local, fp64=False)
     peak64 = _native.measure_peak(local, fp64=True)
@@ -830,6 +887,7 @@ def main():
             "jacobian": jac,
             "ragged": ragged,
             "reliability": reliability,
+            "uniform": uniform,
         }
         print(json.dumps(line))
     if world > 1:

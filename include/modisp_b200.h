@@ -199,7 +199,7 @@ int md200_graph_launch(md200_engine *engine, void *stream);
  * adjoint sweep through the layer recurrence (adjoint.cuh).  Rows of zero
  * thickness (padding) and the half-space thickness get 0; NaN rows mark a
  * missing root (or, for jac_group, a missing group velocity where `group` is
- * given) or a root with F_k = 0 or F_omega = 0.  Models of up to 145 rows.
+ * given) or a root with F_k = 0 or F_omega = 0.  Models of up to 265 rows.
  * Device pointers, enqueued on `stream` (NULL = the engine's stream). */
 int md200_jacobian_device(md200_engine *engine, const double *thickness, const double *vp,
                           const double *vs, const double *rho, int models, const double *periods,
@@ -367,6 +367,82 @@ int md200_group_roots_static(const double *thickness, const double *vp, const do
                              const double *rho, int layers, int wave, double period,
                              const double *roots, int known, int modes, double close_rtol,
                              double *group, unsigned *group_flags);
+
+/* ---------------------------------------------------------------------------
+ * Legacy uniform-grid Rayleigh path (the reference's search_strategy="uniform",
+ * python/modisp/_legacy.py:124-431, bound as the plugin classes CoarseScan and
+ * Refine of cpp/cuda/bindings.cpp:121-345).  One object type serves both of the
+ * reference's stage states: a scan object (md200_uniform_grid with nmodes = 0)
+ * holds FP32 secular values on the grid c_i = cmin + i (cmax - cmin) / (nc - 1)
+ * per (model, period); a refinement object (nmodes > 0) reads a scan object's
+ * values and holds roots [models][nmodes][periods] (NaN where a mode is
+ * missing), per-trace flags (1 unresolved bracket, 2 relocated bracket) and six
+ * counters (brackets, rejected_sign, rejected_f, troughs, hidden_roots,
+ * relocated).  Solid models only (every vs > 0); periods are kept in single
+ * precision as the reference keeps them.  Work is enqueued on the legacy default
+ * stream (so calls on different objects are ordered); copies to the host wait
+ * for it.  Errors return 1 with md200_last_error(); numerical problems are
+ * flags and NaN, never errors.
+ * ------------------------------------------------------------------------- */
+typedef struct md200_uniform md200_uniform;
+
+/* Replaces md_cuda_create (cpp/cuda/coarse_scan.cu:63) and md_refine_create
+ * (cpp/cuda/refine.cu:48): B models of L rows (layers plus half-space, L >= 2). */
+md200_uniform *md200_uniform_create(int models, int layers);
+
+/* Replaces md_cuda_upload_models (coarse_scan.cu:89) / md_refine_upload_models
+ * (refine.cu:73): four [B][L] arrays; zero-thickness rows are identity steps. */
+int md200_uniform_models(md200_uniform *u, const double *thickness, const double *vp, const double *vs,
+                         const double *rho);
+
+/* Replaces md_cuda_upload_periods (coarse_scan.cu:111) / md_refine_upload_periods
+ * (refine.cu:94); a different period count drops the allocated outputs. */
+int md200_uniform_periods(md200_uniform *u, int periods, const double *values);
+
+/* Replaces md_cuda_set_output (coarse_scan.cu:150; nmodes = 0, nc >= 1) and
+ * md_refine_set_output (refine.cu:138; nmodes >= 1, nc >= 2). */
+int md200_uniform_grid(md200_uniform *u, int nc, int nmodes);
+
+/* Replaces md_cuda_run (coarse_scan.cu:183): enqueue the FP32 values over
+ * [cmin, cmax]; cells past the half-space shear velocity's last cell are NaN. */
+int md200_uniform_scan(md200_uniform *u, double cmin, double cmax);
+
+/* Replaces md_cuda_download (coarse_scan.cu:252): float [B][periods][nc]. */
+int md200_uniform_rows(md200_uniform *u, float *rows);
+
+/* Stage 1 values from the caller instead of md200_uniform_scan: float
+ * [B][periods][nc] as md200_uniform_rows returns them, taken as a scan over
+ * [cmin, cmax].  No counterpart in the reference (whose refinement reads only its
+ * own scan's device buffer, cpp/cuda/bindings.cpp:263-279); it lets stage 2 run
+ * on values computed elsewhere, such as another implementation's stage 1. */
+int md200_uniform_set_rows(md200_uniform *u, const float *rows, double cmin, double cmax);
+
+/* Replaces md_refine_run (refine.cu:191): enqueue stage 2 on `scan`'s values
+ * (same B, L, periods and nc; the range its last md200_uniform_scan ran with).
+ * nmodes 0 keeps the allocated count; c_tol_rel sets the bisection count
+ * (md200_uniform_iterations), f_accept < 1 rejects roots with |F| above it. */
+int md200_uniform_refine(md200_uniform *u, const md200_uniform *scan, double cmin, double cmax,
+                         double c_tol_rel, double f_accept, int nmodes);
+
+/* Replaces md_cuda_sync / md_refine_sync (coarse_scan.cu:225, refine.cu:256). */
+int md200_uniform_sync(void);
+
+/* Replace md_refine_download (refine.cu:262), md_refine_flags (refine.cu:376)
+ * and md_refine_stats (refine.cu:291; n >= 6). */
+int md200_uniform_velocity(md200_uniform *u, double *velocity);
+int md200_uniform_flags(md200_uniform *u, uint32_t *flags);
+int md200_uniform_stats(md200_uniform *u, uint64_t *stats, int n);
+
+/* Replaces md_refine_iters_for (refine.cu:333): bisections for a cell of width
+ * dc to reach c_tol_rel * cmin (1..60). */
+int md200_uniform_iterations(double dc, double c_tol_rel, double cmin);
+
+/* Replaces md_cuda_kernel_report / md_refine_kernel_report (coarse_scan.cu:279,
+ * refine.cu:337): stage 0 the scan kernel, 1 the bisection kernel. */
+int md200_uniform_kernel_report(int stage, int layers, int block, char *text, int length);
+
+/* Replaces md_cuda_free / md_refine_free. */
+void md200_uniform_destroy(md200_uniform *u);
 
 #ifdef __cplusplus
 }

@@ -92,7 +92,24 @@ EXPORTS = {
     "md200_mode_reliability": (_I, [_I, _P, _P, _P, _I, _I, _I, _P, _P, _D, _D, _D, _P, _P]),
     "md200_mode_reliability_device": (_I, [_P, _P, _P, _I, _I, _I, _P, _P, _D, _D, _D, _P, _P, _P]),
     "md200_mode_reliability_planned": (_I, [_P, _P, _P, _I, _I, _I, _P, _P, _D, _D, _D, _P, _P, _P]),
+    "md200_uniform_create": (_P, [_I, _I]),
+    "md200_uniform_destroy": (None, [_P]),
+    "md200_uniform_models": (_I, [_P, _P, _P, _P, _P]),
+    "md200_uniform_periods": (_I, [_P, _I, _P]),
+    "md200_uniform_grid": (_I, [_P, _I, _I]),
+    "md200_uniform_scan": (_I, [_P, _D, _D]),
+    "md200_uniform_rows": (_I, [_P, _P]),
+    "md200_uniform_set_rows": (_I, [_P, _P, _D, _D]),
+    "md200_uniform_refine": (_I, [_P, _P, _D, _D, _D, _D, _I]),
+    "md200_uniform_sync": (_I, []),
+    "md200_uniform_velocity": (_I, [_P, _P]),
+    "md200_uniform_flags": (_I, [_P, _P]),
+    "md200_uniform_stats": (_I, [_P, _P, _I]),
+    "md200_uniform_iterations": (_I, [_D, _D, _D]),
+    "md200_uniform_kernel_report": (_I, [_I, _I, _I, ctypes.c_char_p, _I]),
 }
+# counters of the legacy uniform path, in C ABI order (cpp/cuda/bindings.cpp:58-59)
+UNIFORM_STAT_NAMES = ("brackets", "rejected_sign", "rejected_f", "troughs", "hidden_roots", "relocated")
 # md200_period_plan (include/modisp_b200.h)
 PERIOD_PLAN = np.dtype([("prev", np.int32), ("older", np.int32), ("kind", np.int32), ("dup_begin", np.int32),
                         ("dup_end", np.int32), ("reserved", np.int32), ("ratio", np.float64)])
@@ -455,3 +472,85 @@ def kernel_report(layers: int, single_precision: bool = False) -> dict:
     buf = ctypes.create_string_buffer(8192)
     check(lib().md200_kernel_report(int(layers), int(bool(single_precision)), buf, 8192))
     return json.loads(buf.value.decode())
+
+
+class Uniform:
+    """One md200_uniform object (the legacy uniform-grid path): a scan object
+    after ``grid(nc)``, a refinement object after ``grid(nc, nmodes)``.  Plain
+    handle methods over the C ABI; argument checks and the reference's error
+    types live in the plugin's CoarseScan and Refine."""
+
+    def __init__(self, models: int, layers: int):
+        self.B, self.L = int(models), int(layers)
+        self._h = lib().md200_uniform_create(self.B, self.L)
+        if not self._h:
+            raise RuntimeError(last_error())
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().md200_uniform_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def models(self, h, vp, vs, rho) -> None:
+        a = [np.ascontiguousarray(x, dtype=np.float64) for x in (h, vp, vs, rho)]
+        check(lib().md200_uniform_models(self._h, *(ptr(x) for x in a)))
+
+    def periods(self, periods) -> None:
+        p = np.ascontiguousarray(periods, dtype=np.float64)
+        check(lib().md200_uniform_periods(self._h, int(p.size), ptr(p)))
+
+    def grid(self, nc: int, nmodes: int = 0) -> None:
+        check(lib().md200_uniform_grid(self._h, int(nc), int(nmodes)))
+
+    def scan(self, cmin: float, cmax: float) -> None:
+        check(lib().md200_uniform_scan(self._h, float(cmin), float(cmax)))
+
+    def rows(self, nf: int, nc: int) -> np.ndarray:
+        out = np.empty((self.B, nf, nc), np.float32)
+        check(lib().md200_uniform_rows(self._h, ptr(out)))
+        return out
+
+    def set_rows(self, rows, cmin: float, cmax: float) -> None:
+        r = np.ascontiguousarray(rows, dtype=np.float32)
+        if r.size != self.B * np.prod(r.shape[1:]) or r.shape[0] != self.B:
+            raise ValueError("rows must be [models, periods, nc]")
+        check(lib().md200_uniform_set_rows(self._h, ptr(r), float(cmin), float(cmax)))
+
+    def refine(self, scan: "Uniform", cmin, cmax, c_tol_rel, f_accept, nmodes) -> None:
+        check(lib().md200_uniform_refine(self._h, scan._h, float(cmin), float(cmax), float(c_tol_rel),
+                                         float(f_accept), int(nmodes)))
+
+    @staticmethod
+    def sync() -> None:
+        check(lib().md200_uniform_sync())
+
+    def velocity(self, nmodes: int, nf: int) -> np.ndarray:
+        out = np.empty((self.B, nmodes, nf), np.float64)
+        check(lib().md200_uniform_velocity(self._h, ptr(out)))
+        return out
+
+    def flags(self, nf: int) -> np.ndarray:
+        out = np.empty((self.B, nf), np.uint32)
+        check(lib().md200_uniform_flags(self._h, ptr(out)))
+        return out
+
+    def stats(self) -> dict:
+        out = np.zeros(len(UNIFORM_STAT_NAMES), np.uint64)
+        check(lib().md200_uniform_stats(self._h, ptr(out), out.size))
+        return {k: int(v) for k, v in zip(UNIFORM_STAT_NAMES, out)}
+
+    @staticmethod
+    def iterations(dc: float, c_tol_rel: float, cmin: float) -> int:
+        return int(lib().md200_uniform_iterations(float(dc), float(c_tol_rel), float(cmin)))
+
+    @staticmethod
+    def kernel_report(stage: int, layers: int, block: int = 256) -> str:
+        buf = ctypes.create_string_buffer(512)
+        check(lib().md200_uniform_kernel_report(int(stage), int(layers), int(block), buf, 512))
+        return buf.value.decode()

@@ -233,8 +233,6 @@ class Solver:
             raise ValueError("backend must be auto, cuda or b200")
         if search_strategy not in ("shape_adaptive", "qe_adaptive", "uniform"):
             raise ValueError("invalid search_strategy")
-        if search_strategy == "uniform":
-            raise NotImplementedError("the legacy uniform strategy is not offered; use an adaptive strategy")
         if not isinstance(continuity_check, (bool, np.bool_)):
             raise ValueError("continuity_check must be boolean")
         if not isinstance(group_velocity, (bool, np.bool_)):
@@ -247,22 +245,33 @@ class Solver:
         if (not isinstance(anchor_stride, (int, np.integer)) or isinstance(anchor_stride, (bool, np.bool_))
                 or anchor_stride < 2):
             raise ValueError("anchor_stride must be an integer of at least 2")
+        uniform = search_strategy == "uniform"  # the legacy path (python/modisp/__init__.py:194-217)
+        if uniform and (group_velocity or frequency_strategy != "independent"):
+            raise NotImplementedError("group velocity and frequency continuation require an adaptive solver")
         if not isinstance(precision, str) or precision not in ("float64", "float32", "mixed"):
             raise ValueError("precision must be float64, mixed or float32")
+        if uniform and precision != "float64":
+            raise ValueError("precision='float32' requires an adaptive CUDA solver")
         if secular not in (None, "dunkin", "fast"):
             raise ValueError("secular must be None, 'dunkin' or 'fast'")
         if refinement is None:
-            refinement = "brent"
+            refinement = "legacy" if uniform else "brent"
         if refinement not in ("legacy", "brent", "chandrupatla"):
             raise ValueError("refinement must be legacy, brent or chandrupatla")
         if love_strategy not in ("phase", "scan"):
             raise ValueError("love_strategy must be phase or scan")
-        if accuracy is None:
-            accuracy = DEFAULT_ACCURACY
+        if uniform and refinement != "legacy":
+            raise NotImplementedError("uniform supports only legacy refinement")
+        if uniform and secular == "fast":
+            raise NotImplementedError("secular='fast' is not available on the legacy uniform CUDA path")
+        if accuracy is None or (accuracy == "auto" and uniform):
+            accuracy = "uniform" if uniform else DEFAULT_ACCURACY
         elif accuracy not in ("auto", "high", "balanced", "fast"):
             raise ValueError("accuracy must be auto, high, balanced or fast")
+        elif uniform:
+            raise ValueError("accuracy applies only to adaptive strategies; uniform is the legacy fixed path")
         if adaptive_period_threshold is not None:
-            if accuracy == "high":
+            if accuracy in ("high", "uniform"):
                 raise ValueError("adaptive_period_threshold applies only to auto/balanced/fast")
             if not np.isfinite(adaptive_period_threshold) or adaptive_period_threshold <= 0:
                 raise ValueError("adaptive_period_threshold must be finite and positive")
@@ -272,12 +281,12 @@ class Solver:
         if sampling_rtol is not None and search_strategy != "shape_adaptive":
             raise ValueError("sampling_rtol applies only to shape_adaptive")
         if sampling_rtol is None:
-            sampling_rtol = {"auto": 1e-2, "high": 1e-3, "balanced": 1e-2, "fast": 5e-2}[accuracy]
+            sampling_rtol = {"auto": 1e-2, "high": 1e-3, "balanced": 1e-2, "fast": 5e-2, "uniform": 1e-3}[accuracy]
         if (not np.isscalar(sampling_rtol) or np.iscomplexobj(sampling_rtol) or not np.isfinite(sampling_rtol)
                 or not 0 < sampling_rtol <= 1):
             raise ValueError("sampling_rtol must be finite and between 0 and 1")
         if c_tol_rel is None:
-            c_tol_rel = {"auto": 1e-5, "high": 1e-6, "balanced": 1e-5, "fast": 1e-4}[accuracy]
+            c_tol_rel = {"auto": 1e-5, "high": 1e-6, "balanced": 1e-5, "fast": 1e-4, "uniform": 1e-6}[accuracy]
         for name, v in (("cmin", cmin), ("cmax", cmax)):
             if v is not None and (not np.isfinite(v) or v <= 0):
                 raise ValueError(f"{name} must be finite and positive")
@@ -311,6 +320,7 @@ class Solver:
                            warps_per_block=warps_per_block, blocks_per_sm=blocks_per_sm)
         self._engine = None
         self._engine_key = None
+        self._legacy = None
         self._calls = 0
         self._last_stats = None
         self.last_result = None
@@ -387,6 +397,8 @@ class Solver:
             if per.max() > max_value or per.min() < 2. * np.pi / max_value:
                 raise ValueError("periods or their angular frequencies are outside the float32 range")
         backend, reason = self._select()
+        if self.search_strategy == "uniform":
+            return self._solve_uniform(h, a, b, r, per, nmodes, wave, backend, reason, started)
         input_periods = per
         inverse = None
         # frequency strategy (python/modisp/__init__.py:318-340): continuation runs on
@@ -493,6 +505,42 @@ class Solver:
         self.last_result = result
         return result
 
+    def _solve_uniform(self, h, a, b, r, per, nmodes, wave, backend, reason, started):
+        """The legacy uniform path as the reference's Solver wraps it
+        (python/modisp/__init__.py:302-311): solid Rayleigh only, cmin 0.2 unless
+        given, every trace flagged TRACE_RANGE_TRUNCATED, search level -2."""
+        from .legacy import UniformSolver
+        B, L = h.shape
+        if wave != "rayleigh" or np.any(b == 0) or L < 2:
+            raise NotImplementedError("uniform is the legacy CUDA solid-Rayleigh option; use qe_adaptive for this "
+                                      "combination")
+        cmin = .2 if self.cmin is None else self.cmin
+        if self._legacy is None:
+            self._legacy = UniformSolver(self.nc, cmin, self.cmax, self.c_tol_rel, self.f_accept, self.block)
+        velocity, flags, legacy_stats, _ = self._legacy(h, a, b, r, per, nmodes)
+        vs_hs = b[:, -1]
+        bounds = np.empty((B, 2))
+        bounds[:, 0] = cmin
+        bounds[:, 1] = np.fmin(vs_hs if self.cmax is None else self.cmax, np.nextafter(vs_hs, 0.))
+        flags = flags | TRACE_RANGE_TRUNCATED
+        levels = np.full((B, per.size), -2, np.int32)
+        counts = np.sum(np.isfinite(velocity), axis=1, dtype=np.int32)
+        result = DispersionBatch(velocity, per, nmodes, wave, flags, levels, counts, bounds, backend, reason,
+                                 accuracy="uniform", close_root_rtol=self.close_root_rtol, search_strategy="uniform",
+                                 secular="dunkin", refinement="legacy")
+        stats = dict(legacy_stats)
+        stats.update(backend=backend, accuracy="uniform", precision=self.precision,
+                     close_root_rtol=self.close_root_rtol, secular="dunkin", secular_kernel="dunkin",
+                     refinement="legacy", love_strategy=None, group_velocity=False, group_rtol=self.group_rtol,
+                     frequency_strategy="independent", frequency_strategy_used="independent",
+                     anchor_stride=self.anchor_stride)
+        if self.profile:
+            stats["timings_s"] = {"solver_total": time.perf_counter() - started}
+        self._last_stats = stats
+        self._calls += 1
+        self.last_result = result
+        return result
+
     @property
     def calls(self):
         return self._calls
@@ -504,6 +552,11 @@ class Solver:
 
     def kernel_report(self):
         from . import plugin
+        if self.search_strategy == "uniform" and self._legacy is not None:
+            return {"backend": "cuda", "precision": "float32 scan / float64 refinement", "accuracy": "uniform",
+                    "secular": "dunkin", "secular_kernel": "dunkin", "refinement": "legacy", "love_strategy": None,
+                    "group_velocity": False, "frequency_strategy": "independent",
+                    "frequency_strategy_used": "independent", "legacy": self._legacy.kernel_report()}
         L = self._engine.layers if self._engine is not None else 21
         report = plugin.qe_kernel_report(L, int(self.accuracy != "high"), True, self.precision != "float64")
         report.update(backend="cuda", precision=self.precision, accuracy=self.accuracy,
@@ -516,6 +569,9 @@ class Solver:
                 self._engine.close()
             self._engine = None
             self._engine_key = None
+            if self._legacy is not None:
+                self._legacy.close()
+            self._legacy = None
 
     def __enter__(self):
         return self

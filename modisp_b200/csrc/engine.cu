@@ -22,6 +22,7 @@
 #include "reliability.cuh"
 #include "continuation.cuh"
 #include "split_scan.cuh"
+#include "uniform.cuh"
 
 using namespace md200;
 
@@ -1540,6 +1541,364 @@ int md200_group_roots_static(const double *h, const double *vp, const double *vs
     MD200_CK(cudaGetLastError());
     MD200_CK(cudaMemcpy(group, dgrp, sizeof(double) * modes, cudaMemcpyDeviceToHost));
     MD200_CK(cudaMemcpy(group_flags, dfl, sizeof(unsigned) * modes, cudaMemcpyDeviceToHost));
+    return 0;
+  } catch (...) {
+    return fail_exception();
+  }
+}
+
+
+// ---------------------------------------------------------------------------
+// Legacy uniform-grid path (the reference's search_strategy="uniform"): one
+// object type for the reference's two stage states, md_cuda_state
+// (cpp/cuda/coarse_scan.cu:63-300) and md_refine_state (cpp/cuda/refine.cu:48-400).
+// A scan object holds the stage 1 rows, a refinement object the roots, flags and
+// counters; both hold their models' tables.  All work runs on the legacy default
+// stream, as the reference's does, so a refinement and the scan whose rows it
+// reads, and the next scan that overwrites them, are ordered without events.
+// ---------------------------------------------------------------------------
+}  // extern "C"
+
+struct md200_uniform {
+  int B = 0, L = 0, nf = 0, nc = 0, K = 0;
+  int alloc_nf = 0, alloc_nc = 0, alloc_K = 0;  // geometry of the allocated outputs
+  bool models = false, ran = false;
+  double cmin = 0., cmax = 0.;  // range of the last scan
+  int sms = 148;
+  double *in = nullptr, *layer64 = nullptr, *out = nullptr;
+  float *layer32 = nullptr, *periods = nullptr, *rows = nullptr;
+  int *mL = nullptr, *list = nullptr, *count = nullptr;
+  unsigned *flags = nullptr;
+  unsigned long long *stats = nullptr;
+  UniformBracket *br = nullptr;
+};
+
+namespace {
+
+UniformDev uniform_dev(const md200_uniform *u, const float *rows) {
+  UniformDev d{};
+  d.B = u->B;
+  d.Lmax = u->L;
+  d.Ls = u->L;
+  d.nf = u->nf;
+  d.nc = u->nc;
+  d.K = u->K;
+  const size_t n = static_cast<size_t>(u->B) * u->L;
+  d.h = u->in;
+  d.vp = u->in + n;
+  d.vs = u->in + 2 * n;
+  d.rho = u->in + 3 * n;
+  d.layer64 = u->layer64;
+  d.layer32 = u->layer32;
+  d.mL = u->mL;
+  d.periods = u->periods;
+  d.rows = rows;
+  d.out = u->out;
+  d.flags = u->flags;
+  d.stats = u->stats;
+  d.br = u->br;
+  d.list = u->list;
+  d.count = u->count;
+  return d;
+}
+
+void uniform_free_outputs(md200_uniform *u) {
+  cudaFree(u->rows);
+  cudaFree(u->out);
+  cudaFree(u->flags);
+  cudaFree(u->br);
+  cudaFree(u->list);
+  u->rows = nullptr;
+  u->out = nullptr;
+  u->flags = nullptr;
+  u->br = nullptr;
+  u->list = nullptr;
+  u->alloc_nf = u->alloc_nc = u->alloc_K = 0;
+}
+
+// cpp/cuda/refine.cuh:38-45: halvings for |c1 - c2| <= tol at the grid minimum
+int uniform_iters(double dc, double tol) {
+  if (!(tol > 0.0) || !(dc > tol)) return 1;
+  const int n = static_cast<int>(std::ceil(std::log2(dc / tol)));
+  return n < 1 ? 1 : (n > 60 ? 60 : n);
+}
+
+std::string num(int x) { return std::to_string(x); }
+
+int uniform_geometry(const md200_uniform *u, const char *who) {
+  if (u->nf != u->alloc_nf || u->nc != u->alloc_nc)
+    return fail(std::string(who) + ": geometry changed since allocation (allocated nf=" + num(u->alloc_nf) +
+                " nc=" + num(u->alloc_nc) + ", now nf=" + num(u->nf) + " nc=" + num(u->nc) +
+                "); call set_output() again");
+  return 0;
+}
+
+// persistent grid: `per_sm` blocks per SM at most, fewer when there is less work
+int uniform_blocks(const md200_uniform *u, long long units_per_block_work, long long work, int per_sm) {
+  const long long need = (work + units_per_block_work - 1) / units_per_block_work;
+  return static_cast<int>(std::max(1LL, std::min(need, static_cast<long long>(u->sms) * per_sm)));
+}
+
+}  // namespace
+
+extern "C" {
+
+md200_uniform *md200_uniform_create(int models, int layers) {
+  try {
+    if (models <= 0 || layers < 2) {
+      fail("md200_uniform_create: bad shape B=" + num(models) + " L=" + num(layers) +
+           " (L must be >= 2: layers plus half-space)");
+      return nullptr;
+    }
+    auto *u = new md200_uniform;
+    u->B = models;
+    u->L = layers;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&u->sms, cudaDevAttrMultiProcessorCount, dev);
+    const size_t n = static_cast<size_t>(models) * layers;
+    if (dalloc(&u->in, 4 * n) != cudaSuccess || dalloc(&u->layer64, ROWS * n) != cudaSuccess ||
+        dalloc(&u->layer32, ROWS * n) != cudaSuccess || dalloc(&u->mL, models) != cudaSuccess ||
+        dalloc(&u->stats, US_COUNT) != cudaSuccess || dalloc(&u->count, 1) != cudaSuccess) {
+      const cudaError_t e = cudaGetLastError();
+      md200_uniform_destroy(u);
+      fail(std::string("md200_uniform_create: cudaMalloc (model arrays): ") + cudaGetErrorString(e));
+      return nullptr;
+    }
+    return u;
+  } catch (...) {
+    fail_exception();
+    return nullptr;
+  }
+}
+
+void md200_uniform_destroy(md200_uniform *u) {
+  if (!u) return;
+  uniform_free_outputs(u);
+  cudaFree(u->in);
+  cudaFree(u->layer64);
+  cudaFree(u->layer32);
+  cudaFree(u->mL);
+  cudaFree(u->periods);
+  cudaFree(u->stats);
+  cudaFree(u->count);
+  delete u;
+}
+
+int md200_uniform_models(md200_uniform *u, const double *h, const double *vp, const double *vs,
+                         const double *rho) {
+  try {
+    if (!u || !h || !vp || !vs || !rho) return fail("md200_uniform_models: null argument");
+    const size_t n = static_cast<size_t>(u->B) * u->L;
+    const double *src[4] = {h, vp, vs, rho};
+    for (int i = 0; i < 4; ++i)
+      MD200_CK(cudaMemcpy(u->in + i * n, src[i], n * sizeof(double), cudaMemcpyHostToDevice));
+    uniform_prep<<<(u->B + 3) / 4, 128>>>(uniform_dev(u, nullptr));
+    MD200_CK(cudaGetLastError());
+    u->models = true;
+    return 0;
+  } catch (...) {
+    return fail_exception();
+  }
+}
+
+int md200_uniform_periods(md200_uniform *u, int periods, const double *values) {
+  try {
+    if (!u || !values) return fail("md200_uniform_periods: null argument");
+    if (periods <= 0) return fail("md200_uniform_periods: nf must be positive, got " + num(periods));
+    // a different period count invalidates outputs sized against the old one
+    if (periods != u->nf) uniform_free_outputs(u);
+    cudaFree(u->periods);
+    u->periods = nullptr;
+    MD200_CK(dalloc(&u->periods, periods));
+    std::vector<float> single(values, values + periods);  // the reference keeps periods in single precision
+    MD200_CK(cudaMemcpy(u->periods, single.data(), sizeof(float) * periods, cudaMemcpyHostToDevice));
+    u->nf = periods;
+    return 0;
+  } catch (...) {
+    return fail_exception();
+  }
+}
+
+int md200_uniform_grid(md200_uniform *u, int nc, int nmodes) {
+  try {
+    if (!u) return fail("md200_uniform_grid: null state");
+    if (nmodes < 0) return fail("md200_uniform_grid: nmodes must be >= 0, got " + num(nmodes));
+    if (nmodes == 0 && nc <= 0) return fail("md200_uniform_grid: nc must be positive, got " + num(nc));
+    if (nmodes > 0 && nc < 2)
+      return fail("md200_uniform_grid: need nc >= 2 and nmodes >= 1, got nc=" + num(nc) + " nmodes=" +
+                  num(nmodes));
+    if (u->nf <= 0)
+      return fail("md200_uniform_grid: upload_periods() first -- the output size depends on the period count");
+    const size_t rows = static_cast<size_t>(u->B) * u->nf;
+    if (nmodes > 0 && rows * nmodes >= (1ull << 31))
+      return fail("md200_uniform_grid: models x periods x modes must stay below 2^31");
+    uniform_free_outputs(u);
+    if (nmodes == 0) {
+      MD200_CK(dalloc(&u->rows, rows * nc));
+    } else {
+      MD200_CK(dalloc(&u->out, rows * nmodes));
+      MD200_CK(dalloc(&u->flags, rows));
+      MD200_CK(dalloc(&u->br, rows * nmodes));
+      MD200_CK(dalloc(&u->list, rows * nmodes));
+      u->K = u->alloc_K = nmodes;
+    }
+    u->nc = u->alloc_nc = nc;
+    u->alloc_nf = u->nf;
+    return 0;
+  } catch (...) {
+    return fail_exception();
+  }
+}
+
+int md200_uniform_scan(md200_uniform *u, double cmin, double cmax) {
+  try {
+    if (!u || !u->periods) return fail("md200_uniform_scan: periods not uploaded");
+    if (!u->rows) return fail("md200_uniform_scan: output not allocated");
+    if (!u->models) return fail("md200_uniform_scan: models not uploaded");
+    if (uniform_geometry(u, "md200_uniform_scan")) return 1;
+    const double dc = u->nc > 1 ? (cmax - cmin) / static_cast<double>(u->nc - 1) : 0.;
+    const long long warps = static_cast<long long>(u->B) * u->nf * ((u->nc + 31) / 32);
+    uniform_scan<<<uniform_blocks(u, 8, warps, 16), 256>>>(uniform_dev(u, nullptr), u->rows, cmin, dc);
+    MD200_CK(cudaGetLastError());
+    u->cmin = cmin;
+    u->cmax = cmax;
+    u->ran = true;
+    return 0;
+  } catch (...) {
+    return fail_exception();
+  }
+}
+
+int md200_uniform_rows(md200_uniform *u, float *rows) {
+  try {
+    if (!u || !rows) return fail("md200_uniform_rows: null argument");
+    if (!u->rows) return fail("md200_uniform_rows: output not allocated");
+    if (uniform_geometry(u, "md200_uniform_rows")) return 1;
+    MD200_CK(cudaMemcpy(rows, u->rows, sizeof(float) * u->B * static_cast<size_t>(u->nf) * u->nc,
+                        cudaMemcpyDeviceToHost));
+    return 0;
+  } catch (...) {
+    return fail_exception();
+  }
+}
+
+int md200_uniform_set_rows(md200_uniform *u, const float *rows, double cmin, double cmax) {
+  try {
+    if (!u || !rows) return fail("md200_uniform_set_rows: null argument");
+    if (!u->rows) return fail("md200_uniform_set_rows: output not allocated");
+    if (uniform_geometry(u, "md200_uniform_set_rows")) return 1;
+    MD200_CK(cudaMemcpy(u->rows, rows, sizeof(float) * u->B * static_cast<size_t>(u->nf) * u->nc,
+                        cudaMemcpyHostToDevice));
+    u->cmin = cmin;
+    u->cmax = cmax;
+    u->ran = true;
+    return 0;
+  } catch (...) {
+    return fail_exception();
+  }
+}
+
+int md200_uniform_refine(md200_uniform *u, const md200_uniform *scan, double cmin, double cmax, double c_tol_rel,
+                         double f_accept, int nmodes) {
+  try {
+    if (!u || !u->periods) return fail("md200_uniform_refine: periods not uploaded");
+    if (!u->out || !u->flags) return fail("md200_uniform_refine: output not allocated");
+    if (!u->models) return fail("md200_uniform_refine: models not uploaded");
+    if (!scan || !scan->rows) return fail("md200_uniform_refine: null scan buffer");
+    if (uniform_geometry(u, "md200_uniform_refine")) return 1;
+    if (nmodes > u->alloc_K)
+      return fail("md200_uniform_refine: nmodes=" + num(nmodes) + " exceeds the allocated " + num(u->alloc_K) +
+                  "; call set_output(nc, nmodes) to resize");
+    if (scan->B != u->B || scan->L != u->L || scan->nf != u->nf || scan->nc != u->nc)
+      return fail("md200_uniform_refine: scan and refine geometries differ");
+    if (!scan->ran) return fail("md200_uniform_refine: the scan has not been run");
+    if (scan->cmin != cmin || scan->cmax != cmax) return fail("md200_uniform_refine: scan and refine ranges differ");
+    if (nmodes > 0) u->K = nmodes;
+    const double dc = u->nc > 1 ? (cmax - cmin) / static_cast<double>(u->nc - 1) : 0.;
+    const int iters = uniform_iters(dc, c_tol_rel * cmin);
+    const size_t rows = static_cast<size_t>(u->B) * u->nf;
+    MD200_CK(cudaMemset(u->stats, 0, sizeof(unsigned long long) * US_COUNT));
+    MD200_CK(cudaMemset(u->flags, 0, sizeof(unsigned) * rows));
+    MD200_CK(cudaMemset(u->count, 0, sizeof(int)));
+    const UniformDev d = uniform_dev(u, scan->rows);
+    uniform_walk<<<uniform_blocks(u, 4, static_cast<long long>(rows), 16), 128>>>(d, cmin, dc);
+    MD200_CK(cudaGetLastError());
+    uniform_bisect<<<uniform_blocks(u, 128, static_cast<long long>(rows) * u->K, 8), 128>>>(d, cmin, dc, iters,
+                                                                                           f_accept);
+    MD200_CK(cudaGetLastError());
+    u->ran = true;
+    return 0;
+  } catch (...) {
+    return fail_exception();
+  }
+}
+
+int md200_uniform_sync(void) {
+  MD200_CK(cudaStreamSynchronize(nullptr));
+  return 0;
+}
+
+int md200_uniform_velocity(md200_uniform *u, double *velocity) {
+  try {
+    if (!u || !velocity) return fail("md200_uniform_velocity: null argument");
+    if (!u->out) return fail("md200_uniform_velocity: output not allocated");
+    if (uniform_geometry(u, "md200_uniform_velocity")) return 1;
+    MD200_CK(cudaMemcpy(velocity, u->out, sizeof(double) * u->B * static_cast<size_t>(u->nf) * u->K,
+                        cudaMemcpyDeviceToHost));
+    return 0;
+  } catch (...) {
+    return fail_exception();
+  }
+}
+
+int md200_uniform_flags(md200_uniform *u, uint32_t *flags) {
+  try {
+    if (!u || !flags) return fail("md200_uniform_flags: null argument");
+    if (!u->flags) return fail("md200_uniform_flags: no flags allocated -- call set_output() and run() first");
+    MD200_CK(cudaMemcpy(flags, u->flags, sizeof(uint32_t) * u->B * static_cast<size_t>(u->nf),
+                        cudaMemcpyDeviceToHost));
+    return 0;
+  } catch (...) {
+    return fail_exception();
+  }
+}
+
+int md200_uniform_stats(md200_uniform *u, uint64_t *stats, int n) {
+  try {
+    if (!u || !stats) return fail("md200_uniform_stats: null argument");
+    if (n < US_COUNT)
+      return fail("md200_uniform_stats: need room for " + num(US_COUNT) + " counters, got " + num(n));
+    unsigned long long h[US_COUNT];
+    MD200_CK(cudaMemcpy(h, u->stats, sizeof(h), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < US_COUNT; ++i) stats[i] = h[i];
+    return 0;
+  } catch (...) {
+    return fail_exception();
+  }
+}
+
+int md200_uniform_iterations(double dc, double c_tol_rel, double cmin) { return uniform_iters(dc, c_tol_rel * cmin); }
+
+int md200_uniform_kernel_report(int stage, int layers, int block, char *text, int length) {
+  try {
+    if (!text || length <= 0) return fail("md200_uniform_kernel_report: null buffer");
+    const void *fn = stage == 0 ? reinterpret_cast<const void *>(uniform_scan)
+                                : reinterpret_cast<const void *>(uniform_bisect);
+    const int threads = stage == 0 ? 256 : 128;
+    cudaFuncAttributes a{};
+    MD200_CK(cudaFuncGetAttributes(&a, fn));
+    int blocks = 0;
+    MD200_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, fn, threads, 0));
+    int dev = 0, per_sm = 2048;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxThreadsPerMultiProcessor, dev);
+    std::snprintf(text, length,
+                  "kernel=%s regs=%d spill_bytes=%d smem_static=%zu smem_dynamic=0 block=%d "
+                  "max_blocks_per_sm=%d threads_per_sm=%d occupancy=%.1f%% layers=%d requested_block=%d",
+                  stage == 0 ? "uniform_scan" : "uniform_bisect", a.numRegs, static_cast<int>(a.localSizeBytes),
+                  a.sharedSizeBytes, threads, blocks, blocks * threads, 100.0 * blocks * threads / per_sm, layers,
+                  block);
     return 0;
   } catch (...) {
     return fail_exception();

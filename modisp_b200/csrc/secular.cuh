@@ -704,10 +704,13 @@ MD200_FN void rayleigh_start(N e[5], const N &k, const N &k2, const N &w, const 
 // unnormalised vector: it is smooth across ordinary roots and dips
 // logarithmically where the whole vector nearly vanishes, the signature of a
 // close root pair.  With `levan`, the part of that logarithm the evanescent
-// scaling factored out (base 2 of exp(sum r h)).
+// scaling factored out (base 2 of exp(sum r h)).  With `fmax` (solid models),
+// F on the scale of a recurrence renormalised to max |e_i| = 1 after every
+// layer: F / max |e_i| of the final vector, |value| <= 1.
 template <class N, class T, int S>
 MD200_FN void rayleigh_multi(const LayerView<T> &m, const N *k, const N &w, N *F, N *shape,
-                             typename Base<N>::type *lmag, typename Base<N>::type *levan = nullptr) {
+                             typename Base<N>::type *lmag, typename Base<N>::type *levan = nullptr,
+                             typename Base<N>::type *fmax = nullptr) {
   using B = typename Base<N>::type;
   const B tiny = sizeof(B) == 4 ? B(1e-30) : B(1e-40);
   const N iw = lift_one<N>() / w;
@@ -775,6 +778,12 @@ MD200_FN void rayleigh_multi(const LayerView<T> &m, const N *k, const N &w, N *F
                       e[s][4] * e[s][4];
       if (shape) shape[s] = e[s][0] * m_rsqrt(norm2 + lift_one<N>() * tiny);
       if (lmag) lmag[s] += B(0.5) * m_log2(val(norm2) + tiny);
+      if (fmax) {
+        B big = B(0);
+#pragma unroll
+        for (int i = 0; i < 5; ++i) big = m_max(big, m_abs(val(e[s][i])));
+        fmax[s] = big > B(0) ? val(e[s][0]) / big : val(e[s][0]);
+      }
       F[s] = e[s][0];
     }
   }

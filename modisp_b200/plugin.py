@@ -5,7 +5,10 @@ modisp selects a GPU backend by importing ``modisp_cuda`` and calling its
 This module is that extension's interface, implemented over the engine's C ABI:
 the same constants, module functions and ``QeSolver`` class with the same
 argument meaning, return layout and error behaviour
-(cpp/cuda/qe.cu:1124-1170, cpp/common/review_groups.hpp:39-63).  The package
+(cpp/cuda/qe.cu:1124-1170, cpp/common/review_groups.hpp:39-63), and the legacy
+uniform path's stage classes ``CoarseScan`` and ``Refine`` with ``STAT_NAMES``
+(cpp/cuda/bindings.cpp:121-406) that modisp's ``search_strategy="uniform"``
+drives (python/modisp/_legacy.py:300-340).  The package
 ``modisp_cuda`` at the repository root re-exports it, so an unmodified modisp
 picks the engine with ``Solver(backend="cuda")``.
 
@@ -230,6 +233,156 @@ class QeSolver:
             self.close()
         except Exception:
             pass
+
+
+# Counter names of the legacy uniform path's Refine.stats(), in order
+# (cpp/cuda/bindings.cpp:58-59, exported as the module's STAT_NAMES at :348-351).
+STAT_NAMES = _native.UNIFORM_STAT_NAMES
+
+
+def _as_2d(obj, rows, cols, name):
+    """Contiguous float64 [rows, cols] (cpp/cuda/bindings.cpp:79-93: TypeError when
+    not array-like, ValueError on a shape mismatch)."""
+    try:
+        a = np.ascontiguousarray(obj, dtype=np.float64)
+    except (TypeError, ValueError) as exc:
+        raise TypeError(f"{name} must be an array-like of real numbers") from exc
+    if a.ndim != 2 or a.shape != (rows, cols):
+        raise ValueError(f"{name} must have shape ({rows}, {cols}), got {a.shape}")
+    return a
+
+
+def _as_periods(periods):
+    try:
+        p = np.ascontiguousarray(periods, dtype=np.float64)
+    except (TypeError, ValueError):
+        p = None
+    if p is None or p.ndim != 1 or p.size == 0:
+        raise ValueError("periods must be a non-empty 1-D array")
+    return p
+
+
+class _UniformStage:
+    """State shared by the legacy path's two stage objects: B models of L rows,
+    the uploaded periods and the allocated grid."""
+
+    def __init__(self, B, L):
+        self._u = _native.Uniform(int(B), int(L))
+        self.B, self.L = int(B), int(L)
+        self.nf = self.nc = 0
+        self._uploaded = False
+
+    def upload_models(self, thickness, vp, vs, rho):
+        arrays = [_as_2d(x, self.B, self.L, n) for x, n in ((thickness, "thickness"), (vp, "vp"), (vs, "vs"),
+                                                           (rho, "rho"))]
+        self._u.models(*arrays)
+        self._uploaded = True
+
+    def upload_periods(self, periods):
+        p = _as_periods(periods)
+        self._u.periods(p)
+        if p.size != self.nf:
+            self.nc = 0  # outputs sized for another period count are dropped
+            if hasattr(self, "nmodes"):
+                self.nmodes = 0
+        self.nf = int(p.size)
+
+    def sync(self):
+        _native.Uniform.sync()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        return None
+
+    def close(self):
+        self._u.close()
+
+
+class CoarseScan(_UniformStage):
+    """Stage 1 of the legacy uniform path: FP32 secular values over a (period,
+    velocity) grid (cpp/cuda/bindings.cpp:121-196, cpp/cuda/coarse_scan.cu)."""
+
+    def __init__(self, B, L):
+        super().__init__(B, L)
+        self._range = None
+
+    def allocate(self, nc):
+        self._u.grid(int(nc), 0)
+        self.nc = int(nc)
+
+    def run(self, cmin, cmax, block=256, sync=False):
+        del block  # the kernel's block shape is fixed; results do not depend on it
+        if not self._uploaded:
+            raise RuntimeError("upload_models() first")
+        self._u.scan(cmin, cmax)
+        self._range = (float(cmin), float(cmax))
+        if sync:
+            self.sync()
+
+    def download(self):
+        if not self.nc:
+            raise RuntimeError("allocate() first")
+        return self._u.rows(self.nf, self.nc)
+
+    def scan(self, cmin, cmax, block=256):
+        self.run(cmin, cmax, block, True)
+        return self.download()
+
+    def kernel_report(self, block=256):
+        return _native.Uniform.kernel_report(0, self.L, block)
+
+
+class Refine(_UniformStage):
+    """Stages 2-3 of the legacy uniform path: roots located from a CoarseScan's
+    values and bisected in FP64 (cpp/cuda/bindings.cpp:200-345, cpp/cuda/refine.cu)."""
+
+    def __init__(self, B, L):
+        super().__init__(B, L)
+        self.nmodes = 0
+
+    def allocate(self, nc, nmodes):
+        self._u.grid(int(nc), int(nmodes))
+        self.nc, self.nmodes = int(nc), int(nmodes)
+
+    def run(self, scan, cmin, cmax, c_tol_rel=1e-6, f_accept=1.0, nmodes=0, block=256, sync=True):
+        del block
+        if not self.nf:
+            raise RuntimeError("upload_periods() first")
+        if not self.nmodes:
+            raise RuntimeError("allocate() first")
+        if (scan.B, scan.L, scan.nf, scan.nc) != (self.B, self.L, self.nf, self.nc):
+            raise ValueError(f"scan and refine geometries differ: scan has B={scan.B} L={scan.L} nf={scan.nf} "
+                             f"nc={scan.nc}, refine has B={self.B} L={self.L} nf={self.nf} nc={self.nc}")
+        if scan._range is None:
+            raise ValueError("this scan has not been run, so its rows hold nothing to refine; call run() on it "
+                             "first")
+        if scan._range != (float(cmin), float(cmax)):
+            raise ValueError(f"scan and refine ranges differ: the scan ran over {scan._range}, the refinement was "
+                             f"given ({float(cmin)}, {float(cmax)}); the range sets the grid spacing, so every "
+                             "grid point would move")
+        self._u.refine(scan._u, cmin, cmax, c_tol_rel, f_accept, nmodes)
+        if int(nmodes) > 0:
+            self.nmodes = int(nmodes)
+        if sync:
+            self.sync()
+
+    def download(self):
+        if not self.nmodes:
+            raise RuntimeError("allocate() first")
+        return self._u.velocity(self.nmodes, self.nf)
+
+    def stats(self):
+        return self._u.stats()
+
+    def flags(self):
+        if not self.nf or not self.nmodes:
+            raise RuntimeError("allocate() first")
+        return self._u.flags(self.nf)
+
+    def kernel_report(self, block=256):
+        return _native.Uniform.kernel_report(1, self.L, block)
 
 
 _current_device = 0

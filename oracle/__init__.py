@@ -67,6 +67,9 @@ def lib():
         L.mdo_group.argtypes = [P, P, P, P, i, i, d, d, d, d, P]
         L.mdo_parameter_derivatives.restype = None
         L.mdo_parameter_derivatives.argtypes = [P, P, P, P, i, i, d, d, P, P]
+        L.mdo_uniform_refine.restype = None
+        V = ctypes.c_void_p
+        L.mdo_uniform_refine.argtypes = [V, i, P, P, P, P, i, ctypes.c_float, i, d, d, d, d, P, V, V]
         _LIB = L
     return _LIB
 
@@ -300,3 +303,29 @@ def reference_solve(h, vp, vs, rho, periods, nmodes, wave=0, tol=1e-12, threads=
     return dict(phase_velocity=velocity, trace_flags=flags, stats=stats, search_level=levels,
                 root_count=counts, group_velocity=extras["group_velocity"],
                 group_velocity_flags=extras["group_velocity_flags"], search_bounds=bnd)
+
+
+def uniform_refine(rows, h, vp, vs, rho, periods, nmodes, cmin, cmax, c_tol_rel=1e-6, f_accept=1.0):
+    """Stage 2 of the legacy uniform path (cpp/cuda/refine.cuh:131-317) on given
+    stage 1 values ``rows`` [B, T, nc] (float32): velocity [B, nmodes, T], trace
+    flags [B, T] and the six counters, computed trace by trace on the CPU."""
+    rows = np.ascontiguousarray(rows, dtype=np.float32)
+    h, vp, vs, rho = (np.atleast_2d(np.ascontiguousarray(x, dtype=np.float64)) for x in (h, vp, vs, rho))
+    B, T, nc = rows.shape
+    per = np.asarray(periods, dtype=np.float32)
+    out = np.full((B, nmodes, T), np.nan)
+    flags = np.zeros((B, T), np.uint32)
+    stats = np.zeros(6, np.uint64)
+    o = np.empty(nmodes)
+    fl = np.zeros(1, np.uint32)
+    for b in range(B):
+        row_args = [np.ascontiguousarray(x[b]) for x in (h, vp, vs, rho)]
+        for t in range(T):
+            fl[0] = 0
+            lib().mdo_uniform_refine(rows[b, t].ctypes.data, nc, *(_ptr(x) for x in row_args), h.shape[1],
+                                     float(per[t]), int(nmodes), float(cmin), float(cmax), float(c_tol_rel),
+                                     float(f_accept), _ptr(o), fl.ctypes.data, stats.ctypes.data)
+            out[b, :, t] = o
+            flags[b, t] = fl[0]
+    names = ("brackets", "rejected_sign", "rejected_f", "troughs", "hidden_roots", "relocated")
+    return out, flags, {k: int(v) for k, v in zip(names, stats)}

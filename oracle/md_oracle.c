@@ -748,3 +748,153 @@ void mdo_parameter_derivatives(const double *h, const double *vp, const double *
   *dfdc = (double)(cimagl(cx_eval(&m, kc, w)) / STEP);
   free(m.h);
 }
+
+/* ------------------------------------------------------------------------- */
+/* Legacy uniform-grid path, stage 2 (cpp/cuda/refine.cuh:131-317): one mode */
+/* at a time, each walking the row from the start as the reference's thread  */
+/* for that mode does; FP64 values from mdo_rayleigh (the normalised Dunkin   */
+/* recurrence, dunkin_secular_omega<double, true>).                          */
+/* ------------------------------------------------------------------------- */
+static double uni_c(double cmin, double dc, int i) { return fma(dc, (double)i, cmin); } /* refine.cuh:33-35 */
+
+typedef struct {
+  const double *h, *vp, *vs, *rho;
+  int L;
+  double omega;
+} UniModel;
+
+static double uni_f(const UniModel *m, double c) { return mdo_rayleigh(m->h, m->vp, m->vs, m->rho, m->L, m->omega, c, NULL); }
+
+/* refine.cuh:63-80 */
+static int uni_retry(const UniModel *m, int cell, int dir, int i_last, double cmin, double dc, double *lo,
+                     double *hi, double *flo) {
+  const int c2 = cell + dir;
+  if (c2 < 0 || c2 > i_last) return 0;
+  const double a = uni_c(cmin, dc, c2), b = uni_c(cmin, dc, c2 + 1);
+  const double fa = uni_f(m, a), fb = uni_f(m, b);
+  if ((fa < 0.0) == (fb < 0.0)) return 0;
+  *lo = a;
+  *hi = b;
+  *flo = fa;
+  return 1;
+}
+
+/* refine.cuh:83-116 */
+static double uni_bisect(const UniModel *m, double lo, double hi, double flo, int iters, double f_accept,
+                         unsigned long long *stats) {
+  for (int k = 0; k < iters; ++k) {
+    const double mid = 0.5 * (lo + hi);
+    const double fm = uni_f(m, mid);
+    if ((fm < 0.0) == (flo < 0.0)) {
+      lo = mid;
+      flo = fm;
+    } else {
+      hi = mid;
+    }
+  }
+  const double root = 0.5 * (lo + hi);
+  if (f_accept < 1.0 && fabs(uni_f(m, root)) > f_accept) {
+    ++stats[2];
+    return NAN;
+  }
+  return root;
+}
+
+void mdo_uniform_refine(const float *row, int nc, const double *h, const double *vp, const double *vs,
+                        const double *rho, int L, float period, int nmodes, double cmin, double cmax,
+                        double c_tol_rel, double f_accept, double *out, unsigned *flags,
+                        unsigned long long *stats) {
+  const double dc = nc > 1 ? (cmax - cmin) / (double)(nc - 1) : 0.0;
+  const double tol = c_tol_rel * cmin;
+  int iters = 1; /* refine.cuh:38-45 */
+  if (tol > 0.0 && dc > tol) {
+    iters = (int)ceil(log2(dc / tol));
+    if (iters < 1) iters = 1;
+    if (iters > 60) iters = 60;
+  }
+  UniModel m = {h, vp, vs, rho, L, MDO_TWO_PI / (double)period};
+  const double c_cap = vs[L - 1];
+  int i_last = (int)((c_cap - cmin) / dc); /* scan_grid.hpp:19-24 */
+  if (i_last > nc - 2) i_last = nc - 2;
+  for (int target = 0; target < nmodes; ++target) {
+    out[target] = NAN;
+    int mode = 0, cell = -1, have_hidden = 0, n_point = 0;
+    double h_lo = 0., h_hi = 0., h_flo = 0.;
+    for (int i = 0; i + 1 < nc && i <= i_last && cell < 0 && !have_hidden;) {
+      if ((row[i] < 0.0f) != (row[i + 1] < 0.0f)) {
+        if (mode == target) {
+          cell = i;
+          break;
+        }
+        ++mode;
+        ++i;
+        continue;
+      }
+      const int tc = i + 1;
+      int wlo = -1, whi = -1;
+      if (tc >= 1 && tc + 1 < nc && tc <= i_last) {
+        const float am = fabsf(row[tc - 1]), bm = fabsf(row[tc]), cm = fabsf(row[tc + 1]);
+        const int no_sc_right = (row[tc] < 0.0f) == (row[tc + 1] < 0.0f);
+        if (no_sc_right && am > bm && bm < cm && bm < 0.05f) {
+          wlo = tc - 1;
+          whi = tc + 1;
+          ++n_point;
+        }
+      }
+      if (wlo < 0) {
+        ++i;
+        continue;
+      }
+      const double c_a = uni_c(cmin, dc, wlo), c_b = uni_c(cmin, dc, whi), span = c_b - c_a;
+      double prev_c = c_a, prev_f = uni_f(&m, c_a);
+      for (int j = 1; j <= 65; ++j) {
+        const double cj = c_a + span * (double)j / 65.0;
+        const double fj = uni_f(&m, cj);
+        if ((prev_f < 0.0) != (fj < 0.0)) {
+          if (mode == target) {
+            h_lo = prev_c;
+            h_hi = cj;
+            h_flo = prev_f;
+            have_hidden = 1;
+            break;
+          }
+          ++mode;
+        }
+        prev_c = cj;
+        prev_f = fj;
+      }
+      i = whi;
+    }
+    stats[3] += (unsigned long long)n_point;
+    double root = NAN;
+    if (cell >= 0) {
+      ++stats[0];
+      const double lo = uni_c(cmin, dc, cell), hi = uni_c(cmin, dc, cell + 1);
+      const double flo = uni_f(&m, lo), fhi = uni_f(&m, hi);
+      if ((flo < 0.0) == (fhi < 0.0)) {
+        ++stats[1];
+        const int cl = cell - 1, cr = cell + 1;
+        const int cand_l = cl >= 0 && ((row[cl] < 0.0f) == (row[cl + 1] < 0.0f));
+        const int cand_r = cr + 1 < nc && cr <= i_last && ((row[cr] < 0.0f) == (row[cr + 1] < 0.0f));
+        double llo = 0., lhi = 0., lflo = 0., rlo = 0., rhi = 0., rflo = 0.;
+        const int left = cand_l && uni_retry(&m, cell, -1, i_last, cmin, dc, &llo, &lhi, &lflo);
+        const int right = cand_r && uni_retry(&m, cell, +1, i_last, cmin, dc, &rlo, &rhi, &rflo);
+        if (left != right) {
+          ++stats[5];
+          *flags |= 2u;
+          root = left ? uni_bisect(&m, llo, lhi, lflo, iters, f_accept, stats)
+                      : uni_bisect(&m, rlo, rhi, rflo, iters, f_accept, stats);
+        } else {
+          *flags |= 1u;
+        }
+      } else {
+        root = uni_bisect(&m, lo, hi, flo, iters, f_accept, stats);
+      }
+    } else if (have_hidden) {
+      ++stats[4];
+      root = uni_bisect(&m, h_lo, h_hi, h_flo, iters, f_accept, stats);
+    }
+    if (root == root && root >= c_cap) root = NAN;
+    out[target] = root;
+  }
+}

@@ -73,6 +73,19 @@ void mdo_parameter_derivatives(const double *h, const double *vp, const double *
                                const double *rho, int L, int wave, double omega, double c,
                                double *dfdtheta, double *dfdc);
 
+/* Stage 2 of the legacy uniform-grid path for one (model, period) trace
+ * (cpp/cuda/refine.cuh:131-317 and :33-116, cpp/cuda/refine.cu:233): each mode
+ * m < nmodes walks the row of single-precision values `row` [nc] from the
+ * start, as the reference's thread for mode m does, then confirms, relocates and
+ * bisects its bracket in FP64.  `period` is the single-precision period the
+ * reference stores.  Writes out[nmodes] (NaN where absent), ORs the trace flags
+ * (1 unresolved, 2 relocated) into *flags and adds the six counters (brackets,
+ * rejected_sign, rejected_f, troughs, hidden_roots, relocated) to stats. */
+void mdo_uniform_refine(const float *row, int nc, const double *h, const double *vp, const double *vs,
+                        const double *rho, int L, float period, int nmodes, double cmin, double cmax,
+                        double c_tol_rel, double f_accept, double *out, unsigned *flags,
+                        unsigned long long *stats);
+
 #ifdef __cplusplus
 }
 #endif

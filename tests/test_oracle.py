@@ -274,3 +274,19 @@ def test_jacobian_fixtures_agree_with_the_oracle(name, oracle_lib):
                 worst = max(worst, np.abs(jac - g["jac_phase_fd"][b, m, f]).max() / np.abs(jac).max())
                 checked += 1
     assert checked > 50 and worst < 1e-6
+
+
+@pytest.mark.parametrize("case", ["crustal12", "lvz12", "lowc6", "deep4"])
+def test_uniform_stage2_restatement_is_the_reference(case, oracle_lib):
+    """mdo_uniform_refine on the reference's own stage 1 values (the fixtures of
+    tests/golden/make_uniform_golden.py, made by the reference's CUDA legacy path)
+    returns its roots bit for bit, its trace flags and its six counters."""
+    g = load_golden(f"uniform_{case}")
+    model = [g[k] for k in ("thickness", "vp", "vs", "rho")]
+    v, flags, stats = oracle_lib.uniform_refine(g["rows"], *model, g["periods"], int(g["nmodes"]), float(g["cmin"]),
+                                                float(g["cmax"]), float(g["c_tol_rel"]), float(g["f_accept"]))
+    ref = g["phase_velocity"]
+    np.testing.assert_array_equal(np.isfinite(v), np.isfinite(ref))
+    np.testing.assert_array_equal(v[np.isfinite(ref)], ref[np.isfinite(ref)])
+    np.testing.assert_array_equal(flags, g["trace_flags"])
+    assert stats == {str(k): int(x) for k, x in zip(g["stat_names"], g["stats"])}
