@@ -826,7 +826,7 @@ MD200_FN void love_multi(const LayerView<T> &m, const N *k, const N &w, N *F, N 
     ex[s] = 0;
     ev[s] = B(0);
   }
-  for (int j = last - 1; j >= m.water; --j) {
+  auto layer = [&](int j) {
     const T h = m.h(j), mu = m.rho(j) * m.vs2(j), imu = m.imu(j), ivs = m.ivs(j);
 #pragma unroll
     for (int s = 0; s < S; ++s) {
@@ -855,6 +855,15 @@ MD200_FN void love_multi(const LayerView<T> &m, const N *k, const N &w, N *F, N 
       e[s][1] = v;
       ex[s] += scale_vector(e[s], 2, tiny);
     }
+  };
+  if constexpr (sizeof(N) == sizeof(float)) {
+    // two layers per iteration: the next layer's special functions overlap this
+    // one's recurrence (measured 5 % faster for the FP32 Love scan, 9 % slower
+    // for the FP64 one, whose longer body already fills the pipes)
+#pragma unroll 2
+    for (int j = last - 1; j >= m.water; --j) layer(j);
+  } else {
+    for (int j = last - 1; j >= m.water; --j) layer(j);
   }
 #pragma unroll
   for (int s = 0; s < S; ++s) {
