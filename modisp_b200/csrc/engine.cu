@@ -129,8 +129,12 @@ struct md200_engine {
   long long *rg_outbase = nullptr;
   double *rg_periods = nullptr;
   std::vector<void *> owned;
-  // host-path pipelining: one event per chunk of models
+  // host-path pipelining: chunks of models solved on `stream`, each chunk's outputs
+  // copied back on `copy_stream` once its solve has ended (solved_ev) while the next
+  // chunk is solved; chunk_ev marks the end of a chunk's copies
   static constexpr int MAX_CHUNKS = 8;
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t solved_ev[MAX_CHUNKS] = {};
   cudaEvent_t chunk_ev[MAX_CHUNKS] = {};
   // per-stage timing (cudaEvent pairs on the run's stream)
   static constexpr int NSTAGE = 10;
@@ -162,6 +166,7 @@ void release(md200_engine *e) {
   cudaGetDevice(&prev);
   cudaSetDevice(e->device);
   if (e->stream) cudaStreamSynchronize(e->stream);
+  if (e->copy_stream) cudaStreamSynchronize(e->copy_stream);
   for (void *p : e->owned) cudaFree(p);
   e->owned.clear();
   if (e->pinned) cudaFreeHost(e->pinned);
@@ -169,11 +174,14 @@ void release(md200_engine *e) {
     if (x) cudaEventDestroy(x);
   for (auto &x : e->chunk_ev)
     if (x) cudaEventDestroy(x);
+  for (auto &x : e->solved_ev)
+    if (x) cudaEventDestroy(x);
   for (auto &x : e->sp_ev)
     if (x) cudaEventDestroy(x);
   if (e->graph_exec) cudaGraphExecDestroy(e->graph_exec);
   if (e->graph) cudaGraphDestroy(e->graph);
   if (e->stream) cudaStreamDestroy(e->stream);
+  if (e->copy_stream) cudaStreamDestroy(e->copy_stream);
   cudaSetDevice(prev);
 }
 
@@ -185,6 +193,7 @@ size_t scan_smem(int warps, int Ls, size_t elem) {
 int setup(md200_engine *e) {
   MD200_CK(cudaSetDevice(e->device));
   MD200_CK(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+  MD200_CK(cudaStreamCreateWithFlags(&e->copy_stream, cudaStreamNonBlocking));
   const int B = e->cap, L = e->L, T = e->T, nm = e->nmodes;
   Dev &d = e->d;
   d.Lmax = L;
@@ -289,6 +298,7 @@ int setup(md200_engine *e) {
   e->prep_smem = static_cast<size_t>(e->prep_warps) * cap2 * (sizeof(double) + sizeof(int));
   for (auto &x : e->ev) MD200_CK(cudaEventCreate(&x));
   for (auto &x : e->chunk_ev) MD200_CK(cudaEventCreateWithFlags(&x, cudaEventDisableTiming));
+  for (auto &x : e->solved_ev) MD200_CK(cudaEventCreateWithFlags(&x, cudaEventDisableTiming));
   if (d.fp32)
     for (auto &x : e->sp_ev) MD200_CK(cudaEventCreate(&x));
   MD200_CK(cudaFuncSetAttribute(prep_models, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -743,6 +753,8 @@ int md200_run(md200_engine *e, const double *h, const double *vp, const double *
     if (e->d.group && (!group || !group_flags))
       return fail("modisp_b200: group-velocity engine needs group output arrays");
     MD200_CK(cudaSetDevice(e->device));
+    // copies left in flight by a call that failed part-way write the staging buffer
+    MD200_CK(cudaStreamSynchronize(e->copy_stream));
     const size_t B = models, L = e->L, T = e->T, nm = e->nmodes, nt = B * T;
     // stage inputs through pinned memory
     unsigned char *p = e->pinned;
@@ -796,26 +808,30 @@ int md200_run(md200_engine *e, const double *h, const double *vp, const double *
                   prediction_flags ? e->out_pred + ct : nullptr, continuity_flags ? e->out_cflags + ct : nullptr,
                   e->in_bounds + 2 * b0, cstats, s))
         return 1;
-      MD200_CK(cudaMemcpyAsync(ov + cm, e->out_vel + cm, sizeof(double) * cells, cudaMemcpyDeviceToHost, s));
-      MD200_CK(cudaMemcpyAsync(ofl + ct, e->out_flags + ct, sizeof(unsigned) * traces, cudaMemcpyDeviceToHost, s));
-      MD200_CK(cudaMemcpyAsync(olv + ct, e->out_levels + ct, sizeof(int) * traces, cudaMemcpyDeviceToHost, s));
-      MD200_CK(cudaMemcpyAsync(oct + ct, e->out_counts + ct, sizeof(int) * traces, cudaMemcpyDeviceToHost, s));
+      // this chunk's copies wait for its solve only; the next chunk is solved meanwhile
+      cudaStream_t cs = e->copy_stream;
+      MD200_CK(cudaEventRecord(e->solved_ev[c], s));
+      MD200_CK(cudaStreamWaitEvent(cs, e->solved_ev[c], 0));
+      MD200_CK(cudaMemcpyAsync(ov + cm, e->out_vel + cm, sizeof(double) * cells, cudaMemcpyDeviceToHost, cs));
+      MD200_CK(cudaMemcpyAsync(ofl + ct, e->out_flags + ct, sizeof(unsigned) * traces, cudaMemcpyDeviceToHost, cs));
+      MD200_CK(cudaMemcpyAsync(olv + ct, e->out_levels + ct, sizeof(int) * traces, cudaMemcpyDeviceToHost, cs));
+      MD200_CK(cudaMemcpyAsync(oct + ct, e->out_counts + ct, sizeof(int) * traces, cudaMemcpyDeviceToHost, cs));
       if (grp) {
-        MD200_CK(cudaMemcpyAsync(og + cm, e->out_grp + cm, sizeof(double) * cells, cudaMemcpyDeviceToHost, s));
-        MD200_CK(cudaMemcpyAsync(ogf + cm, e->out_gflags + cm, sizeof(unsigned) * cells, cudaMemcpyDeviceToHost, s));
+        MD200_CK(cudaMemcpyAsync(og + cm, e->out_grp + cm, sizeof(double) * cells, cudaMemcpyDeviceToHost, cs));
+        MD200_CK(cudaMemcpyAsync(ogf + cm, e->out_gflags + cm, sizeof(unsigned) * cells, cudaMemcpyDeviceToHost, cs));
       }
       if (prediction_flags)
-        MD200_CK(cudaMemcpyAsync(opr + ct, e->out_pred + ct, sizeof(unsigned) * traces, cudaMemcpyDeviceToHost, s));
+        MD200_CK(cudaMemcpyAsync(opr + ct, e->out_pred + ct, sizeof(unsigned) * traces, cudaMemcpyDeviceToHost, cs));
       if (continuity_flags)
-        MD200_CK(cudaMemcpyAsync(ocf + ct, e->out_cflags + ct, traces, cudaMemcpyDeviceToHost, s));
+        MD200_CK(cudaMemcpyAsync(ocf + ct, e->out_cflags + ct, traces, cudaMemcpyDeviceToHost, cs));
       // the prep stage wrote the windows it used over the (already consumed) input windows
       if (bounds_out)
         MD200_CK(cudaMemcpyAsync(obd + 2 * b0, e->in_bounds + 2 * b0, sizeof(double) * 2 * nb,
-                                 cudaMemcpyDeviceToHost, s));
-      MD200_CK(cudaEventRecord(e->chunk_ev[c], s));
+                                 cudaMemcpyDeviceToHost, cs));
+      MD200_CK(cudaEventRecord(e->chunk_ev[c], cs));
     }
     MD200_CK(cudaMemcpyAsync(ost, e->d_stats, sizeof(unsigned long long) * MD200_STAT_COUNT * nchunk,
-                             cudaMemcpyDeviceToHost, s));
+                             cudaMemcpyDeviceToHost, e->copy_stream));
     for (int c = 0; c < nchunk; ++c) {
       MD200_CK(cudaEventSynchronize(e->chunk_ev[c]));
       const size_t b0 = chunk_begin(c), nb = chunk_begin(c + 1) - b0;
@@ -834,6 +850,7 @@ int md200_run(md200_engine *e, const double *h, const double *vp, const double *
       parallel_copy(out);
     }
     MD200_CK(cudaStreamSynchronize(s));
+    MD200_CK(cudaStreamSynchronize(e->copy_stream));
     if (stats && nstats > 0) {
       const int n = std::min(nstats, int(MD200_STAT_COUNT));
       for (int i = 0; i < n; ++i) {
