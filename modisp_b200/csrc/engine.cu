@@ -59,18 +59,19 @@ int fail_exception() {
   } while (0)
 
 // Host copies between pinned staging and the caller's arrays, spread over up to
-// 8 threads: the caller's output arrays are usually fresh (first-touch page
-// faults) and a single core copies them at a fraction of the memory bandwidth.
+// `max_threads` threads (8 while the GPU still works, more when nothing else is
+// left): the caller's output arrays are usually fresh (first-touch page faults)
+// and a single core copies them at a fraction of the memory bandwidth.
 struct HostCopy {
   void *dst;
   const void *src;
   size_t bytes;
 };
-void parallel_copy(const std::vector<HostCopy> &jobs) {
+void parallel_copy(const std::vector<HostCopy> &jobs, unsigned max_threads = 8) {
   size_t total = 0;
   for (const HostCopy &j : jobs) total += j.bytes;
   const unsigned hw = std::thread::hardware_concurrency();
-  const unsigned nth = static_cast<unsigned>(std::min<size_t>(std::min(8u, hw ? hw : 1u), total >> 21));
+  const unsigned nth = static_cast<unsigned>(std::min<size_t>(std::min(max_threads, hw ? hw : 1u), total >> 21));
   auto part = [&](size_t lo, size_t hi) {  // byte range [lo, hi) of the jobs laid end to end
     size_t off = 0;
     for (const HostCopy &j : jobs) {
@@ -796,7 +797,12 @@ int md200_run(md200_engine *e, const double *h, const double *vp, const double *
         (reinterpret_cast<uintptr_t>(opr + nt) + 7) & ~uintptr_t(7));
     double *obd = reinterpret_cast<double *>(ost + static_cast<size_t>(MD200_STAT_COUNT) * md200_engine::MAX_CHUNKS);
     unsigned char *ocf = reinterpret_cast<unsigned char *>(obd + 2 * B);
-    auto chunk_begin = [&](int c) { return B * c / nchunk; };
+    // decreasing chunk sizes: the last chunk's copies are the only ones nothing
+    // overlaps, so it is the smallest (the tenth of the batch)
+    static const double edge[5] = {0., .4, .7, .9, 1.};
+    auto chunk_begin = [&](int c) -> size_t {
+      return nchunk == 1 ? B * c : (c >= nchunk ? B : static_cast<size_t>(B * edge[c]));
+    };
     for (int c = 0; c < nchunk; ++c) {
       const size_t b0 = chunk_begin(c), nb = chunk_begin(c + 1) - b0;
       const size_t cm = b0 * nm * T, ct = b0 * T, cells = nb * nm * T, traces = nb * T;
@@ -847,7 +853,7 @@ int md200_run(md200_engine *e, const double *h, const double *vp, const double *
       if (prediction_flags) out.push_back({prediction_flags + ct, opr + ct, sizeof(unsigned) * traces});
       if (continuity_flags) out.push_back({continuity_flags + ct, ocf + ct, traces});
       if (bounds_out) out.push_back({bounds_out + 2 * b0, obd + 2 * b0, sizeof(double) * 2 * nb});
-      parallel_copy(out);
+      parallel_copy(out, c + 1 == nchunk ? 16u : 8u);  // nothing left to overlap the last
     }
     MD200_CK(cudaStreamSynchronize(s));
     MD200_CK(cudaStreamSynchronize(e->copy_stream));
