@@ -92,6 +92,45 @@ def test_solver_validation_matches_reference_rules():
         _models(np.ones(300), np.full(300, 5.), np.full(300, 3.), np.ones(300))
 
 
+def test_uniform_strategy_options_follow_the_reference_rules():
+    """search_strategy="uniform" takes the reference's constructor rules
+    (python/modisp/__init__.py:194-217): legacy refinement and the dunkin secular
+    only, no group velocity or continuation, no FP32 output, no accuracy preset;
+    its accuracy label is "uniform" and its tolerances the uniform defaults."""
+    import modisp_b200 as md
+    s = md.Solver(search_strategy="uniform")
+    assert (s.accuracy, s.refinement, s.c_tol_rel, s.sampling_rtol) == ("uniform", "legacy", 1e-6, 1e-3)
+    assert md.Solver(search_strategy="uniform", accuracy="auto").accuracy == "uniform"
+    for kwargs, err in ((dict(group_velocity=True), NotImplementedError),
+                        (dict(frequency_strategy="anchor_continuation"), NotImplementedError),
+                        (dict(refinement="brent"), NotImplementedError),
+                        (dict(secular="fast"), NotImplementedError),
+                        (dict(precision="float32"), ValueError),
+                        (dict(accuracy="high"), ValueError),
+                        (dict(adaptive_period_threshold=1.), ValueError)):
+        with pytest.raises(err):
+            md.Solver(search_strategy="uniform", **kwargs)
+    from modisp_b200 import legacy
+    with pytest.raises(ValueError, match="nc must be at least 3"):
+        legacy.UniformSolver(nc=2)
+    with pytest.raises(ValueError, match="cmin must be positive"):
+        legacy.UniformSolver(cmin=0.)
+    # input checks of the legacy solver (python/modisp/_legacy.py:224-290), before any device work
+    u = legacy.UniformSolver()
+    h, vp, vs, rho = [1., 0.], [3., 5.], [1.5, 2.8], [2., 2.5]
+    for args, match in ((([1., 0.], [1.4, 5.], vs, rho), "vp must exceed vs"),
+                        (([-1., 0.], vp, vs, rho), "non-negative"),
+                        ((h, vp, [0., 2.8], rho), "vs must be positive"),
+                        ((h, vp, vs, [2., np.nan]), "rho must be finite"),
+                        (([1.], [3.], [1.5], [2.]), "at least 2 layers")):
+        with pytest.raises(ValueError, match=match):
+            u(*args, [1.])
+    with pytest.raises(ValueError, match="periods must be positive"):
+        u(h, vp, vs, rho, [0.])
+    with pytest.raises(ValueError, match="above the largest half-space Vs"):
+        legacy.UniformSolver(cmax=3.)(h, vp, vs, rho, [1.])
+
+
 def test_workloads_have_the_stated_shapes():
     from modisp_b200 import workloads
     batch, periods, nmodes = workloads.config2(64)
