@@ -1713,6 +1713,9 @@ int md200_uniform_models(md200_uniform *u, const double *h, const double *vp, co
   try {
     if (!u || !h || !vp || !vs || !rho) return fail("md200_uniform_models: null argument");
     const size_t n = static_cast<size_t>(u->B) * u->L;
+    for (size_t i = 0; i < n; ++i)
+      if (!(vs[i] > 0.) || !(vp[i] > 0.) || !(rho[i] > 0.))
+        return fail("md200_uniform_models: the uniform path takes solid models (vp, vs, rho > 0 in every row)");
     const double *src[4] = {h, vp, vs, rho};
     for (int i = 0; i < 4; ++i)
       MD200_CK(cudaMemcpy(u->in + i * n, src[i], n * sizeof(double), cudaMemcpyHostToDevice));

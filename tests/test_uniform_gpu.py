@@ -134,6 +134,10 @@ def test_stage_errors_follow_the_reference():
         plugin.CoarseScan(B, L).upload_models(model[0][:, :-1], *model[1:])
     with pytest.raises(ValueError, match="non-empty 1-D"):
         plugin.Refine(B, L).upload_periods([])
+    water = [x.copy() for x in model]
+    water[2][:, 0] = 0.  # a fluid top layer: not a model of this path
+    with pytest.raises(RuntimeError, match="solid models"):
+        plugin.CoarseScan(B, L).upload_models(*water)
     scan, refine = plugin.CoarseScan(B, L), plugin.Refine(B, L)
     with pytest.raises(RuntimeError, match="upload_models"):
         scan.run(.2, 4.)
