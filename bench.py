@@ -61,12 +61,12 @@ WORKLOAD = ("mixed-precision batch: 100000 models x 8-20 layers, 30 % with one l
 # each 1, an FMA 2; the elementary functions counted separately: 2 rsqrt and
 # 2 sin/cos-or-exp per Rayleigh step, 1 rsqrt and 1 sin/cos-or-exp per Love step).
 FLOPS_PER_STEP = {0: 170, 1: 24}
-# DRAM traffic of the split scan's Rayleigh evaluation kernel (split_eval32<0>) per
+# DRAM traffic of the split scan's Rayleigh evaluation kernel (split_eval32_pair) per
 # FP32 layer step it evaluates: dram__bytes_read.sum + dram__bytes_write.sum over
-# the 9 launches of one run (1,090.3 MB + 717.8 MB), from an ncu capture of 2,000
+# the 9 launches of one run (1,090.4 MB + 715.0 MB), from an ncu capture of 2,000
 # mixed-precision models, divided by that run's evaluated layer steps
-# (MD200_STAT_SPLIT_EVAL_STEPS, 437,543,083).
-EVAL_DRAM_BYTES_PER_STEP = (1090339328 + 717784832) / 437543083
+# (MD200_STAT_SPLIT_EVAL_STEPS, 437,558,855).
+EVAL_DRAM_BYTES_PER_STEP = (1090408192 + 715028480) / 437558855
 
 
 def split_rounds(n_traces):
@@ -863,7 +863,8 @@ def main():
             "e2e": {"value": e2e_value, "unit": "roots/s", "h2d_bytes_per_step": 2 * per_wave_in,
                     "d2h_bytes_per_step": 2 * per_wave_out},
             "roofline": {"bound": "fp32-cuda-core",
-                         "kernel": "split_eval32<0>: the FP32 Rayleigh evaluations of the split scan",
+                         "kernel": "split_eval32_pair: the FP32 Rayleigh evaluations of the split scan, "
+                                   "two samples per thread in paired FP32 instructions",
                          "achieved": achieved / 1e12, "peak": peak32 / 1e12, "unit": "TFLOP/s",
                          "frac": achieved / peak32,
                          "traffic": (EVAL_DRAM_BYTES_PER_STEP * eval_steps / eval_launches

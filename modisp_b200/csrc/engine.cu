@@ -358,7 +358,12 @@ int split_scan(md200_engine *e, const Dev &d, int rounds, cudaStream_t s) {
     split_feed_fill<<<fill_blocks, 256, 0, s>>>(d, p);
     split_positions<<<pos_blocks, 128, 0, s>>>(d, p);
     if (!e->capturing && cudaEventRecord(e->sp_ev[2 * r], s) != cudaSuccess) return -1;
-    split_eval32<WAVE><<<eval_blocks, 128, 0, s>>>(d, p);
+#if MD200_SPLIT_PAIR
+    if (WAVE == 0)
+      split_eval32_pair<<<eval_blocks, 128, 0, s>>>(d, p);
+    else
+#endif
+      split_eval32<WAVE><<<eval_blocks, 128, 0, s>>>(d, p);
     if (!e->capturing && cudaEventRecord(e->sp_ev[2 * r + 1], s) != cudaSuccess) return -1;
     split_redo<WAVE><<<sms * 8, 128, 0, s>>>(d, p);
     split_book<WAVE><<<book_blocks, 128, 0, s>>>(d, p);

@@ -696,6 +696,373 @@ MD200_FN void rayleigh_start(N e[5], const N &k, const N &k2, const N &w, const 
   e[4] = k2 - rarb;
 }
 
+// ---------------------------------------------------------------------------
+// Explicitly rounded single precision for the scan's Rayleigh evaluations.
+// Every addition, multiplication and fused multiply-add of the recurrence is
+// one PTX instruction with round-to-nearest and flush-to-zero, so no compiler
+// contraction chooses a rounding.  The arithmetic is written once over a lane
+// type: R1 carries one sample per thread, R2 two samples of the same trace per
+// thread in sm_100's paired single-precision instructions (add/mul/fma .f32x2,
+// one issue slot for both samples).  Per-lane work -- special functions,
+// comparisons, selections, the power-of-two normalisation -- runs on each half
+// with the same scalar code.  Each half of an R2 result is therefore bit for bit
+// the R1 result of that sample: the split scan's paired evaluations and the
+// fused scan's single ones return the same values.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float x_mul(float a, float b) {
+  float r;
+  asm("mul.rn.ftz.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ float x_add(float a, float b) {
+  float r;
+  asm("add.rn.ftz.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ float x_fma(float a, float b, float c) {
+  float r;
+  asm("fma.rn.ftz.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+}
+
+struct R1 {
+  using V = float;
+  static constexpr int NL = 1;
+  using M = bool;
+  static __device__ __forceinline__ V mul(V a, V b) { return x_mul(a, b); }
+  static __device__ __forceinline__ V add(V a, V b) { return x_add(a, b); }
+  static __device__ __forceinline__ V fma(V a, V b, V c) { return x_fma(a, b, c); }
+  static __device__ __forceinline__ V splat(float a) { return a; }
+  static __device__ __forceinline__ V neg(V a) { return -a; }
+  static __device__ __forceinline__ V abs(V a) { return fabsf(a); }
+  static __device__ __forceinline__ M lt(V a, float b) { return a < b; }
+  static __device__ __forceinline__ M gt0(V a) { return a > 0.f; }
+  static __device__ __forceinline__ V sel(M m, V a, V b) { return m ? a : b; }
+  static __device__ __forceinline__ V rsqrt0(V a) { return a > 0.f ? rsqrtf(a) : 0.f; }
+  static __device__ __forceinline__ V expneg(V a) { return __expf(-a); }
+  static __device__ __forceinline__ V rint(V a) { return rintf(a); }
+  static __device__ __forceinline__ void sincos(V r, V *s, V *c) { __sincosf(r, s, c); }
+};
+
+struct R2 {
+  using V = float2;
+  static constexpr int NL = 2;
+  struct M {
+    bool x, y;
+  };
+  static __device__ __forceinline__ unsigned long long pk(V a) {
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a.x), "f"(a.y));
+    return r;
+  }
+  static __device__ __forceinline__ V upk(unsigned long long r) {
+    V a;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a.x), "=f"(a.y) : "l"(r));
+    return a;
+  }
+  static __device__ __forceinline__ V mul(V a, V b) {
+    unsigned long long r;
+    asm("mul.rn.ftz.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pk(a)), "l"(pk(b)));
+    return upk(r);
+  }
+  static __device__ __forceinline__ V add(V a, V b) {
+    unsigned long long r;
+    asm("add.rn.ftz.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pk(a)), "l"(pk(b)));
+    return upk(r);
+  }
+  static __device__ __forceinline__ V fma(V a, V b, V c) {
+    unsigned long long r;
+    asm("fma.rn.ftz.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(pk(a)), "l"(pk(b)), "l"(pk(c)));
+    return upk(r);
+  }
+  static __device__ __forceinline__ V splat(float a) { return make_float2(a, a); }
+  static __device__ __forceinline__ V neg(V a) { return make_float2(-a.x, -a.y); }
+  static __device__ __forceinline__ V abs(V a) { return make_float2(fabsf(a.x), fabsf(a.y)); }
+  static __device__ __forceinline__ M lt(V a, float b) { return {a.x < b, a.y < b}; }
+  static __device__ __forceinline__ M gt0(V a) { return {a.x > 0.f, a.y > 0.f}; }
+  static __device__ __forceinline__ V sel(M m, V a, V b) { return make_float2(m.x ? a.x : b.x, m.y ? a.y : b.y); }
+  static __device__ __forceinline__ V rsqrt0(V a) { return make_float2(R1::rsqrt0(a.x), R1::rsqrt0(a.y)); }
+  static __device__ __forceinline__ V expneg(V a) { return make_float2(__expf(-a.x), __expf(-a.y)); }
+  static __device__ __forceinline__ V rint(V a) { return make_float2(rintf(a.x), rintf(a.y)); }
+  static __device__ __forceinline__ void sincos(V r, V *s, V *c) {
+    __sincosf(r.x, &s->x, &c->x);
+    __sincosf(r.y, &s->y, &c->y);
+  }
+};
+
+// sin and cos of a phase: reduction by 2 pi with a two-constant Cody-Waite split
+// (exact for the |x| < 2^12 rad phases of the recurrences), then the
+// special-function unit (absolute error ~4e-7, far below the scan's
+// sign-decision threshold).
+template <class P>
+__device__ __forceinline__ void sincos32(typename P::V x, typename P::V *s, typename P::V *c) {
+  const typename P::V n = P::rint(P::mul(x, P::splat(0.15915494309189535f)));
+  const typename P::V r = P::fma(n, P::splat(-1.7484555e-07f), P::fma(n, P::splat(-6.28318548f), x));
+  P::sincos(r, s, c);
+}
+
+// e <- M e for the 15 entries (t = -2 k^2 carried by the e[2] column).
+template <class P>
+__device__ __forceinline__ void apply32(typename P::V e[5], typename P::V k2, typename P::V A, typename P::V B,
+                                        typename P::V C, typename P::V D, typename P::V E, typename P::V F,
+                                        typename P::V G, typename P::V H, typename P::V I, typename P::V J,
+                                        typename P::V K, typename P::V Lm, typename P::V M, typename P::V Nn,
+                                        typename P::V O) {
+  const typename P::V e0 = e[0], e1 = e[1], e2 = e[2], e3 = e[3], e4 = e[4];
+  const typename P::V e2t = P::mul(e2, P::mul(k2, P::splat(-2.f)));
+  e[0] = P::fma(O, e4, P::fma(F, e3, P::fma(J, e2t, P::fma(E, e1, P::mul(A, e0)))));
+  e[1] = P::fma(F, e4, P::fma(Nn, e3, P::fma(H, e2t, P::fma(B, e1, P::mul(D, e0)))));
+  e[2] = P::fma(J, e4, P::fma(H, e3, P::fma(K, e2, P::fma(G, e1, P::mul(I, e0)))));
+  e[3] = P::fma(E, e4, P::fma(B, e3, P::fma(G, e2t, P::fma(M, e1, P::mul(C, e0)))));
+  e[4] = P::fma(A, e4, P::fma(D, e3, P::fma(I, e2t, P::fma(C, e1, P::mul(Lm, e0)))));
+}
+
+// One standard Dunkin layer step (both waves trigonometric or scaled
+// hyperbolic, selected per lane), the algebra of rayleigh_layer_f32.  ka, kb,
+// gammk and the density powers are the layer's per-trace constants.  Returns
+// the exponent P + Q factored out of the evanescent waves.
+template <class P>
+__device__ __forceinline__ typename P::V step32(typename P::V e[5], typename P::V k, typename P::V k2, float ka,
+                                                float kb, float gammk, float h, float rho, float irho, float rho2,
+                                                float irho2) {
+  using V = typename P::V;
+  const V one = P::splat(1.f), zero = P::splat(0.f), half = P::splat(.5f), mhalf = P::splat(-.5f);
+  const V gam = P::mul(P::splat(gammk), k2);
+  const V Xa = P::mul(P::add(k, P::splat(ka)), P::abs(P::add(k, P::splat(-ka))));
+  const V Xb = P::mul(P::add(k, P::splat(kb)), P::abs(P::add(k, P::splat(-kb))));
+  const V ira = P::rsqrt0(Xa), irb = P::rsqrt0(Xb);
+  const V ra = P::mul(Xa, ira), rb = P::mul(Xb, irb);
+  const V p = P::mul(ra, P::splat(h)), q = P::mul(rb, P::splat(h));
+  V sp, cp, sq, cq;
+  sincos32<P>(p, &sp, &cp);
+  sincos32<P>(q, &sq, &cq);
+  const V ep = P::expneg(p), eq = P::expneg(q);
+  const V fp = P::mul(ep, ep), fq = P::mul(eq, eq);
+  const typename P::M pp = P::lt(k, ka), pq = P::lt(k, kb);  // propagating P / S
+  const V cosp = P::sel(pp, cp, P::fma(fp, half, half)), sinp = P::sel(pp, sp, P::fma(fp, mhalf, half));
+  const V cosq = P::sel(pq, cq, P::fma(fq, half, half)), sinq = P::sel(pq, sq, P::fma(fq, mhalf, half));
+  // sin(r h)/r -> h as r -> 0
+  const V wv = P::sel(P::gt0(Xa), P::mul(sinp, ira), P::splat(h));
+  const V yv = P::sel(P::gt0(Xb), P::mul(sinq, irb), P::splat(h));
+  const V tp = P::mul(ra, sinp), tq = P::mul(rb, sinq);
+  const V xv = P::sel(pp, P::neg(tp), tp), zv = P::sel(pq, P::neg(tq), tq);
+  const V a0 = P::mul(P::sel(pp, one, ep), P::sel(pq, one, eq));
+  const V expo = P::add(P::sel(pp, zero, p), P::sel(pq, zero, q));
+  const V cpcq = P::mul(cosp, cosq), cpy = P::mul(cosp, yv), cpz = P::mul(cosp, zv);
+  const V cqw = P::mul(cosq, wv), cqx = P::mul(cosq, xv);
+  const V xy = P::mul(xv, yv), xz = P::mul(xv, zv), wy = P::mul(wv, yv), wz = P::mul(wv, zv);
+  const V gmk = P::splat(gammk);
+  const V gm1 = P::add(gam, P::splat(-1.f)), twgm1 = P::add(gam, gm1);
+  const V gmgmk = P::mul(gam, gmk), gmgm1 = P::mul(gam, gm1), gm1sq = P::mul(gm1, gm1);
+  const V a0pq = P::add(a0, P::neg(cpcq));
+  const V k2gm1 = P::mul(k2, gm1), k2gm1sq = P::mul(k2, gm1sq);
+  V A = P::fma(P::mul(gmgm1, P::splat(-2.f)), a0pq, cpcq);
+  A = P::fma(P::neg(gmgmk), xz, A);
+  A = P::fma(P::neg(k2gm1sq), wy, A);
+  const V D = P::mul(P::fma(k2, cpy, P::neg(cqx)), P::splat(irho));
+  const V I = P::mul(P::fma(k2gm1, wy, P::fma(twgm1, a0pq, P::mul(gmk, xz))), P::splat(-irho));
+  const V C = P::mul(P::fma(P::neg(k2), cqw, cpz), P::splat(irho));
+  const V Lm = P::mul(P::fma(P::mul(k2, k2), wy, P::fma(P::mul(k2, P::splat(2.f)), a0pq, xz)), P::splat(-irho2));
+  const V E = P::mul(P::fma(gmgmk, cpz, P::neg(P::mul(gm1sq, cqw))), P::splat(rho));
+  const V G = P::fma(gmk, cpz, P::neg(P::mul(gm1, cqw)));
+  const V F = P::mul(P::fma(gm1sq, cpy, P::neg(P::mul(gmgmk, cqx))), P::splat(rho));
+  const V H = P::fma(gm1, cpy, P::neg(P::mul(gmk, cqx)));
+  const V gg = P::mul(gmgmk, gm1sq);
+  const V O = P::mul(P::fma(P::mul(gm1sq, gm1sq), wy, P::fma(P::mul(gg, P::splat(2.f)), a0pq,
+                                                             P::mul(P::mul(gmgmk, gmgmk), xz))),
+                     P::splat(-rho2));
+  const V J = P::mul(P::fma(P::mul(gm1, gm1sq), wy, P::fma(P::mul(P::mul(gmk, gm1), twgm1), a0pq,
+                                                           P::mul(P::mul(gmgmk, gmk), xz))),
+                     P::splat(-rho));
+  const V K = P::fma(P::splat(2.f), P::add(cpcq, P::neg(A)), a0);
+  apply32<P>(e, k2, A, cpcq, C, D, E, F, G, H, I, J, K, Lm, P::neg(wz), P::neg(xy), O);
+  return expo;
+}
+
+// The factored step of rayleigh_layer_evanescent (both waves deeply evanescent,
+// c < vs / MD200_EVANESCENT_RATIO) for one sample, explicitly rounded.
+__device__ __forceinline__ float evanescent32(float e[5], float k, float k2, float c, float h, float ivp, float ivs,
+                                              float rho, float irho, float rho2, float irho2) {
+  const float cp = x_mul(c, ivp), cs = x_mul(c, ivs), u = x_mul(cp, cp), v = x_mul(cs, cs);
+  const float p = sqrtf(x_add(1.f, -u)), s = sqrtf(x_add(1.f, -v)), R = x_mul(p, s);
+  const float loss = x_fma(x_add(1.f, -u), v, u) / x_add(1.f, R);
+  const float g = 2.f / v, contrast = x_add(v, -u);
+  const float kh = x_mul(k, h), q = x_mul(kh, s);
+  float sp = .5f, sq = .5f, a0 = 0.f, delta = 0.f, gap = 0.f;
+  if (q < 16.f) {
+    const float pq = x_mul(kh, contrast) / x_add(p, s);  // P - Q, the phase difference
+    const float eq = __expf(-q), diff = x_mul(-eq, expm1f(-pq));
+    sp = x_mul(-.5f, expm1f(x_mul(-2.f, x_add(q, pq))));
+    sq = x_mul(-.5f, expm1f(x_mul(-2.f, q)));
+    a0 = x_mul(eq, x_add(eq, -diff));
+    delta = x_mul(x_mul(-.5f, diff), x_fma(2.f, eq, -diff));  // cos_p sin_q - cos_q sin_p (scaled)
+    gap = x_mul(x_mul(.5f, diff), diff);                       // cos_p cos_q - a0 - sin_p sin_q (scaled)
+  }
+  const float gm1 = x_add(g, -1.f), twgm1 = x_add(g, gm1);
+  const float gl = x_mul(g, loss);
+  const float d1 = x_add(1.f, -gl), d2 = x_fma(g, x_add(2.f, -gl), -1.f);
+  const float ps = x_mul(sp, sq), psr = ps / R;
+  const float y = x_mul(x_add(1.f, -sq), sp), x = x_mul(x_add(1.f, -sp), sq);
+  const float q1 = x_mul(x_mul(x_mul(2.f, g), gm1), gap), q2 = x_mul(x_mul(psr, d1), d1);
+  const float kp = k / p, ks = k / s, ip = 1.f / x_mul(k, p), is = 1.f / x_mul(k, s), ik2 = 1.f / k2;
+  const float B = x_mul(x_add(1.f, -sp), x_add(1.f, -sq)), A = x_add(x_add(B, q1), -q2);
+  const float D = x_mul(x_mul(ks, x_fma(loss, y, delta)), irho);
+  const float C = x_mul(x_mul(kp, x_fma(-loss, x, delta)), irho);
+  const float G = x_mul(x_fma(x_mul(g, R), delta, x_mul(d1, y)), ip);
+  const float H = x_mul(x_fma(gm1, delta, -x_mul(d1, y)), is);
+  const float E = x_mul(x_mul(x_fma(x_mul(x_mul(g, g), R), delta, x_mul(d2, y)), ip), rho);
+  const float F = x_mul(x_mul(x_fma(x_mul(gm1, gm1), delta, -x_mul(d2, y)), is), rho);
+  const float I = x_mul(x_fma(twgm1, gap, x_mul(x_mul(psr, loss), d1)), irho);
+  const float Lm = x_mul(x_mul(k2, x_fma(2.f, gap, -x_mul(x_mul(psr, loss), loss))), irho2);
+  const float J = x_mul(x_mul(x_fma(x_mul(x_mul(g, gm1), twgm1), gap, -x_mul(x_mul(psr, d1), d2)), rho), ik2);
+  const float O = x_mul(x_mul(x_fma(x_mul(g, gm1), q1, -x_mul(x_mul(psr, d2), d2)), rho2), ik2);
+  const float K = x_fma(2.f, x_add(q2, -q1), a0);
+  const float M = x_mul(-ps, s / p), Nn = x_mul(-ps, p / s);
+  apply32<R1>(e, k2, A, B, C, D, E, F, G, H, I, J, K, Lm, M, Nn, O);
+  return x_mul(kh, x_add(p, s));  // P + Q
+}
+
+// Per-lane access to a lane type's values.
+__device__ __forceinline__ float &lane_of(float &v, int) { return v; }
+__device__ __forceinline__ float &lane_of(float2 &v, int i) { return i ? v.y : v.x; }
+__device__ __forceinline__ float lane_of(const float &v, int) { return v; }
+__device__ __forceinline__ float lane_of(const float2 &v, int i) { return i ? v.y : v.x; }
+
+// Half-space start vector (the standard form, then per lane the factored form
+// well below the shear velocity).
+template <class P>
+__device__ __forceinline__ void start32(typename P::V e[5], typename P::V k, typename P::V k2, typename P::V c,
+                                        float w, float iw2, float ivp, float ivs, float vs2, float rh) {
+  using V = typename P::V;
+  const float ka = x_mul(w, ivp), kb = x_mul(w, ivs), gammk = x_mul(x_mul(iw2, vs2), 2.f), rh2 = x_mul(rh, rh);
+  const V Xa = P::mul(P::add(k, P::splat(ka)), P::abs(P::add(k, P::splat(-ka))));
+  const V Xb = P::mul(P::add(k, P::splat(kb)), P::abs(P::add(k, P::splat(-kb))));
+  const V ra = P::mul(Xa, P::rsqrt0(Xa)), rb = P::mul(Xb, P::rsqrt0(Xb));
+  const V gam = P::mul(P::splat(gammk), k2), gm1 = P::add(gam, P::splat(-1.f)), rarb = P::mul(ra, rb);
+  e[0] = P::mul(P::fma(gm1, gm1, P::neg(P::mul(P::mul(gam, P::splat(gammk)), rarb))), P::splat(rh2));
+  e[1] = P::mul(ra, P::splat(-rh));
+  e[2] = P::mul(P::fma(P::splat(-gammk), rarb, gm1), P::splat(rh));
+  e[3] = P::mul(rb, P::splat(rh));
+  e[4] = P::add(k2, P::neg(rarb));
+#pragma unroll
+  for (int i = 0; i < P::NL; ++i) {
+    const float cc = lane_of(c, i), kk = lane_of(k, i);
+    if (x_mul(x_mul(MD200_EVANESCENT_RATIO, cc), ivs) < 1.f) {
+      const float cp = x_mul(cc, ivp), cs = x_mul(cc, ivs), u = x_mul(cp, cp), v = x_mul(cs, cs);
+      const float p = sqrtf(x_add(1.f, -u)), sh = sqrtf(x_add(1.f, -v)), R = x_mul(p, sh);
+      const float loss = x_fma(x_add(1.f, -u), v, u) / x_add(1.f, R), g = 2.f / v;
+      const float d1 = x_fma(-g, loss, 1.f);
+      lane_of(e[0], i) = x_mul(rh2, x_fma(-g, x_add(1.f, d1), 1.f));
+      lane_of(e[1], i) = x_mul(x_mul(-rh, kk), p);
+      lane_of(e[2], i) = x_mul(-rh, d1);
+      lane_of(e[3], i) = x_mul(x_mul(rh, kk), sh);
+      lane_of(e[4], i) = x_mul(lane_of(k2, i), loss);
+    }
+  }
+}
+
+// Rayleigh secular value, shape feature and base-2 log-magnitude of one (R1) or
+// two (R2) samples of one trace at frequency w: the single-precision path of
+// rayleigh_multi, explicitly rounded.  c holds the samples' velocities w / k.
+template <class P>
+__device__ __forceinline__ void rayleigh_eval32(const LayerView<float> &m, typename P::V k, typename P::V c, float w,
+                                                typename P::V *F, typename P::V *shape, typename P::V *lmag) {
+  using V = typename P::V;
+  constexpr int NL = P::NL;
+  const float tiny = 1e-30f;
+  const float iw = 1.f / w, iw2 = x_mul(iw, iw);
+  const int last = m.L - 1;
+  const V k2 = P::mul(k, k);
+  V e[5];
+  start32<P>(e, k, k2, c, w, iw2, m.ivp(last), m.ivs(last), m.vs2(last), m.rho(last));
+  int ex[NL];
+  V ev = P::splat(0.f);
+#pragma unroll
+  for (int i = 0; i < NL; ++i) {
+    float t[5] = {lane_of(e[0], i), lane_of(e[1], i), lane_of(e[2], i), lane_of(e[3], i), lane_of(e[4], i)};
+    ex[i] = scale_vector(t, 5, tiny);
+#pragma unroll
+    for (int j = 0; j < 5; ++j) lane_of(e[j], i) = t[j];
+  }
+  for (int l = m.L - 2; l >= m.water; --l) {
+    const float h = m.h(l), ivp = m.ivp(l), vs2 = m.vs2(l), ivs = m.ivs(l), rho = m.rho(l), irho = m.irho(l);
+    const float ka = x_mul(w, ivp), kb = x_mul(w, ivs), gammk = x_mul(x_mul(iw2, vs2), 2.f);
+    const float rho2 = x_mul(rho, rho), irho2 = x_mul(irho, irho);
+    bool evan[NL], any = false, all = true;
+#pragma unroll
+    for (int i = 0; i < NL; ++i) {
+      evan[i] = x_mul(x_mul(MD200_EVANESCENT_RATIO, lane_of(c, i)), ivs) < 1.f;
+      any |= evan[i];
+      all &= evan[i];
+    }
+    V en[5] = {e[0], e[1], e[2], e[3], e[4]};
+    V expo = P::splat(0.f);
+    if (!all) expo = step32<P>(en, k, k2, ka, kb, gammk, h, rho, irho, rho2, irho2);
+    if (any) {
+#pragma unroll
+      for (int i = 0; i < NL; ++i) {
+        if (evan[i]) {
+          float t[5] = {lane_of(e[0], i), lane_of(e[1], i), lane_of(e[2], i), lane_of(e[3], i), lane_of(e[4], i)};
+          lane_of(expo, i) = evanescent32(t, lane_of(k, i), lane_of(k2, i), lane_of(c, i), h, ivp, ivs, rho, irho,
+                                          rho2, irho2);
+#pragma unroll
+          for (int j = 0; j < 5; ++j) lane_of(en[j], i) = t[j];
+        }
+      }
+    }
+    ev = P::add(ev, expo);
+#pragma unroll
+    for (int i = 0; i < NL; ++i) {
+      float t[5] = {lane_of(en[0], i), lane_of(en[1], i), lane_of(en[2], i), lane_of(en[3], i), lane_of(en[4], i)};
+      ex[i] += scale_vector(t, 5, tiny);
+#pragma unroll
+      for (int j = 0; j < 5; ++j) lane_of(e[j], i) = t[j];
+    }
+  }
+  V lm;
+#pragma unroll
+  for (int i = 0; i < NL; ++i) lane_of(lm, i) = static_cast<float>(ex[i]);
+  lm = P::fma(ev, P::splat(1.4426950408889634f), lm);
+  if (m.water) {
+    const float h0 = m.h(0), ivp0 = m.ivp(0), rho0 = m.rho(0), ka = x_mul(w, ivp0);
+#pragma unroll
+    for (int i = 0; i < NL; ++i) {
+      const float kk = lane_of(k, i);
+      const float X = x_mul(x_add(kk, ka), fabsf(x_add(kk, -ka)));
+      const float irf = R1::rsqrt0(X), rf = x_mul(X, irf), ph = x_mul(rf, h0);
+      float cpw, wv;
+      if (kk < ka) {
+        float sn;
+        sincos32<R1>(ph, &sn, &cpw);
+        wv = x_mul(sn, irf);
+      } else if (kk == ka) {
+        cpw = 1.f;
+        wv = h0;
+      } else {
+        const float ez = __expf(-ph), z = x_mul(ez, ez);
+        cpw = x_fma(z, .5f, .5f);
+        wv = x_mul(x_fma(z, -.5f, .5f), irf);
+      }
+      float pair[2] = {x_mul(cpw, lane_of(e[0], i)), x_mul(x_mul(wv, lane_of(e[1], i)), rho0)};
+      const int pex = scale_vector(pair, 2, tiny);
+      const float u = pair[0], v = pair[1], nn = x_add(x_fma(v, v, x_mul(u, u)), tiny), Fv = x_add(u, -v);
+      if (shape) lane_of(*shape, i) = x_mul(Fv, rsqrtf(nn));
+      if (lmag) lane_of(*lmag, i) = x_add(lane_of(lm, i), x_fma(.5f, log2f(nn), static_cast<float>(pex)));
+      lane_of(*F, i) = Fv;
+    }
+  } else {
+    const V n2 = P::add(P::fma(e[4], e[4], P::fma(e[3], e[3], P::fma(e[2], e[2], P::fma(e[1], e[1],
+                                                                                     P::mul(e[0], e[0]))))),
+                        P::splat(tiny));
+#pragma unroll
+    for (int i = 0; i < NL; ++i) {
+      const float nn = lane_of(n2, i);
+      if (shape) lane_of(*shape, i) = x_mul(lane_of(e[0], i), rsqrtf(nn));
+      if (lmag) lane_of(*lmag, i) = x_fma(.5f, log2f(nn), lane_of(lm, i));
+    }
+    *F = e[0];
+  }
+}
 // Rayleigh secular values F(k_s, w) of S samples at one frequency, with shape
 // features g = F / |e| (water top: the fluid form).  Units: k = w / c in rad/km,
 // w in rad/s.  The S recurrences are independent and interleaved layer by layer
@@ -712,6 +1079,15 @@ MD200_FN void rayleigh_multi(const LayerView<T> &m, const N *k, const N &w, N *F
                              typename Base<N>::type *lmag, typename Base<N>::type *levan = nullptr,
                              typename Base<N>::type *fmax = nullptr) {
   using B = typename Base<N>::type;
+#if defined(__CUDA_ARCH__)
+  // the scan's single-precision evaluations: explicitly rounded (rayleigh_eval32)
+  if constexpr (std::is_same<N, float>::value && std::is_same<T, float>::value && S == 1) {
+    if (levan == nullptr && fmax == nullptr) {
+      rayleigh_eval32<R1>(m, k[0], w / k[0], w, F, shape, lmag);
+      return;
+    }
+  }
+#endif
   const B tiny = sizeof(B) == 4 ? B(1e-30) : B(1e-40);
   const N iw = lift_one<N>() / w;
   const N iw2 = iw * iw;

@@ -13,6 +13,9 @@
 //   split_eval32           one thread per sample: the FP32 secular value; the
 //                          near-cutoff band takes the trace's FP64 tail values;
 //                          sign-uncertain samples are listed for FP64
+//   split_eval32_pair      Rayleigh: the same with one thread per two samples of
+//                          a trace, evaluated together in paired FP32
+//                          instructions (sm_100 .f32x2)
 //   split_redo             one thread per listed sample: its FP64 value
 //   split_book             one thread per trace: the samples in order through
 //                          the fused scan's bookkeeping (sign changes, regular
@@ -36,13 +39,22 @@ namespace md200 {
 
 // Compile-time tuning: 32-sample steps per trace per round (two measured best:
 // fewer samples evaluated past a trace's last bracket than four, half the
-// rounds of one) and the evaluation kernel's minimum resident CTAs per SM (1:
-// no register cap; capping it measured no faster).
+// rounds of one); the evaluation kernel's minimum resident CTAs per SM (1: no
+// register cap; capping it measured no faster); Rayleigh values two samples
+// per thread in paired FP32 instructions (split_eval32_pair, on with two steps
+// per round) and that kernel's minimum resident CTAs per SM (4: 122 registers,
+// no spills; uncapped, 138 registers and 3 CTAs ran 13 % slower, 5 CTAs spill).
 #ifndef MD200_SPLIT_STEPS
 #define MD200_SPLIT_STEPS 2
 #endif
 #ifndef MD200_SPLIT_EVAL_BLOCKS
 #define MD200_SPLIT_EVAL_BLOCKS 1
+#endif
+#ifndef MD200_SPLIT_PAIR
+#define MD200_SPLIT_PAIR (MD200_SPLIT_STEPS == 2)
+#endif
+#ifndef MD200_SPLIT_PAIR_BLOCKS
+#define MD200_SPLIT_PAIR_BLOCKS 4
 #endif
 constexpr int SPLIT_STEPS = MD200_SPLIT_STEPS;    // 32-sample steps per trace per round
 constexpr int SPLIT_SAMPLES = 32 * SPLIT_STEPS;  // sample slots per active trace
@@ -184,6 +196,22 @@ __global__ void __launch_bounds__(128) split_positions(Dev d, int p) {
   }
 }
 
+// A near-cutoff sample: the trace's FP64 tail value when it is at this position
+// (returns false), else true (the sample goes to the FP64 list).
+__device__ __forceinline__ bool split_near(const Dev &d, int t, SplitSample &smp, double c, unsigned &k) {
+  const double4 *tail = d.tail + 2 * static_cast<size_t>(t);
+  const double4 t0 = tail[0], t1 = tail[1];
+  const double4 tv = c == t0.x ? t0 : t1;
+  if (c == tv.x && isfinite(tv.y)) {
+    smp.F = tv.y;
+    smp.g = static_cast<float>(tv.z);
+    smp.M = static_cast<float>(tv.w);
+    k |= SK_EXACT;
+    return false;
+  }
+  return true;
+}
+
 // One thread per sample slot: the FP32 value (the fused scan's scan_eval call on
 // the same single-precision position), or the trace's FP64 tail value in the
 // near-cutoff band; samples the FP32 value leaves sign-uncertain, and near-cutoff
@@ -204,17 +232,7 @@ __global__ void __launch_bounds__(128, MD200_SPLIT_EVAL_BLOCKS) split_eval32(Dev
     if (c < INFINITY) {
       const SplitTrace tr = d.sp_tr[i];
       if (k & SK_NEAR) {
-        const double4 *tail = d.tail + 2 * static_cast<size_t>(tr.t);
-        const double4 t0 = tail[0], t1 = tail[1];
-        const double4 tv = c == t0.x ? t0 : t1;
-        if (c == tv.x && isfinite(tv.y)) {
-          smp.F = tv.y;
-          smp.g = static_cast<float>(tv.z);
-          smp.M = static_cast<float>(tv.w);
-          k |= SK_EXACT;
-        } else {
-          redo = true;
-        }
+        redo = split_near(d, tr.t, smp, c, k);
       } else {
         const LayerView<float> view = make_view<float>(layer_table<float>(d, tr.b), d.Ls, tr.L, tr.water);
         const float c32 = static_cast<float>(c);
@@ -237,6 +255,69 @@ __global__ void __launch_bounds__(128, MD200_SPLIT_EVAL_BLOCKS) split_eval32(Dev
     if (lane == 0 && steps) atomicAdd(&d.stats[19], steps);
   }
 }
+
+#if MD200_SPLIT_PAIR
+// Rayleigh: one thread per pair of sample slots of an active trace -- slot j of
+// its first 32-sample step and slot j of its second -- whose FP32 values come
+// from one paired evaluation (rayleigh_eval32<R2>: each half bit for bit the
+// single evaluation split_eval32 and the fused scan make).  A slot past the
+// window or in the near-cutoff band leaves its half to a copy of the other
+// sample, whose result is not stored.
+static_assert(SPLIT_SAMPLES == 64, "the paired evaluation takes the two 32-sample steps of a round");
+__global__ void __launch_bounds__(128, MD200_SPLIT_PAIR_BLOCKS) split_eval32_pair(Dev d, int p) {
+  const int lane = threadIdx.x & 31;
+  const long long n = static_cast<long long>(d.ctr[C_SP_ACT0 + p]) * 32;
+  const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
+  unsigned long long steps = 0;
+  // whole warps run the loop (n and stride are multiples of 32): appends are warp-wide
+  for (long long q = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; q < n; q += stride) {
+    const int i = static_cast<int>(q >> 5);
+    const long long q0 = static_cast<long long>(i) * SPLIT_SAMPLES + (q & 31), q1 = q0 + 32;
+    SplitSample &s0 = d.sp_s[q0], &s1 = d.sp_s[q1];
+    const double c0 = s0.c, c1 = s1.c;
+    unsigned k0 = s0.k, k1 = s1.k;
+    bool redo0 = false, redo1 = false;
+    if (c0 < INFINITY || c1 < INFINITY) {
+      const SplitTrace tr = d.sp_tr[i];
+      const bool e0 = c0 < INFINITY && !(k0 & SK_NEAR), e1 = c1 < INFINITY && !(k1 & SK_NEAR);
+      if (c0 < INFINITY && !e0) redo0 = split_near(d, tr.t, s0, c0, k0);
+      if (c1 < INFINITY && !e1) redo1 = split_near(d, tr.t, s1, c1, k1);
+      if (e0 || e1) {
+        const LayerView<float> view = make_view<float>(layer_table<float>(d, tr.b), d.Ls, tr.L, tr.water);
+        const float w = static_cast<float>(tr.w);
+        const float x0 = static_cast<float>(e0 ? c0 : c1), x1 = static_cast<float>(e1 ? c1 : c0);
+        const float2 kk = make_float2(w / x0, w / x1);
+        float2 F, g, M;
+        rayleigh_eval32<R2>(view, kk, make_float2(w / kk.x, w / kk.y), w, &F, &g, &M);
+        const unsigned long long ls = layer_steps(tr.L, tr.water);
+        if (e0) {
+          s0.F = F.x;
+          s0.g = g.x;
+          s0.M = M.x;
+          redo0 = !(fabs(static_cast<double>(g.x)) > MD200_REDO_G);
+          steps += ls;
+        }
+        if (e1) {
+          s1.F = F.y;
+          s1.g = g.y;
+          s1.M = M.y;
+          redo1 = !(fabs(static_cast<double>(g.y)) > MD200_REDO_G);
+          steps += ls;
+        }
+      }
+      if (c0 < INFINITY && !redo0) s0.k = k0;
+      if (c1 < INFINITY && !redo1) s1.k = k1;
+    }
+    int at = warp_append(&d.ctr[C_SP_REDO], (redo0 ? 1 : 0) + (redo1 ? 1 : 0), lane);
+    if (redo0) d.sp_redo[at++] = static_cast<int>(q0);
+    if (redo1) d.sp_redo[at] = static_cast<int>(q1);
+  }
+  if (d.stats) {
+    for (int o = 16; o; o >>= 1) steps += __shfl_xor_sync(FULL, steps, o);
+    if (lane == 0 && steps) atomicAdd(&d.stats[19], steps);
+  }
+}
+#endif  // MD200_SPLIT_PAIR
 
 // One thread per listed sample: its FP64 value (eval64_outline, as in the fused
 // scan).
