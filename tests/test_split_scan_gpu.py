@@ -2,11 +2,14 @@
 
 The single-precision scan runs either as one fused kernel (a warp scans one trace
 from start to end) or as rounds of split kernels over an active set of traces
-(positions one warp per trace, FP32 values one thread per sample, FP64
-re-evaluations one thread per listed sample, bookkeeping one thread per trace,
-trough windows and last cells one warp per request; modisp_b200/csrc/split_scan.cuh).
-Every decision follows the same rule in the same order, so both must return the
-same brackets -- and therefore identical velocities, group velocities, flags,
+(positions one warp per trace, FP32 values one thread per sample -- for Rayleigh
+one thread per two samples in paired f32x2 instructions --, FP64 re-evaluations
+one thread per listed sample, bookkeeping one thread per trace, trough windows and
+last cells one warp per request; modisp_b200/csrc/split_scan.cuh).  The paired
+Rayleigh evaluation must give each sample the value the fused kernel's single
+evaluation gives (both are explicitly rounded, rayleigh_eval32), pairs mixing
+propagating, evanescent and water-top lanes included, and every decision follows
+the same rule in the same order, so both must return the same brackets -- and therefore identical velocities, group velocities, flags,
 levels and counts, bit for bit -- on crustal, low-velocity-layer and water-layer
 batches, the reference suite's frozen fixtures, the large uneven workload (whose
 deep models outlast the rounds and are finished by the fused kernel), and with
