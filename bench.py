@@ -92,6 +92,10 @@ def parse():
     p.add_argument("--no-reliability", action="store_true")
     p.add_argument("--no-reference-cuda", action="store_true")
     p.add_argument("--no-uniform", action="store_true")
+    p.add_argument("--no-autotune", action="store_true",
+                   help="the engine's default launch shape and scan form (4 warps per CTA, CTAs per SM "
+                        "from registers, automatic scan form) instead of tuning them on a sample; for runs "
+                        "under a profiler, whose serialised launches mislead the tuner")
     return p.parse_args()
 
 
@@ -727,7 +731,8 @@ def main():
     # launch shape and FP32 scan form, chosen by the autotuner on a 1,000-model sample
     from modisp_b200 import autotune
     sample = {k: v[:1000] for k, v in batch.items()}
-    tuned = {single: autotune.autotune(sample, periods, nmodes, None, single, device=local, use_cache=False)
+    tuned = {single: ((4, 0, 0) if args.no_autotune else
+                      autotune.autotune(sample, periods, nmodes, None, single, device=local, use_cache=False))
              for single in (True, False)}
 
     def engine(single):
@@ -853,10 +858,11 @@ def main():
                        "waves": ["rayleigh", "love"], "c_tol_rel": TOL, "l2": "flushed between steps (256 MiB write)",
                        "parallelism": f"model-sharded x{world}",
                        "scan_launch_shape": {"fp32": list(tuned[True]), "fp64": list(tuned[False]),
-                                             "chosen_by": "autotuner on 1,000 of the models, both waves: fused-scan warps "
-                                                           "per CTA, CTAs per SM, FP32 scan form (0 automatic: "
-                                                           "split rounds for Rayleigh, fused for Love; 1 fused; "
-                                                           "2 split)"}},
+                                             "chosen_by": ("engine defaults (--no-autotune)" if args.no_autotune else
+                                                           "autotuner on 1,000 of the models, both waves") +
+                                                          ": fused-scan warps per CTA, CTAs per SM, FP32 scan form "
+                                                          "(0 automatic: split rounds for Rayleigh, fused for Love; "
+                                                          "1 fused; 2 split)"}},
             "fp64": {"value": value64, "unit": "roots/s", "ms_per_step": ms64 / args.steps,
                      "fp32_scan_speedup": value / value64,
                      "stage_ms": {("rayleigh" if w == 0 else "love"): stage64[w] for w in (0, 1)}},
