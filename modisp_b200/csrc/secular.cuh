@@ -997,16 +997,22 @@ __device__ __forceinline__ void rayleigh_eval32(const LayerView<float> &m, typen
     }
     V en[5] = {e[0], e[1], e[2], e[3], e[4]};
     V expo = P::splat(0.f);
-    if (!all) expo = step32<P>(en, k, k2, ka, kb, gammk, h, rho, irho, rho2, irho2);
-    if (any) {
+    if constexpr (NL == 1) {
+      if (evan[0]) expo = evanescent32(en, k, k2, c, h, ivp, ivs, rho, irho, rho2, irho2);
+      else expo = step32<P>(en, k, k2, ka, kb, gammk, h, rho, irho, rho2, irho2);
+    } else {
+      if (!all) expo = step32<P>(en, k, k2, ka, kb, gammk, h, rho, irho, rho2, irho2);
+      if (any) {
 #pragma unroll
-      for (int i = 0; i < NL; ++i) {
-        if (evan[i]) {
-          float t[5] = {lane_of(e[0], i), lane_of(e[1], i), lane_of(e[2], i), lane_of(e[3], i), lane_of(e[4], i)};
-          lane_of(expo, i) = evanescent32(t, lane_of(k, i), lane_of(k2, i), lane_of(c, i), h, ivp, ivs, rho, irho,
-                                          rho2, irho2);
+        for (int i = 0; i < NL; ++i) {
+          if (evan[i]) {
+            float t[5] = {lane_of(e[0], i), lane_of(e[1], i), lane_of(e[2], i), lane_of(e[3], i),
+                          lane_of(e[4], i)};
+            lane_of(expo, i) = evanescent32(t, lane_of(k, i), lane_of(k2, i), lane_of(c, i), h, ivp, ivs, rho,
+                                            irho, rho2, irho2);
 #pragma unroll
-          for (int j = 0; j < 5; ++j) lane_of(en[j], i) = t[j];
+            for (int j = 0; j < 5; ++j) lane_of(en[j], i) = t[j];
+          }
         }
       }
     }
