@@ -360,7 +360,7 @@ int split_scan(md200_engine *e, const Dev &d, int rounds, cudaStream_t s) {
     if (!e->capturing && cudaEventRecord(e->sp_ev[2 * r], s) != cudaSuccess) return -1;
 #if MD200_SPLIT_PAIR
     if (WAVE == 0)
-      split_eval32_pair<<<eval_blocks, 128, 0, s>>>(d, p);
+      split_eval32_pair<<<sms * MD200_SPLIT_PAIR_GRID, 128, 0, s>>>(d, p);
     else
 #endif
       split_eval32<WAVE><<<eval_blocks, 128, 0, s>>>(d, p);

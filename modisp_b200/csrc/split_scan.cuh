@@ -42,8 +42,10 @@ namespace md200 {
 // rounds of one); the evaluation kernel's minimum resident CTAs per SM (1: no
 // register cap; capping it measured no faster); Rayleigh values two samples
 // per thread in paired FP32 instructions (split_eval32_pair, on with two steps
-// per round) and that kernel's minimum resident CTAs per SM (4: 122 registers,
-// no spills; uncapped, 138 registers and 3 CTAs ran 13 % slower, 5 CTAs spill).
+// per round), that kernel's minimum resident CTAs per SM (4: 122 registers,
+// no spills; uncapped, 138 registers and 3 CTAs ran 13 % slower, 5 CTAs spill)
+// and its grid in CTAs per SM (64: 2.4 % faster than 16, 128 no faster; the
+// grid-stride loop then takes a few pairs per thread).
 #ifndef MD200_SPLIT_STEPS
 #define MD200_SPLIT_STEPS 2
 #endif
@@ -55,6 +57,9 @@ namespace md200 {
 #endif
 #ifndef MD200_SPLIT_PAIR_BLOCKS
 #define MD200_SPLIT_PAIR_BLOCKS 4
+#endif
+#ifndef MD200_SPLIT_PAIR_GRID
+#define MD200_SPLIT_PAIR_GRID 64
 #endif
 constexpr int SPLIT_STEPS = MD200_SPLIT_STEPS;    // 32-sample steps per trace per round
 constexpr int SPLIT_SAMPLES = 32 * SPLIT_STEPS;  // sample slots per active trace
