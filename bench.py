@@ -63,10 +63,10 @@ WORKLOAD = ("mixed-precision batch: 100000 models x 8-20 layers, 30 % with one l
 FLOPS_PER_STEP = {0: 170, 1: 24}
 # DRAM traffic of the split scan's Rayleigh evaluation kernel (split_eval32_pair) per
 # FP32 layer step it evaluates: dram__bytes_read.sum + dram__bytes_write.sum over
-# the 9 launches of one run (1,090.4 MB + 715.0 MB), from an ncu capture of 2,000
+# the 9 launches of one run (1,090.4 MB + 715.8 MB), from an ncu capture of 2,000
 # mixed-precision models, divided by that run's evaluated layer steps
 # (MD200_STAT_SPLIT_EVAL_STEPS, 437,558,855).
-EVAL_DRAM_BYTES_PER_STEP = (1090408192 + 715028480) / 437558855
+EVAL_DRAM_BYTES_PER_STEP = (1090352896 + 715775488) / 437558855
 
 
 def split_rounds(n_traces):
